@@ -1,0 +1,673 @@
+// C ABI of the k-NN graph builder: argument checks, device scratch, stage order.
+//
+// Replaces the orchestration of EuclideanDistanceMatrixGPU
+// (euclideandistancematrixgpu.cu:2759-2819 initialize, :2861-2896 calculate,
+// :2908-2915 the result copy of saveResultToResultFile).  The reference owns one
+// pitched column-major copy of the points, per-block N-byte bitmaps
+// (SMs*10*N bytes, .cu:2797) and candidate buffers; here the points are
+// row-major and padded to whole float4s, and scratch is O(trees*n + n*k),
+// owned by a reusable context.  Errors come back as status codes; nothing is
+// printed and the device is never reset.
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+
+#include "knn_internal.cuh"
+#include "knn_kernels.cuh"
+
+namespace knn {
+int exact_fp64(const float* X, int64_t n, int d, int dpad, int k, int metric,
+               const int64_t* queries, int64_t nq, double* norms, double* part_dist,
+               uint32_t* part_idx, int slices, double* out_dist, int32_t* out_idx,
+               cudaStream_t st);
+void launch_normalize_reference(float* X, int64_t n, int d, cudaStream_t st);
+}  // namespace knn
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& what) {
+  g_last_error = what;
+  return code;
+}
+int fail_cuda(cudaError_t e, const char* where) {
+  g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? KNN_ERR_OOM : KNN_ERR_CUDA;
+}
+
+#define KNN_CK(call)                                  \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) return fail_cuda(e_, #call); \
+  } while (0)
+
+struct Buffer {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct knn_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[8] = {};
+  std::map<std::string, Buffer> bufs;
+
+  // Device buffer `name` of at least `bytes`; grows by reallocation.
+  int get(const char* name, size_t bytes, void** out) {
+    Buffer& b = bufs[name];
+    if (bytes == 0) bytes = 16;
+    if (b.bytes < bytes) {
+      if (b.p) {
+        cudaError_t e = cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+        if (e != cudaSuccess) return fail_cuda(e, "cudaFree");
+      }
+      cudaError_t e = cudaMalloc(&b.p, bytes);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail_cuda(e, (std::string("cudaMalloc ") + name).c_str());
+      }
+      b.bytes = bytes;
+    }
+    *out = b.p;
+    return KNN_OK;
+  }
+  template <typename T>
+  int get(const char* name, size_t count, T** out) {
+    void* p = nullptr;
+    int rc = get(name, count * sizeof(T), &p);
+    *out = static_cast<T*>(p);
+    return rc;
+  }
+  int64_t bytes_held() const {
+    int64_t s = 0;
+    for (const auto& kv : bufs) s += (int64_t)kv.second.bytes;
+    return s;
+  }
+  ~knn_context() {
+    int cur = 0;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != device) cudaSetDevice(device);
+    for (auto& kv : bufs)
+      if (kv.second.p) cudaFree(kv.second.p);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+    if (cur != device) cudaSetDevice(cur);
+  }
+};
+
+namespace {
+
+int make_context(int device, knn_context** out) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(KNN_ERR_NO_DEVICE, "no CUDA device");
+  }
+  if (device < 0) KNN_CK(cudaGetDevice(&device));
+  if (device >= count) return fail(KNN_ERR_ARGS, "device ordinal out of range");
+  KNN_CK(cudaSetDevice(device));
+  std::unique_ptr<knn_context> c(new knn_context());
+  c->device = device;
+  KNN_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  for (auto& ev : c->ev) KNN_CK(cudaEventCreate(&ev));
+  *out = c.release();
+  return KNN_OK;
+}
+
+thread_local std::map<int, std::unique_ptr<knn_context>> g_default;
+
+int default_context(int device, knn_context** out) {
+  if (device < 0) {
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(KNN_ERR_NO_DEVICE, "no CUDA device");
+    }
+  }
+  auto it = g_default.find(device);
+  if (it != g_default.end()) {
+    *out = it->second.get();
+    return KNN_OK;
+  }
+  knn_context* c = nullptr;
+  int rc = make_context(device, &c);
+  if (rc) return rc;
+  g_default[device].reset(c);
+  *out = c;
+  return KNN_OK;
+}
+
+int check_common(const void* points, int64_t n, int d, int k, int metric) {
+  if (!points) return fail(KNN_ERR_ARGS, "points is NULL");
+  if (n < 1 || n >= (int64_t)INT32_MAX) return fail(KNN_ERR_ARGS, "n out of range");
+  if (d < 1) return fail(KNN_ERR_ARGS, "d must be >= 1");
+  if (k < 1 || k > KNN_MAX_K) return fail(KNN_ERR_ARGS, "k must be in 1..KNN_MAX_K");
+  if (metric < 0 || metric > 2) return fail(KNN_ERR_ARGS, "unknown metric");
+  if (n <= k) return fail(KNN_ERR_N_LE_K, "n must exceed k");
+  return KNN_OK;
+}
+
+inline int round4(int d) { return (d + 3) & ~3; }
+
+struct Prepared {
+  const float* X = nullptr;
+  int dpad = 0;
+};
+
+// Points -> zero-padded float32 rows on the device.
+int prepare_points(knn_context* C, const void* points, int64_t n, int d, const knn_options& o,
+                   cudaStream_t st, Prepared* P, knn::LaunchLog& log) {
+  const int dpad = round4(d);
+  const int64_t ld = o.ld ? o.ld : d;
+  if (ld < d) return fail(KNN_ERR_ARGS, "ld < d");
+  P->dpad = dpad;
+  const size_t esz = o.dtype == KNN_F32 ? 4 : 2;
+  if (o.points_on_device) {
+    if (o.dtype == KNN_F32 && ld == d && (d & 3) == 0 && ((uintptr_t)points & 15) == 0) {
+      P->X = static_cast<const float*>(points);
+      return KNN_OK;
+    }
+    float* X = nullptr;
+    int rc = C->get("X", (size_t)n * dpad, &X);
+    if (rc) return rc;
+    knn::launch_pad_rows(points, o.dtype, n, d, ld, X, dpad, st);
+    log.add();
+    P->X = X;
+    return KNN_OK;
+  }
+  float* X = nullptr;
+  int rc = C->get("X", (size_t)n * dpad, &X);
+  if (rc) return rc;
+  if (o.dtype == KNN_F32) {
+    KNN_CK(cudaMemcpy2DAsync(X, (size_t)dpad * 4, points, (size_t)ld * 4, (size_t)d * 4, (size_t)n,
+                             cudaMemcpyHostToDevice, st));
+    if (dpad != d)
+      KNN_CK(cudaMemset2DAsync(X + d, (size_t)dpad * 4, 0, (size_t)(dpad - d) * 4, (size_t)n, st));
+  } else {
+    void* stage = nullptr;
+    rc = C->get("stage", (size_t)n * ld * esz, &stage);
+    if (rc) return rc;
+    KNN_CK(cudaMemcpyAsync(stage, points, (size_t)n * ld * esz, cudaMemcpyHostToDevice, st));
+    knn::launch_pad_rows(stage, o.dtype, n, d, ld, X, dpad, st);
+    log.add();
+  }
+  P->X = X;
+  return KNN_OK;
+}
+
+struct Trees {
+  int32_t* perm = nullptr;
+  int depth = 0;
+};
+
+int run_trees(knn_context* C, const float* X, int64_t n, int d, int dpad, int trees, int leaf,
+              uint64_t seed, cudaStream_t st, Trees* T, knn::LaunchLog& log) {
+  const int depth = knn::tree_depth(n, leaf);
+  if (depth > 30) return fail(KNN_ERR_ARGS, "tree too deep (n / leaf too large)");
+  knn::TreeArgs a{};
+  a.X = X;
+  a.n = n;
+  a.d = d;
+  a.dpad = dpad;
+  a.trees = trees;
+  a.depth = depth;
+  a.seed = seed;
+  int rc = C->get("perm", (size_t)trees * n, &a.perm);
+  if (!rc) rc = C->get("perm_alt", (size_t)trees * n, &a.perm_alt);
+  if (!rc) rc = C->get("keys", (size_t)trees * n, &a.keys);
+  const size_t dir_nodes = depth > 0 ? ((size_t)1 << (depth - 1)) : 1;
+  if (!rc) rc = C->get("dirs", (size_t)trees * dir_nodes * dpad, &a.dirs);
+  if (rc) return rc;
+  a.stream = st;
+  rc = knn::tree_build(a, log);
+  if (rc) return fail_cuda(cudaGetLastError(), "tree build launch");
+  T->perm = a.perm;
+  T->depth = depth;
+  return KNN_OK;
+}
+
+struct Lists {
+  float* key[2];
+  uint32_t* id[2];
+  uint32_t* flags[2];
+  int cur = 0;
+};
+
+int get_lists(knn_context* C, int64_t n, int k, Lists* L) {
+  const int kw = (k + 31) / 32;
+  int rc = C->get("key0", (size_t)n * k, &L->key[0]);
+  if (!rc) rc = C->get("key1", (size_t)n * k, &L->key[1]);
+  if (!rc) rc = C->get("id0", (size_t)n * k, &L->id[0]);
+  if (!rc) rc = C->get("id1", (size_t)n * k, &L->id[1]);
+  if (!rc) rc = C->get("flags0", (size_t)n * kw, &L->flags[0]);
+  if (!rc) rc = C->get("flags1", (size_t)n * kw, &L->flags[1]);
+  L->cur = 0;
+  return rc;
+}
+
+int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, int trees,
+             int depth, int metric, const int32_t* perm, const float* norms, Lists* L,
+             unsigned long long* counter, cudaStream_t st, knn::LaunchLog& log) {
+  const int kw = (k + 31) / 32;
+  knn::launch_init_lists(L->key[L->cur], L->id[L->cur], L->flags[L->cur], n, k, kw, st);
+  log.add(2);
+  knn::LeafArgs a{};
+  a.X = X;
+  a.n = n;
+  a.d = d;
+  a.dpad = dpad;
+  a.k = k;
+  a.trees = trees;
+  a.depth = depth;
+  a.metric = metric;
+  a.perm = perm;
+  a.norms = norms;
+  a.rkey = L->key[L->cur];
+  a.rid = L->id[L->cur];
+  a.pair_counter = counter;
+  a.stream = st;
+  int rc = knn::leaf_stage(a, log);
+  if (rc) return fail_cuda(cudaGetLastError(), "leaf stage launch");
+  (void)C;
+  return KNN_OK;
+}
+
+int run_prop(const float* X, int64_t n, int d, int dpad, int k, int metric, const float* norms,
+             const int32_t* order, Lists* L, bool with_flags, unsigned long long* counter,
+             cudaStream_t st, knn::LaunchLog& log) {
+  knn::PropArgs a{};
+  a.X = X;
+  a.n = n;
+  a.d = d;
+  a.dpad = dpad;
+  a.k = k;
+  a.metric = metric;
+  a.norms = norms;
+  a.order = order;
+  a.key_in = L->key[L->cur];
+  a.id_in = L->id[L->cur];
+  a.flags_in = with_flags ? L->flags[L->cur] : nullptr;
+  a.key_out = L->key[1 - L->cur];
+  a.id_out = L->id[1 - L->cur];
+  a.flags_out = L->flags[1 - L->cur];
+  a.cand_counter = counter;
+  a.stream = st;
+  int rc = knn::propagate_step(a, log);
+  if (rc == KNN_ERR_UNSUPPORTED) return fail(rc, "propagation scratch exceeds shared memory (k or d too large)");
+  if (rc) return fail_cuda(cudaGetLastError(), "propagation launch");
+  L->cur = 1 - L->cur;
+  return KNN_OK;
+}
+
+int resolve_options(const knn_options* opt, knn_options* o) {
+  knn_default_options(o);
+  if (opt) {
+    if (opt->struct_size != (int32_t)sizeof(knn_options))
+      return fail(KNN_ERR_ARGS, "knn_options.struct_size mismatch");
+    *o = *opt;
+  }
+  if (o->dtype < 0 || o->dtype > 2) return fail(KNN_ERR_ARGS, "unknown dtype");
+  if (o->precision < 0 || o->precision > 1) return fail(KNN_ERR_ARGS, "unknown precision mode");
+  return KNN_OK;
+}
+
+int enter_device(knn_context** ctx, const knn_options& o) {
+  if (!*ctx) {
+    int rc = default_context(o.device, ctx);
+    if (rc) return rc;
+  } else if (o.device >= 0 && o.device != (*ctx)->device) {
+    return fail(KNN_ERR_ARGS, "context device differs from options.device");
+  }
+  KNN_CK(cudaSetDevice((*ctx)->device));
+  return KNN_OK;
+}
+
+int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t k,
+               int32_t trees, int32_t leaf, int32_t props, int32_t metric, uint64_t seed,
+               int32_t* out_idx, float* out_dist, const knn_options& o, knn_stats* stats) {
+  cudaStream_t st = o.stream ? static_cast<cudaStream_t>(o.stream) : C->stream;
+  knn::LaunchLog log;
+  const bool timed = stats != nullptr;
+  if (timed) KNN_CK(cudaEventRecord(C->ev[0], st));
+
+  unsigned long long* counters = nullptr;
+  int rc = C->get("counters", 2 + KNN_MAX_PROPS, &counters);
+  if (rc) return rc;
+  if (stats) KNN_CK(cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * (2 + KNN_MAX_PROPS), st));
+
+  Prepared P;
+  rc = prepare_points(C, points, n, d, o, st, &P, log);
+  if (rc) return rc;
+  float* norms = nullptr;
+  if (metric == KNN_METRIC_COSINE) {
+    rc = C->get("norms", (size_t)n, &norms);
+    if (rc) return rc;
+    knn::launch_norms(P.X, n, d, P.dpad, norms, st);
+    log.add();
+  }
+  if (timed) KNN_CK(cudaEventRecord(C->ev[1], st));
+
+  Trees T;
+  rc = run_trees(C, P.X, n, d, P.dpad, trees, leaf, seed, st, &T, log);
+  if (rc) return rc;
+  if (timed) KNN_CK(cudaEventRecord(C->ev[2], st));
+
+  Lists L;
+  rc = get_lists(C, n, k, &L);
+  if (rc) return rc;
+  rc = run_leaf(C, P.X, n, d, P.dpad, k, trees, T.depth, metric, T.perm, norms, &L,
+                stats ? counters : nullptr, st, log);
+  if (rc) return rc;
+  if (timed) KNN_CK(cudaEventRecord(C->ev[3], st));
+
+  for (int p = 0; p < props; ++p) {
+    rc = run_prop(P.X, n, d, P.dpad, k, metric, norms, T.perm, &L, true,
+                  stats ? counters + 2 + p : nullptr, st, log);
+    if (rc) return rc;
+  }
+  if (timed) KNN_CK(cudaEventRecord(C->ev[4], st));
+
+  // Finalise into the caller's buffers (or staging, then copy to the host).
+  float* dd = out_dist;
+  int32_t* di = out_idx;
+  if (!o.outputs_on_device) {
+    rc = C->get("out_dist", (size_t)n * k, &dd);
+    if (!rc) rc = C->get("out_idx", (size_t)n * k, &di);
+    if (rc) return rc;
+  }
+  knn::launch_finalize(L.key[L.cur], L.id[L.cur], n, k, metric, dd, di, st);
+  log.add();
+  if (!o.outputs_on_device) {
+    KNN_CK(cudaMemcpyAsync(out_dist, dd, sizeof(float) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
+    KNN_CK(cudaMemcpyAsync(out_idx, di, sizeof(int32_t) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
+  }
+  if (timed) KNN_CK(cudaEventRecord(C->ev[5], st));
+  KNN_CK(cudaPeekAtLastError());
+
+  const bool async_ok = o.stream && o.outputs_on_device && !stats;
+  if (!async_ok) KNN_CK(cudaStreamSynchronize(st));
+
+  if (stats) {
+    const int32_t sz = stats->struct_size;
+    std::memset(stats, 0, sizeof(knn_stats));
+    stats->struct_size = sz;
+    stats->depth = T.depth;
+    float ms = 0;
+    KNN_CK(cudaEventElapsedTime(&ms, C->ev[0], C->ev[5]));
+    stats->ms_total = ms;
+    KNN_CK(cudaEventElapsedTime(&ms, C->ev[0], C->ev[1]));
+    stats->ms_upload = ms;
+    KNN_CK(cudaEventElapsedTime(&ms, C->ev[1], C->ev[2]));
+    stats->ms_trees = ms;
+    KNN_CK(cudaEventElapsedTime(&ms, C->ev[2], C->ev[3]));
+    stats->ms_leaf = ms;
+    KNN_CK(cudaEventElapsedTime(&ms, C->ev[3], C->ev[4]));
+    stats->ms_propagate = ms;
+    KNN_CK(cudaEventElapsedTime(&ms, C->ev[4], C->ev[5]));
+    stats->ms_download = ms;
+    stats->launches = log.count;
+    stats->props_run = props;
+    unsigned long long host[2 + KNN_MAX_PROPS];
+    KNN_CK(cudaMemcpy(host, counters, sizeof(host), cudaMemcpyDeviceToHost));
+    stats->leaf_pairs = (int64_t)host[0];
+    for (int p = 0; p < props && p < KNN_MAX_PROPS; ++p) stats->prop_candidates[p] = (int64_t)host[2 + p];
+  }
+  return KNN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void knn_default_options(knn_options* opt) {
+  if (!opt) return;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->struct_size = (int32_t)sizeof(knn_options);
+  opt->device = -1;
+  opt->dtype = KNN_F32;
+  opt->precision = KNN_PREC_FP32;
+}
+
+int knn_version(void) { return 100; }
+
+const char* knn_status_string(int status) {
+  switch (status) {
+    case KNN_OK: return "ok";
+    case KNN_ERR_ARGS: return "invalid argument";
+    case KNN_ERR_N_LE_K: return "n must exceed k";
+    case KNN_ERR_OOM: return "out of memory";
+    case KNN_ERR_CUDA: return "CUDA error";
+    case KNN_ERR_TIMEOUT: return "device wait timed out";
+    case KNN_ERR_UNSUPPORTED: return "unsupported request";
+    case KNN_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char* knn_last_error(void) { return g_last_error.c_str(); }
+
+knn_context* knn_context_create(int32_t device) {
+  knn_context* c = nullptr;
+  if (make_context(device, &c)) return nullptr;
+  return c;
+}
+
+void knn_context_destroy(knn_context* ctx) { delete ctx; }
+
+int64_t knn_context_scratch_bytes(const knn_context* ctx) { return ctx ? ctx->bytes_held() : 0; }
+
+int knn_build(const void* points, int64_t n, int32_t d, int32_t k, int32_t trees, int32_t leaf,
+              int32_t props, int32_t metric, uint64_t seed, int32_t* out_idx, float* out_dist) {
+  return knn_build_ex(nullptr, points, n, d, k, trees, leaf, props, metric, seed, out_idx,
+                      out_dist, nullptr, nullptr);
+}
+
+int knn_build_ex(knn_context* ctx, const void* points, int64_t n, int32_t d, int32_t k,
+                 int32_t trees, int32_t leaf, int32_t props, int32_t metric, uint64_t seed,
+                 int32_t* out_idx, float* out_dist, const knn_options* opt, knn_stats* stats) {
+  knn_options o;
+  int rc = resolve_options(opt, &o);
+  if (rc) return rc;
+  rc = check_common(points, n, d, k, metric);
+  if (rc) return rc;
+  if (!out_idx || !out_dist) return fail(KNN_ERR_ARGS, "output pointer is NULL");
+  if (trees < 1 || leaf < 1) return fail(KNN_ERR_ARGS, "trees and leaf must be >= 1");
+  if (props < 0 || props > KNN_MAX_PROPS) return fail(KNN_ERR_ARGS, "props out of range");
+  if (stats && stats->struct_size != (int32_t)sizeof(knn_stats))
+    return fail(KNN_ERR_ARGS, "knn_stats.struct_size mismatch");
+  if (o.precision != KNN_PREC_FP32 || o.learned_splits)
+    return fail(KNN_ERR_UNSUPPORTED, "precision/learned mode not available in this build");
+  rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  return build_impl(ctx, points, n, d, k, trees, leaf, props, metric, seed, out_idx, out_dist, o,
+                    stats);
+}
+
+int knn_build_trees(knn_context* ctx, const float* points, int64_t n, int32_t d, int32_t trees,
+                    int32_t leaf, uint64_t seed, int32_t* out_perm) {
+  if (!points || !out_perm) return fail(KNN_ERR_ARGS, "NULL pointer");
+  if (n < 1 || n >= (int64_t)INT32_MAX || d < 1 || trees < 1 || leaf < 1)
+    return fail(KNN_ERR_ARGS, "size out of range");
+  knn_options o;
+  knn_default_options(&o);
+  int rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  cudaStream_t st = ctx->stream;
+  knn::LaunchLog log;
+  Prepared P;
+  rc = prepare_points(ctx, points, n, d, o, st, &P, log);
+  if (rc) return rc;
+  Trees T;
+  rc = run_trees(ctx, P.X, n, d, P.dpad, trees, leaf, seed, st, &T, log);
+  if (rc) return rc;
+  KNN_CK(cudaMemcpyAsync(out_perm, T.perm, sizeof(int32_t) * (size_t)trees * n, cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaStreamSynchronize(st));
+  return KNN_OK;
+}
+
+int knn_leaf_stage(knn_context* ctx, const float* points, int64_t n, int32_t d, int32_t k,
+                   int32_t trees, int32_t leaf, int32_t metric, const int32_t* perm,
+                   int32_t* out_idx, float* out_key) {
+  int rc = check_common(points, n, d, k, metric);
+  if (rc) return rc;
+  if (!perm || !out_idx || !out_key || trees < 1 || leaf < 1) return fail(KNN_ERR_ARGS, "bad argument");
+  const int depth = knn::tree_depth(n, leaf);
+  if (depth > 30) return fail(KNN_ERR_ARGS, "tree too deep");
+  knn_options o;
+  knn_default_options(&o);
+  rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  cudaStream_t st = ctx->stream;
+  knn::LaunchLog log;
+  Prepared P;
+  rc = prepare_points(ctx, points, n, d, o, st, &P, log);
+  if (rc) return rc;
+  int32_t* dperm = nullptr;
+  rc = ctx->get("perm", (size_t)trees * n, &dperm);
+  if (rc) return rc;
+  KNN_CK(cudaMemcpyAsync(dperm, perm, sizeof(int32_t) * (size_t)trees * n, cudaMemcpyHostToDevice, st));
+  float* norms = nullptr;
+  if (metric == KNN_METRIC_COSINE) {
+    rc = ctx->get("norms", (size_t)n, &norms);
+    if (rc) return rc;
+    knn::launch_norms(P.X, n, d, P.dpad, norms, st);
+  }
+  Lists L;
+  rc = get_lists(ctx, n, k, &L);
+  if (rc) return rc;
+  rc = run_leaf(ctx, P.X, n, d, P.dpad, k, trees, depth, metric, dperm, norms, &L, nullptr, st, log);
+  if (rc) return rc;
+  KNN_CK(cudaMemcpyAsync(out_key, L.key[L.cur], sizeof(float) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
+  int32_t* di = nullptr;
+  rc = ctx->get("out_idx", (size_t)n * k, &di);
+  if (rc) return rc;
+  float* dd = nullptr;
+  rc = ctx->get("out_dist", (size_t)n * k, &dd);
+  if (rc) return rc;
+  knn::launch_finalize(L.key[L.cur], L.id[L.cur], n, k, metric, dd, di, st);
+  KNN_CK(cudaMemcpyAsync(out_idx, di, sizeof(int32_t) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaStreamSynchronize(st));
+  return KNN_OK;
+}
+
+int knn_propagate_step(knn_context* ctx, const float* points, int64_t n, int32_t d, int32_t k,
+                       int32_t metric, const int32_t* idx_in, const float* key_in,
+                       int32_t* idx_out, float* key_out) {
+  int rc = check_common(points, n, d, k, metric);
+  if (rc) return rc;
+  if (!idx_in || !key_in || !idx_out || !key_out) return fail(KNN_ERR_ARGS, "NULL pointer");
+  for (int64_t g = 0; g < n * k; ++g)
+    if (idx_in[g] < 0 || idx_in[g] >= n) return fail(KNN_ERR_ARGS, "neighbour id out of range");
+  knn_options o;
+  knn_default_options(&o);
+  rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  cudaStream_t st = ctx->stream;
+  knn::LaunchLog log;
+  Prepared P;
+  rc = prepare_points(ctx, points, n, d, o, st, &P, log);
+  if (rc) return rc;
+  float* norms = nullptr;
+  if (metric == KNN_METRIC_COSINE) {
+    rc = ctx->get("norms", (size_t)n, &norms);
+    if (rc) return rc;
+    knn::launch_norms(P.X, n, d, P.dpad, norms, st);
+  }
+  Lists L;
+  rc = get_lists(ctx, n, k, &L);
+  if (rc) return rc;
+  KNN_CK(cudaMemcpyAsync(L.key[0], key_in, sizeof(float) * (size_t)n * k, cudaMemcpyHostToDevice, st));
+  KNN_CK(cudaMemcpyAsync(L.id[0], idx_in, sizeof(int32_t) * (size_t)n * k, cudaMemcpyHostToDevice, st));
+  rc = run_prop(P.X, n, d, P.dpad, k, metric, norms, nullptr, &L, false, nullptr, st, log);
+  if (rc) return rc;
+  int32_t* di = nullptr;
+  rc = ctx->get("out_idx", (size_t)n * k, &di);
+  if (rc) return rc;
+  float* dd = nullptr;
+  rc = ctx->get("out_dist", (size_t)n * k, &dd);
+  if (rc) return rc;
+  // ids without flag bits; keys as they are
+  knn::launch_finalize(L.key[L.cur], L.id[L.cur], n, k, KNN_METRIC_TAXICAB, dd, di, st);
+  KNN_CK(cudaMemcpyAsync(key_out, dd, sizeof(float) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaMemcpyAsync(idx_out, di, sizeof(int32_t) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaStreamSynchronize(st));
+  return KNN_OK;
+}
+
+int knn_exact_fp64(knn_context* ctx, const void* points, int64_t n, int32_t d, int32_t k,
+                   int32_t metric, const int64_t* queries, int64_t nq, int32_t* out_idx,
+                   double* out_dist, const knn_options* opt) {
+  knn_options o;
+  int rc = resolve_options(opt, &o);
+  if (rc) return rc;
+  rc = check_common(points, n, d, k, metric);
+  if (rc) return rc;
+  if (!queries || nq < 1 || !out_idx || !out_dist) return fail(KNN_ERR_ARGS, "bad query arguments");
+  for (int64_t q = 0; q < nq; ++q)
+    if (queries[q] < 0 || queries[q] >= n) return fail(KNN_ERR_ARGS, "query id out of range");
+  rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  cudaStream_t st = o.stream ? static_cast<cudaStream_t>(o.stream) : ctx->stream;
+  knn::LaunchLog log;
+  knn_options po = o;
+  po.outputs_on_device = 0;
+  Prepared P;
+  rc = prepare_points(ctx, points, n, d, po, st, &P, log);
+  if (rc) return rc;
+  int dev_sms = 148;
+  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  const int64_t qtiles = (nq + 63) / 64;
+  int slices = (int)((4LL * dev_sms + qtiles - 1) / qtiles);
+  if (slices < 1) slices = 1;
+  if (slices > 64) slices = 64;
+  if ((int64_t)slices > (n + 63) / 64) slices = (int)((n + 63) / 64);
+  int64_t* dq = nullptr;
+  double* norms = nullptr;
+  double* pd = nullptr;
+  uint32_t* pi = nullptr;
+  double* od = nullptr;
+  int32_t* oi = nullptr;
+  rc = ctx->get("ex_q", (size_t)nq, &dq);
+  if (!rc) rc = ctx->get("ex_norms", (size_t)n, &norms);
+  if (!rc) rc = ctx->get("ex_pd", (size_t)slices * nq * k, &pd);
+  if (!rc) rc = ctx->get("ex_pi", (size_t)slices * nq * k, &pi);
+  if (!rc) rc = ctx->get("ex_od", (size_t)nq * k, &od);
+  if (!rc) rc = ctx->get("ex_oi", (size_t)nq * k, &oi);
+  if (rc) return rc;
+  KNN_CK(cudaMemcpyAsync(dq, queries, sizeof(int64_t) * (size_t)nq, cudaMemcpyHostToDevice, st));
+  rc = knn::exact_fp64(P.X, n, d, P.dpad, k, metric, dq, nq, norms, pd, pi, slices, od, oi, st);
+  if (rc) return fail_cuda(cudaGetLastError(), "exact launch");
+  KNN_CK(cudaMemcpyAsync(out_dist, od, sizeof(double) * (size_t)nq * k, cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaMemcpyAsync(out_idx, oi, sizeof(int32_t) * (size_t)nq * k, cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaStreamSynchronize(st));
+  return KNN_OK;
+}
+
+int knn_normalize_reference(float* points, int64_t n, int32_t d) {
+  if (!points || n < 1 || d < 1) return fail(KNN_ERR_ARGS, "bad argument");
+  knn_context* ctx = nullptr;
+  knn_options o;
+  knn_default_options(&o);
+  int rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  float* X = nullptr;
+  rc = ctx->get("norm_X", (size_t)n * d, &X);
+  if (rc) return rc;
+  cudaStream_t st = ctx->stream;
+  KNN_CK(cudaMemcpyAsync(X, points, sizeof(float) * (size_t)n * d, cudaMemcpyHostToDevice, st));
+  knn::launch_normalize_reference(X, n, d, st);
+  KNN_CK(cudaPeekAtLastError());
+  KNN_CK(cudaMemcpyAsync(points, X, sizeof(float) * (size_t)n * d, cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaStreamSynchronize(st));
+  return KNN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,79 @@
+// Host-side launchers of the k-NN graph stages and their argument blocks.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace knn {
+
+// Keys of a node staged in shared memory by k_split when it has at most this
+// many points (96 KB).
+constexpr int kSplitSmemKeys = 12288;
+
+// Counts kernel launches of one call.
+struct LaunchLog {
+  int count = 0;
+  void add(int c = 1) { count += c; }
+};
+
+__global__ void k_iota(int32_t* perm, int64_t n, int trees);
+
+// Points are row-major float32 [n][dpad], dpad % 4 == 0, zero padded, 16-byte
+// aligned rows.
+struct TreeArgs {
+  const float* X;
+  int64_t n;
+  int d, dpad;
+  int trees, depth;
+  uint64_t seed;
+  int32_t* perm;      // [trees][n] out: leaf order
+  int32_t* perm_alt;  // [trees][n] scratch
+  uint64_t* keys;     // [trees][n] scratch
+  float* dirs;        // [trees][2^(depth-1)][dpad] scratch
+  cudaStream_t stream;
+};
+int tree_build(const TreeArgs& a, LaunchLog& log);
+
+struct LeafArgs {
+  const float* X;
+  int64_t n;
+  int d, dpad, k, trees, depth, metric;
+  const int32_t* perm;   // [trees][n]
+  const float* norms;    // [n] (COSINE) or null
+  float* rkey;           // [n][k] in/out, sorted
+  uint32_t* rid;         // [n][k] in/out
+  unsigned long long* pair_counter;  // optional
+  cudaStream_t stream;
+};
+int leaf_stage(const LeafArgs& a, LaunchLog& log);
+
+struct PropArgs {
+  const float* X;
+  int64_t n;
+  int d, dpad, k, metric;
+  const float* norms;
+  const int32_t* order;  // query order (a tree's leaf order) or null
+  const float* key_in;
+  const uint32_t* id_in;
+  const uint32_t* flags_in;  // [n][kw] or null: every entry new
+  float* key_out;
+  uint32_t* id_out;
+  uint32_t* flags_out;       // [n][kw]
+  unsigned long long* cand_counter;  // optional
+  cudaStream_t stream;
+};
+int propagate_step(const PropArgs& a, LaunchLog& log);
+
+// Helpers (knn_misc.cu).
+void launch_init_lists(float* key, uint32_t* id, uint32_t* flags, int64_t n, int k, int kw,
+                       cudaStream_t st);
+void launch_set_flags(uint32_t* flags, int64_t n, int k, int kw, cudaStream_t st);
+void launch_norms(const float* X, int64_t n, int d, int dpad, float* norms, cudaStream_t st);
+void launch_pad_rows(const void* src, int dtype, int64_t n, int d, int64_t ld, float* dst,
+                     int dpad, cudaStream_t st);
+void launch_finalize(const float* key, const uint32_t* id, int64_t n, int k, int metric,
+                     float* out_dist, int32_t* out_idx, cudaStream_t st);
+void launch_keys_from_dist(const float* dist, int64_t count, int metric, float* key,
+                           cudaStream_t st);
+
+}  // namespace knn

@@ -1,0 +1,155 @@
+// Small element-wise kernels around the k-NN stages.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "knn_internal.cuh"
+#include "knn_kernels.cuh"
+
+namespace knn {
+
+// Every list slot empty (+inf, no id), every flag "new".  Plays the role of
+// stubInitializationKernel (euclideandistancematrixgpu.cu:2110-2117), whose
+// stub is (id -1, distance 100000).
+__global__ void k_init_lists(float* key, uint32_t* id, int64_t count) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < count) {
+    key[g] = __int_as_float(0x7F800000);
+    id[g] = kNoId;
+  }
+}
+
+__global__ void k_set_flags(uint32_t* flags, int64_t n, int k, int kw) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < n * kw) {
+    const int w = (int)(g % kw);
+    const int bits = min(32, k - 32 * w);
+    flags[g] = bits >= 32 ? 0xFFFFFFFFu : ((1u << bits) - 1u);
+  }
+}
+
+// |x| in the reference's summation order (used for 1 - cos).
+__global__ void k_norms(const float* __restrict__ X, int64_t n, int d, int dpad, float* __restrict__ norms) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) norms[i] = __fsqrt_rn(self_dot_chunked(X + (size_t)i * dpad, d));
+}
+
+// Rows of any input element type -> zero-padded float32 rows of dpad floats.
+template <typename T>
+__device__ __forceinline__ float to_f32(T v);
+template <>
+__device__ __forceinline__ float to_f32<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ float to_f32<__half>(__half v) { return __half2float(v); }
+template <>
+__device__ __forceinline__ float to_f32<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+template <typename T>
+__global__ void k_pad_rows(const T* __restrict__ src, int64_t n, int d, int64_t ld,
+                           float* __restrict__ dst, int dpad) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n * dpad) return;
+  const int64_t i = g / dpad;
+  const int c = (int)(g - i * dpad);
+  dst[g] = c < d ? to_f32<T>(src[i * ld + c]) : 0.0f;
+}
+
+__global__ void k_finalize(const float* __restrict__ key, const uint32_t* __restrict__ id,
+                           int64_t count, int metric, float* __restrict__ dist,
+                           int32_t* __restrict__ idx) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < count) {
+    const float kv = key[g];
+    dist[g] = metric == KNN_METRIC_EUCLIDEAN ? __fsqrt_rn(kv) : kv;
+    idx[g] = (int32_t)(id[g] & kIdMask);
+  }
+}
+
+__global__ void k_keys_from_dist(const float* __restrict__ dist, int64_t count, int metric,
+                                 float* __restrict__ key) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < count) {
+    const float v = dist[g];
+    key[g] = metric == KNN_METRIC_EUCLIDEAN ? __fmul_rn(v, v) : v;
+  }
+}
+
+static inline unsigned blocks_for(int64_t count, int threads) {
+  return (unsigned)((count + threads - 1) / threads);
+}
+
+void launch_init_lists(float* key, uint32_t* id, uint32_t* flags, int64_t n, int k, int kw,
+                       cudaStream_t st) {
+  k_init_lists<<<blocks_for(n * k, 256), 256, 0, st>>>(key, id, n * k);
+  if (flags) k_set_flags<<<blocks_for(n * kw, 256), 256, 0, st>>>(flags, n, k, kw);
+}
+void launch_set_flags(uint32_t* flags, int64_t n, int k, int kw, cudaStream_t st) {
+  k_set_flags<<<blocks_for(n * kw, 256), 256, 0, st>>>(flags, n, k, kw);
+}
+void launch_norms(const float* X, int64_t n, int d, int dpad, float* norms, cudaStream_t st) {
+  k_norms<<<blocks_for(n, 128), 128, 0, st>>>(X, n, d, dpad, norms);
+}
+void launch_pad_rows(const void* src, int dtype, int64_t n, int d, int64_t ld, float* dst,
+                     int dpad, cudaStream_t st) {
+  const unsigned b = blocks_for(n * dpad, 256);
+  if (dtype == KNN_F16)
+    k_pad_rows<__half><<<b, 256, 0, st>>>(static_cast<const __half*>(src), n, d, ld, dst, dpad);
+  else if (dtype == KNN_BF16)
+    k_pad_rows<__nv_bfloat16><<<b, 256, 0, st>>>(static_cast<const __nv_bfloat16*>(src), n, d, ld, dst, dpad);
+  else
+    k_pad_rows<float><<<b, 256, 0, st>>>(static_cast<const float*>(src), n, d, ld, dst, dpad);
+}
+void launch_finalize(const float* key, const uint32_t* id, int64_t n, int k, int metric,
+                     float* out_dist, int32_t* out_idx, cudaStream_t st) {
+  k_finalize<<<blocks_for(n * k, 256), 256, 0, st>>>(key, id, n * k, metric, out_dist, out_idx);
+}
+void launch_keys_from_dist(const float* dist, int64_t count, int metric, float* key,
+                           cudaStream_t st) {
+  k_keys_from_dist<<<blocks_for(count, 256), 256, 0, st>>>(dist, count, metric, key);
+}
+
+// ------------------------------------------- reference normalisation (CLI) --
+// Step 1 (normalizeDataStep1, euclideandistancematrixgpu.cu:19-42): one thread
+// per dimension sums the column sequentially in float, divides by n and
+// subtracts.  Row-major here, so the column walk is strided.
+__global__ void k_norm_step1(float* X, int64_t n, int d) {
+  const int dim = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dim >= d) return;
+  float mean = 0.0f;
+  for (int64_t i = 0; i < n; ++i) mean = __fadd_rn(mean, X[i * d + dim]);
+  mean = __fdiv_rn(mean, (float)n);
+  for (int64_t i = 0; i < n; ++i) X[i * d + dim] = __fsub_rn(X[i * d + dim], mean);
+}
+// Step 2 (normalizeDataStep2, .cu:44-85): a single 256-thread block; thread t
+// covers dimension t only (the reference's `if` is not a loop), takes the
+// largest |x| of its dimension, thread 0 takes the largest over the 256
+// slots, and dimensions < 256 are divided by it.
+__global__ void k_norm_step2(float* X, int64_t n, int d) {
+  __shared__ float mx[256];
+  __shared__ float mglobal;
+  const int t = threadIdx.x;
+  mx[t] = 0.0f;
+  if (t == 0) mglobal = 0.0f;
+  __syncthreads();
+  if (t < d) {
+    float m = 0.0f;
+    for (int64_t i = 0; i < n; ++i) m = fmaxf(fabsf(X[i * d + t]), m);
+    mx[t] = m;
+  }
+  __syncthreads();
+  if (t == 0) {
+    float g = 0.0f;
+    for (int q = 0; q < 256; ++q) g = fmaxf(g, mx[q]);
+    mglobal = g;
+  }
+  __syncthreads();
+  if (t < d) {
+    const float g = mglobal;
+    for (int64_t i = 0; i < n; ++i) X[i * d + t] = __fdiv_rn(X[i * d + t], g);
+  }
+}
+void launch_normalize_reference(float* X, int64_t n, int d, cudaStream_t st) {
+  k_norm_step1<<<(d + 255) / 256, 256, 0, st>>>(X, n, d);
+  k_norm_step2<<<1, 256, 0, st>>>(X, n, d);
+}
+
+}  // namespace knn

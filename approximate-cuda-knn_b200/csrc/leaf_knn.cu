@@ -1,0 +1,206 @@
+// Initial k-NN over leaf blocks, plain FP32 on CUDA cores.
+//
+// Replaces findGraphTraversalStartPoint + findInitialStateOfAproximated{Euclidean,
+// Taxicab,Cosine}KNN (euclideandistancematrixgpu.cu:87-105, :107-1031).  The
+// reference unions every tree's block of a point in an N-byte bitmap, scans the
+// bitmap per point and selects k with a histogram; here each (tree, leaf) block
+// is one tile job: the block's rows are staged in shared memory 32 dims at a
+// time, every (query, candidate) key of the block is computed by a 4x4 register
+// tile per thread in the reference's summation order, and each query's k best
+// are merged into its running sorted list by one warp (bitonic sort + merge via
+// shuffles).  Taking the k best of every tree in turn and dropping ids already
+// listed gives the k best of the union, so no bitmap is needed.
+//
+// The block of a leaf is its smallest ancestor holding at least k+1 points
+// (the climb of .cu:87-105); all points of a leaf share it.
+#include "knn_internal.cuh"
+#include "knn_kernels.cuh"
+
+namespace knn {
+
+namespace {
+constexpr int kTile = 64;   // queries x candidates per tile
+constexpr int kDC = 32;     // dims staged per chunk
+constexpr int kSP = kTile + 4;
+}  // namespace
+
+template <int METRIC, int KPL>
+__global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d, int dpad,
+                                              int64_t n, int k, int depth,
+                                              const int32_t* __restrict__ perm,
+                                              const float* __restrict__ norms,
+                                              float* __restrict__ rkey, uint32_t* __restrict__ rid,
+                                              unsigned long long* __restrict__ pair_counter) {
+  __shared__ __align__(16) float Qs[kDC][kSP];
+  __shared__ __align__(16) float Cs[kDC][kSP];
+  __shared__ float Ks[kTile][kTile + 1];
+  __shared__ int32_t qid[kTile], cid[kTile];
+  __shared__ float qnorm[kTile], cnorm[kTile];
+
+  const int64_t j = blockIdx.x;
+  const int64_t lo = node_lo(n, depth, j), hi = node_lo(n, depth, j + 1);
+  const int nq = (int)(hi - lo);
+  int bl = depth;
+  int64_t bj = j;
+  while (bl > 0 && node_lo(n, bl, bj + 1) - node_lo(n, bl, bj) < k + 1) {
+    --bl;
+    bj >>= 1;
+  }
+  const int64_t blo = node_lo(n, bl, bj), bhi = node_lo(n, bl, bj + 1);
+  const int nb = (int)(bhi - blo);
+
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int warp = tid >> 5, lane = tid & 31;
+  const float kInf = __int_as_float(0x7F800000);
+  const int nchunks = (d + kDC - 1) / kDC;
+
+  if (pair_counter && tid == 0) atomicAdd(pair_counter, (unsigned long long)nq * (unsigned long long)(nb - 1));
+
+  for (int q0 = 0; q0 < nq; q0 += kTile) {
+    const int mq = min(kTile, nq - q0);
+    if (tid < kTile) {
+      const int32_t id = tid < mq ? perm[lo + q0 + tid] : -1;
+      qid[tid] = id;
+      if (METRIC == KNN_METRIC_COSINE) qnorm[tid] = id >= 0 ? norms[id] : 0.f;
+    }
+    for (int c0 = 0; c0 < nb; c0 += kTile) {
+      const int mc = min(kTile, nb - c0);
+      if (tid < kTile) {
+        const int32_t id = tid < mc ? perm[blo + c0 + tid] : -1;
+        cid[tid] = id;
+        if (METRIC == KNN_METRIC_COSINE) cnorm[tid] = id >= 0 ? norms[id] : 0.f;
+      }
+      __syncthreads();
+
+      float part[4][4], total[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          part[a][b] = 0.f;
+          total[a][b] = 0.f;
+        }
+      for (int ch = 0; ch < nchunks; ++ch) {
+        const int cd = ch * kDC;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int f = tid + h * 256;
+          const int r = f >> 3, c4 = f & 7;
+          const int dim = cd + 4 * c4;
+          float4 qv = make_float4(0.f, 0.f, 0.f, 0.f), cv = qv;
+          if (r < mq && dim < dpad) qv = __ldg(reinterpret_cast<const float4*>(X + (size_t)qid[r] * dpad + dim));
+          if (r < mc && dim < dpad) cv = __ldg(reinterpret_cast<const float4*>(X + (size_t)cid[r] * dpad + dim));
+          Qs[4 * c4 + 0][r] = qv.x;
+          Qs[4 * c4 + 1][r] = qv.y;
+          Qs[4 * c4 + 2][r] = qv.z;
+          Qs[4 * c4 + 3][r] = qv.w;
+          Cs[4 * c4 + 0][r] = cv.x;
+          Cs[4 * c4 + 1][r] = cv.y;
+          Cs[4 * c4 + 2][r] = cv.z;
+          Cs[4 * c4 + 3][r] = cv.w;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int dd = 0; dd < kDC; ++dd) {
+          const float4 a4 = *reinterpret_cast<const float4*>(&Qs[dd][ty * 4]);
+          const float4 b4 = *reinterpret_cast<const float4*>(&Cs[dd][tx * 4]);
+          const float qa[4] = {a4.x, a4.y, a4.z, a4.w};
+          const float cb[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) part[a][b] = acc_step<METRIC>(qa[a], cb[b], part[a][b]);
+        }
+        if (((cd + kDC) & 255) == 0 || ch == nchunks - 1) {
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+              total[a][b] = __fadd_rn(total[a][b], part[a][b]);
+              part[a][b] = 0.f;
+            }
+        }
+        __syncthreads();
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int qq = ty * 4 + a, cc = tx * 4 + b;
+          float key = total[a][b];
+          if (METRIC == KNN_METRIC_COSINE) key = cosine_key(key, qnorm[qq], cnorm[cc]);
+          Ks[qq][cc] = (qq < mq && cc < mc) ? key : kInf;
+        }
+      __syncthreads();
+
+      // Merge every query row of the tile into its running list.
+      for (int qq = warp; qq < mq; qq += 8) {
+        const uint32_t i = (uint32_t)qid[qq];
+        WarpList<KPL> L;
+#pragma unroll
+        for (int r = 0; r < KPL; ++r) {
+          const int e = r * 32 + lane;
+          if (e < k) {
+            L.key[r] = rkey[(size_t)i * k + e];
+            L.id[r] = rid[(size_t)i * k + e];
+          } else {
+            L.key[r] = kInf;
+            L.id[r] = kNoId;
+          }
+        }
+        for (int cb = 0; cb < mc; cb += 32) {
+          const int c = cb + lane;
+          const bool inrange = c < mc;
+          const float ck = inrange ? Ks[qq][c] : kInf;
+          const uint32_t ci = inrange ? (uint32_t)cid[c] : kNoId;
+          float tk;
+          uint32_t ti;
+          warp_list_get(L, k - 1, tk, ti);
+          bool pass = inrange && ci != i && cand_less(ck, ci, tk, ti);
+          if (!__any_sync(0xFFFFFFFFu, pass)) continue;
+          const bool dup = warp_list_contains(L, ci, k);
+          pass = pass && !dup;
+          if (!__any_sync(0xFFFFFFFFu, pass)) continue;
+          warp_list_insert(L, pass ? ck : kInf, pass ? ci : kNoId);
+        }
+#pragma unroll
+        for (int r = 0; r < KPL; ++r) {
+          const int e = r * 32 + lane;
+          if (e < k) {
+            rkey[(size_t)i * k + e] = L.key[r];
+            rid[(size_t)i * k + e] = L.id[r];
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+template <int METRIC>
+static void launch_leaf_metric(const LeafArgs& a, int t, int kpl) {
+  const int64_t leaves = int64_t(1) << a.depth;
+  const int32_t* perm = a.perm + (size_t)t * a.n;
+  dim3 grid((unsigned)leaves);
+  if (kpl == 1)
+    k_leaf<METRIC, 1><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.n, a.k, a.depth, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+  else if (kpl == 2)
+    k_leaf<METRIC, 2><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.n, a.k, a.depth, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+  else
+    k_leaf<METRIC, 4><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.n, a.k, a.depth, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+}
+
+// One launch per tree: a point sits in one leaf per tree, so the leaves of a
+// tree update disjoint lists, and stream order serialises the trees.
+int leaf_stage(const LeafArgs& a, LaunchLog& log) {
+  const int kpl = kpl_for(a.k);
+  for (int t = 0; t < a.trees; ++t) {
+    if (a.metric == KNN_METRIC_EUCLIDEAN) launch_leaf_metric<KNN_METRIC_EUCLIDEAN>(a, t, kpl);
+    else if (a.metric == KNN_METRIC_TAXICAB) launch_leaf_metric<KNN_METRIC_TAXICAB>(a, t, kpl);
+    else launch_leaf_metric<KNN_METRIC_COSINE>(a, t, kpl);
+    log.add();
+  }
+  return cudaPeekAtLastError() == cudaSuccess ? KNN_OK : KNN_ERR_CUDA;
+}
+
+}  // namespace knn

@@ -1,0 +1,296 @@
+// Random-projection tree build, all trees level by level.
+//
+// Replaces buildUpTheTrees + makePartitionOfLeaf0..9
+// (euclideandistancematrixgpu.cu:2130-2405, :2407-2686).  Differences by design:
+//   * a tree is only a permutation of point ids (its leaf order); node j of
+//     level l covers positions [floor(j n / 2^l), floor((j+1) n / 2^l)), so no
+//     node records, no host round trip of the trees (.cu:2642-2655) and no
+//     per-level host sync on a "there was a split" flag (.cu:2602-2604);
+//   * split direction v = x[p2] - x[p1] of two member points (as .cu:2145-2160)
+//     with p1, p2 drawn per node from a counter hash instead of one rand() pair
+//     per level (.cu:2329-2333);
+//   * the split is at the node median of (projection, id) -- a per-node radix
+//     select -- followed by a stable partition, instead of the sign test against
+//     0 (.cu:2160) and the atomicInc scatter (.cu:2205-2260).
+// Every kernel is deterministic; the tree equals the CPU restatement's.
+#include "knn_internal.cuh"
+#include "knn_kernels.cuh"
+
+namespace knn {
+
+// One warp per (tree, node): direction = x[b] - x[a].
+__global__ void k_directions(const float* __restrict__ X, int dpad, int64_t n, int level,
+                             int trees, const int32_t* __restrict__ perm, float* __restrict__ dirs,
+                             uint64_t seed) {
+  const int64_t nodes = int64_t(1) << level;
+  const int64_t gw = (int64_t)(blockIdx.x * (blockDim.x >> 5)) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (gw >= nodes * trees) return;
+  const int t = (int)(gw / nodes);
+  const int64_t j = gw - (int64_t)t * nodes;
+  const int64_t lo = node_lo(n, level, j), hi = node_lo(n, level, j + 1);
+  const int64_t cnt = hi - lo;
+  float4* v4 = reinterpret_cast<float4*>(dirs + (size_t)gw * dpad);
+  const int nc = dpad >> 2;
+  if (cnt < 2) {
+    for (int c = lane; c < nc; c += 32) v4[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+    return;
+  }
+  int64_t p1, p2;
+  pivot_positions(seed, t, level, j, cnt, &p1, &p2);
+  const int32_t a = perm[(size_t)t * n + lo + p1];
+  const int32_t b = perm[(size_t)t * n + lo + p2];
+  const float4* xa = reinterpret_cast<const float4*>(X + (size_t)a * dpad);
+  const float4* xb = reinterpret_cast<const float4*>(X + (size_t)b * dpad);
+  for (int c = lane; c < nc; c += 32) {
+    float4 u = __ldg(xa + c), w = __ldg(xb + c);
+    v4[c] = make_float4(__fsub_rn(w.x, u.x), __fsub_rn(w.y, u.y), __fsub_rn(w.z, u.z),
+                        __fsub_rn(w.w, u.w));
+  }
+}
+
+// Keys of every (tree, position): (orderable projection << 32) | id.
+template <int G>
+__global__ void __launch_bounds__(256) k_project(const float* __restrict__ X, int dpad, int64_t n,
+                                                 int level, int trees,
+                                                 const int32_t* __restrict__ perm,
+                                                 const float* __restrict__ dirs,
+                                                 uint64_t* __restrict__ keys) {
+  const int64_t nodes = int64_t(1) << level;
+  const int64_t total = (int64_t)trees * n;
+  constexpr int PER_WARP = 32 / G;
+  const int lane = threadIdx.x & 31;
+  const int gl = lane % G;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * PER_WARP;
+       base < total; base += warps * PER_WARP) {
+    const int64_t gi = base + lane / G;
+    const bool valid = gi < total;
+    const int64_t g = valid ? gi : total - 1;
+    const int t = (int)(g / n);
+    const int64_t p = g - (int64_t)t * n;
+    const int64_t j = node_of(n, level, p);
+    const int32_t id = perm[g];
+    const float proj = group_project<G>(X + (size_t)id * dpad,
+                                        dirs + ((size_t)t * nodes + j) * dpad, dpad, gl);
+    if (valid && gl == 0) keys[g] = proj_key(proj, (uint32_t)id);
+  }
+}
+
+// ---------------------------------------------------------------- select --
+// rank-th smallest (0-based) of cnt distinct 64-bit keys, MSB-first 8-bit
+// radix select by the whole block.  Keys may live in shared or global memory.
+__device__ uint64_t block_radix_select(const uint64_t* K, int64_t cnt, int64_t rank,
+                                       uint32_t* hist /*256*/, uint64_t* sh /*4*/) {
+  const int tid = threadIdx.x;
+  uint64_t prefix = 0;
+  for (int pass = 0; pass < 8; ++pass) {
+    const int shift = 56 - 8 * pass;
+    for (int b = tid; b < 256; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
+    for (int64_t i = tid; i < cnt; i += blockDim.x) {
+      const uint64_t key = K[i];
+      if (pass == 0 || (key >> (shift + 8)) == (prefix >> (shift + 8)))
+        atomicAdd(&hist[(key >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (tid < 32) {
+      uint32_t h[8];
+      uint32_t s = 0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        h[q] = hist[tid * 8 + q];
+        s += h[q];
+      }
+      uint32_t incl = s;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        uint32_t o = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+        if (tid >= off) incl += o;
+      }
+      int64_t c = (int64_t)(incl - s);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        if (c <= rank && rank < c + (int64_t)h[q]) {
+          sh[0] = (uint64_t)(tid * 8 + q);
+          sh[1] = (uint64_t)c;
+          sh[2] = (uint64_t)h[q];
+        }
+        c += h[q];
+      }
+    }
+    __syncthreads();
+    const uint64_t bin = sh[0];
+    const int64_t below = (int64_t)sh[1];
+    const uint64_t inbin = sh[2];
+    prefix |= bin << shift;
+    rank -= below;
+    if (pass == 7) return prefix;
+    if (inbin == 1) {
+      __syncthreads();
+      for (int64_t i = tid; i < cnt; i += blockDim.x) {
+        const uint64_t key = K[i];
+        if ((key >> shift) == (prefix >> shift)) sh[3] = key;
+      }
+      __syncthreads();
+      return sh[3];
+    }
+    __syncthreads();
+  }
+  return prefix;  // not reached
+}
+
+// Block-wide exclusive scan of one value per thread; returns the exclusive
+// prefix and writes the block total to *total.
+__device__ __forceinline__ int64_t block_excl_scan(int64_t v, int64_t* warp_sums, int64_t* total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int64_t incl = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    int64_t o = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+    if (lane >= off) incl += o;
+  }
+  if (lane == 31) warp_sums[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    int64_t s = lane < nw ? warp_sums[lane] : 0;
+    int64_t si = s;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      int64_t o = __shfl_up_sync(0xFFFFFFFFu, si, off);
+      if (lane >= off) si += o;
+    }
+    if (lane < nw) warp_sums[lane] = si - s;
+    if (lane == 31) warp_sums[32] = si;
+  }
+  __syncthreads();
+  const int64_t r = warp_sums[w] + incl - v;
+  *total = warp_sums[32];
+  __syncthreads();
+  return r;
+}
+
+// One block per (tree, node) of `level`: median select + stable partition of
+// the node's positions into perm_out.  SMEM_KEYS: node keys staged in shared
+// memory (count <= kSplitSmemKeys).
+template <bool SMEM_KEYS>
+__global__ void __launch_bounds__(1024) k_split(int64_t n, int level, const uint64_t* __restrict__ keys,
+                                                const int32_t* __restrict__ perm,
+                                                int32_t* __restrict__ perm_out) {
+  extern __shared__ uint64_t dyn_keys[];
+  __shared__ uint32_t hist[256];
+  __shared__ uint64_t sh[4];
+  __shared__ int64_t warp_sums[33];
+  const int64_t nodes = int64_t(1) << level;
+  const int64_t s = blockIdx.x;
+  const int t = (int)(s / nodes);
+  const int64_t j = s - (int64_t)t * nodes;
+  const int64_t lo = node_lo(n, level, j), hi = node_lo(n, level, j + 1);
+  const int64_t mid = node_lo(n, level + 1, 2 * j + 1);
+  const int64_t cnt = hi - lo, nl = mid - lo;
+  const uint64_t* K = keys + (size_t)t * n + lo;
+  const int32_t* Pin = perm + (size_t)t * n + lo;
+  int32_t* Pout = perm_out + (size_t)t * n + lo;
+  if (cnt < 2 || nl <= 0 || nl >= cnt) {
+    for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) Pout[i] = Pin[i];
+    return;
+  }
+  const uint64_t* KS = K;
+  if (SMEM_KEYS) {
+    for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) dyn_keys[i] = K[i];
+    __syncthreads();
+    KS = dyn_keys;
+  }
+  const uint64_t pivot = block_radix_select(KS, cnt, nl, hist, sh);
+  // Stable partition, ITEMS consecutive positions per thread per tile.
+  constexpr int ITEMS = 4;
+  const int64_t tile = (int64_t)blockDim.x * ITEMS;
+  int64_t left_base = 0;
+  for (int64_t t0 = 0; t0 < cnt; t0 += tile) {
+    const int64_t p0 = t0 + (int64_t)threadIdx.x * ITEMS;
+    bool f[ITEMS];
+    int c = 0;
+#pragma unroll
+    for (int e = 0; e < ITEMS; ++e) {
+      const int64_t p = p0 + e;
+      f[e] = p < cnt && KS[p] < pivot;
+      c += f[e];
+    }
+    int64_t total;
+    int64_t before = block_excl_scan(c, warp_sums, &total) + left_base;
+#pragma unroll
+    for (int e = 0; e < ITEMS; ++e) {
+      const int64_t p = p0 + e;
+      if (p < cnt) {
+        const int64_t dst = f[e] ? before : nl + (p - before);
+        if (dst >= 0 && dst < cnt) Pout[dst] = Pin[p];  // exactly nl keys are below the pivot
+        before += f[e];
+      }
+    }
+    left_base += total;
+  }
+}
+
+// ------------------------------------------------------------------ host --
+int tree_build(const TreeArgs& a, LaunchLog& log) {
+  const int64_t n = a.n;
+  const int depth = a.depth;
+  cudaStream_t st = a.stream;
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+    cudaFuncSetAttribute(k_split<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kSplitSmemKeys * (int)sizeof(uint64_t));
+    attr_set[dev & 63] = true;
+  }
+  // identity order for every tree
+  k_iota<<<(unsigned)((a.trees * n + 255) / 256), 256, 0, st>>>(a.perm, n, a.trees);
+  log.add();
+  int32_t* cur = a.perm;
+  int32_t* alt = a.perm_alt;
+  const int G = proj_group(a.d);
+  for (int l = 0; l < depth; ++l) {
+    const int64_t nodes = int64_t(1) << l;
+    const int64_t segs = nodes * a.trees;
+    k_directions<<<(unsigned)((segs + 7) / 8), 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur,
+                                                             a.dirs, a.seed);
+    const int64_t total = (int64_t)a.trees * n;
+    const int per_block = 8 * (32 / G);
+    int64_t blocks = (total + per_block - 1) / per_block;
+    if (blocks > 148LL * 64) blocks = 148LL * 64;
+    switch (G) {
+      case 1: k_project<1><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur, a.dirs, a.keys); break;
+      case 2: k_project<2><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur, a.dirs, a.keys); break;
+      case 4: k_project<4><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur, a.dirs, a.keys); break;
+      case 8: k_project<8><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur, a.dirs, a.keys); break;
+      case 16: k_project<16><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur, a.dirs, a.keys); break;
+      default: k_project<32><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur, a.dirs, a.keys); break;
+    }
+    const int64_t maxcnt = (n + nodes - 1) / nodes;
+    int threads = (int)((maxcnt + 3) / 4);
+    threads = ((threads + 31) / 32) * 32;
+    if (threads < 64) threads = 64;
+    if (threads > 1024) threads = 1024;
+    if (maxcnt <= kSplitSmemKeys) {
+      k_split<true><<<(unsigned)segs, threads, (size_t)maxcnt * sizeof(uint64_t), st>>>(n, l, a.keys, cur, alt);
+    } else {
+      k_split<false><<<(unsigned)segs, threads, 0, st>>>(n, l, a.keys, cur, alt);
+    }
+    log.add(3);
+    int32_t* tmp = cur;
+    cur = alt;
+    alt = tmp;
+  }
+  if (cur != a.perm) {
+    cudaMemcpyAsync(a.perm, cur, sizeof(int32_t) * (size_t)a.trees * n, cudaMemcpyDeviceToDevice, st);
+  }
+  return cudaPeekAtLastError() == cudaSuccess ? KNN_OK : KNN_ERR_CUDA;
+}
+
+__global__ void k_iota(int32_t* perm, int64_t n, int trees) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < (int64_t)trees * n) perm[g] = (int32_t)(g % n);
+}
+
+}  // namespace knn

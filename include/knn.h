@@ -1,0 +1,184 @@
+/*
+ * knn.h -- C ABI of the B200 approximate k-NN graph builder (libacknn.so).
+ *
+ * The builder replaces the compute span of the reference's class
+ * EuclideanDistanceMatrixGPU (euclideandistancematrixgpu.h:50-63): everything
+ * between the start and the end of calculate() (euclideandistancematrixgpu.cu:2861-2896),
+ * i.e. normalisation-free tree build, initial k-NN and neighbour propagation.
+ * The CLI, the CSV reader and the binary writer of the reference sit above
+ * this ABI (see approximate-cuda-knn_b200/cli/hello.cpp).
+ *
+ * Conventions
+ *   - Every function returns KNN_OK (0) or a negative KNN_ERR_* code; none
+ *     prints, exits, or resets the device (the reference calls cudaDeviceReset
+ *     in initialize/deinitialize, euclideandistancematrixgpu.cu:2775, :2856).
+ *   - The caller owns points and outputs (host or device memory, see
+ *     knn_options).  The library owns its scratch through a knn_context,
+ *     reused across calls.  One context per host thread.
+ *   - Output rows are sorted by (distance, index) ascending.  Distances are
+ *     L2 for EUCLIDEAN, L1 for TAXICAB and 1 - cos for COSINE.
+ *   - Plain-FP32 results are bit-identical to the CPU restatement under
+ *     oracle/ (same trees, same neighbour lists, same distances).
+ */
+#ifndef ACKNN_KNN_H_
+#define ACKNN_KNN_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Metric codes, same values as DISTANCE_EUCLIDEAN / DISTANCE_TAXICAB /
+ * DISTANCE_COSINE (euclideandistancematrixgpu.h:16-18). */
+#define KNN_METRIC_EUCLIDEAN 0
+#define KNN_METRIC_TAXICAB 1
+#define KNN_METRIC_COSINE 2
+
+/* Status codes.  The reference signals failure with a bool `true` and a
+ * message on stdout (cucall.h:12-19); these codes replace both. */
+#define KNN_OK 0
+#define KNN_ERR_ARGS -1        /* a size, pointer or option is invalid        */
+#define KNN_ERR_N_LE_K -2      /* n <= k: fewer than k other points exist       */
+#define KNN_ERR_OOM -3         /* device or pinned allocation failed            */
+#define KNN_ERR_CUDA -4        /* a CUDA call failed; see knn_last_error()      */
+#define KNN_ERR_TIMEOUT -5     /* a bounded device-side wait gave up            */
+#define KNN_ERR_UNSUPPORTED -6 /* valid request this build cannot serve        */
+#define KNN_ERR_NO_DEVICE -7   /* no usable CUDA device                         */
+
+/* Element types of the input points. */
+#define KNN_F32 0
+#define KNN_F16 1
+#define KNN_BF16 2
+
+/* Precision modes of the leaf stage. */
+#define KNN_PREC_FP32 0        /* every key in FP32 CUDA-core arithmetic          */
+#define KNN_PREC_BF16_RERANK 1 /* leaf blocks as BF16 tensor-core tiles in the
+                                  |x|^2+|y|^2-2x.y form, each point's best 2k
+                                  re-ranked with exact FP32 keys                 */
+
+#define KNN_MAX_K 128
+#define KNN_MAX_PROPS 64
+
+typedef struct knn_options {
+  int32_t struct_size;       /* sizeof(knn_options)                                  */
+  int32_t device;            /* CUDA device ordinal; -1: the current device          */
+  int32_t points_on_device;  /* 1: `points` is a device pointer                       */
+  int32_t outputs_on_device; /* 1: out_idx / out_dist are device pointers             */
+  int32_t dtype;             /* KNN_F32 / KNN_F16 / KNN_BF16                           */
+  int32_t precision;         /* KNN_PREC_*                                             */
+  int32_t learned_splits;    /* 1: tree directions from the learned split network     */
+  int32_t timing;            /* 1: record per-stage device times in knn_stats         */
+  int64_t ld;                /* row stride of `points` in elements; 0 means d         */
+  void* stream;              /* cudaStream_t; NULL: the context's own stream          */
+  int32_t reserved[8];
+} knn_options;
+
+typedef struct knn_stats {
+  int32_t struct_size;       /* sizeof(knn_stats)                                      */
+  int32_t depth;             /* levels below the root in every tree                    */
+  float ms_total;            /* device time of the call, first to last launch           */
+  float ms_upload;           /* host->device copy and row padding                      */
+  float ms_trees;            /* tree build                                             */
+  float ms_leaf;             /* initial k-NN over leaf blocks                          */
+  float ms_propagate;        /* all propagation iterations                             */
+  float ms_download;         /* finalisation and device->host copy                     */
+  int32_t launches;          /* kernels launched by the call                           */
+  int32_t props_run;         /* propagation iterations run                             */
+  int64_t leaf_pairs;        /* (query, candidate) keys evaluated by the leaf stage     */
+  int64_t prop_candidates[KNN_MAX_PROPS]; /* keys evaluated per propagation iteration  */
+  float ms_prop_iter[KNN_MAX_PROPS];      /* device time per propagation iteration     */
+  int64_t reserved[8];
+} knn_stats;
+
+typedef struct knn_context knn_context;
+
+/* Fill `opt` with defaults: current device, host pointers, FP32 input, plain
+ * precision, random-projection splits, no timing. */
+void knn_default_options(knn_options* opt);
+
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+int knn_version(void);
+
+/* Text of a status code, and the message of the last failure on this thread. */
+const char* knn_status_string(int status);
+const char* knn_last_error(void);
+
+/* Context owning device scratch, stream and events on `device` (-1: current).
+ * Returns NULL on failure (see knn_last_error). */
+knn_context* knn_context_create(int32_t device);
+void knn_context_destroy(knn_context* ctx);
+/* Bytes of device scratch the context currently holds. */
+int64_t knn_context_scratch_bytes(const knn_context* ctx);
+
+/*
+ * knn_build -- the drop-in call.  Replaces EuclideanDistanceMatrixGPU::initialize
+ * + calculate + the device->host copy of saveResultToResultFile
+ * (euclideandistancematrixgpu.cu:2759-2819, :2861-2896, :2908-2915) for points
+ * already in memory.
+ *   points   host float32 [n][d], row-major
+ *   k        neighbours per point (1..KNN_MAX_K), n must exceed k
+ *   trees    random-projection trees (numberOfTrees, main.cpp:27)
+ *   leaf     maximum points per leaf (minSize / numberOfElemsInLeaf, main.cpp:28)
+ *   props    propagation iterations (numberOfPropagations, main.cpp:29)
+ *   metric   KNN_METRIC_*
+ *   seed     seed of the split choices
+ *   out_idx  host int32 [n][k];  out_dist host float32 [n][k]
+ * Uses a per-thread default context on the current device, plain FP32.
+ */
+int knn_build(const void* points, int64_t n, int32_t d, int32_t k, int32_t trees, int32_t leaf,
+              int32_t props, int32_t metric, uint64_t seed, int32_t* out_idx, float* out_dist);
+
+/* knn_build with an explicit context (NULL: per-thread default), options
+ * (NULL: defaults) and optional statistics (NULL: none). */
+int knn_build_ex(knn_context* ctx, const void* points, int64_t n, int32_t d, int32_t k,
+                 int32_t trees, int32_t leaf, int32_t props, int32_t metric, uint64_t seed,
+                 int32_t* out_idx, float* out_dist, const knn_options* opt, knn_stats* stats);
+
+/*
+ * Stage entry points (host memory in and out), for stage-by-stage checks.
+ *   knn_build_trees   leaf order of every tree: out_perm int32 [trees][n]
+ *                     (replaces buildUpTheTrees, euclideandistancematrixgpu.cu:2407-2686)
+ *   knn_leaf_stage    initial k-NN from given leaf orders; out_key holds keys
+ *                     (squared L2 / L1 / 1-cos), rows sorted
+ *                     (replaces findInitialKNN, euclideandistancematrixgpu.cu:2067-2107)
+ *   knn_propagate_step one Jacobi propagation step on keys
+ *                     (replaces one iteration of propagate, euclideandistancematrixgpu.cu:1937-1977)
+ */
+int knn_build_trees(knn_context* ctx, const float* points, int64_t n, int32_t d, int32_t trees,
+                    int32_t leaf, uint64_t seed, int32_t* out_perm);
+int knn_leaf_stage(knn_context* ctx, const float* points, int64_t n, int32_t d, int32_t k,
+                   int32_t trees, int32_t leaf, int32_t metric, const int32_t* perm,
+                   int32_t* out_idx, float* out_key);
+int knn_propagate_step(knn_context* ctx, const float* points, int64_t n, int32_t d, int32_t k,
+                       int32_t metric, const int32_t* idx_in, const float* key_in,
+                       int32_t* idx_out, float* key_out);
+
+/*
+ * knn_exact_fp64 -- exact k-NN of `nq` query rows against all n points in
+ * FP64 on the GPU (self excluded, ties by index).  The judge of recall and
+ * distance error; no counterpart in the reference.
+ *   points host or device (opt->points_on_device) float32 [n][d]
+ *   queries host int64 [nq] row ids;  out_idx host int32 [nq][k];
+ *   out_dist host float64 [nq][k] (L2 / L1 / 1-cos)
+ */
+int knn_exact_fp64(knn_context* ctx, const void* points, int64_t n, int32_t d, int32_t k,
+                   int32_t metric, const int64_t* queries, int64_t nq, int32_t* out_idx,
+                   double* out_dist, const knn_options* opt);
+
+/*
+ * knn_normalize_reference -- the reference's data normalisation
+ * (normalizeDataStep1/2, euclideandistancematrixgpu.cu:19-85, run by calculate()
+ * at :2869-2875) on host float32 [n][d] in place, on the GPU: subtract the
+ * per-dimension mean, then divide dimensions 0..255 by the largest |x| seen
+ * over dimensions 0..255 (dimensions >= 256 stay centred but unscaled, as in
+ * the reference).  Used by the CLI only; knn_build never normalises.
+ */
+int knn_normalize_reference(float* points, int64_t n, int32_t d);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ACKNN_KNN_H_ */
