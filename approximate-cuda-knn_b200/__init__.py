@@ -117,6 +117,7 @@ EXPORTS = {
     "knn_propagate_step": (ctypes.c_int, [_P, _P, _I64, _I32, _I32, _I32, _P, _P, _P, _P]),
     "knn_exact_fp64": (ctypes.c_int, [_P, _P, _I64, _I32, _I32, _I32, _P, _I64, _P, _P, _P]),
     "knn_normalize_reference": (ctypes.c_int, [_P, _I64, _I32]),
+    "knn_exact_fp64_noalloc": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _P, _I64, _P, _P, _P]),
 }
 
 _lib_handle = None

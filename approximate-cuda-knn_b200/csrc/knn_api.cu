@@ -51,6 +51,10 @@ struct Buffer {
 
 }  // namespace
 
+namespace knn {
+void set_last_error(const std::string& what) { g_last_error = what; }
+}  // namespace knn
+
 struct knn_context {
   int device = 0;
   cudaStream_t stream = nullptr;

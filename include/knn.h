@@ -168,6 +168,27 @@ int knn_exact_fp64(knn_context* ctx, const void* points, int64_t n, int32_t d, i
                    double* out_dist, const knn_options* opt);
 
 /*
+ * knn_exact_fp64_noalloc -- knn_exact_fp64 for callers that cannot allocate
+ * device memory while they run (a process whose device memory is all handed to
+ * its own pool at start-up, or a thread that must not pay the device-wide
+ * synchronisation cudaMalloc/cudaFree may bring).  No counterpart in the
+ * reference.  It allocates nothing: its scratch is one 16 MiB array compiled
+ * into the library, held by every GPU that loads it until the process exits.
+ *   points  device float32 [n][d];  queries device int64 [nq];
+ *   out_idx device int32 [nq][k];  out_dist device float64 [nq][k];
+ *   stream  cudaStream_t (NULL: legacy default stream); the call returns once
+ *           the stream has finished.
+ * Results equal knn_exact_fp64's.  The first call on a device looks up the
+ * scratch address, so make it before any stream capture.  All calls share the
+ * scratch: calls that overlap on the GPU race.  Requests whose scratch exceeds
+ * 16 MiB (about 16 bytes per (query, neighbour) pair, plus 8 bytes per point
+ * for COSINE) return KNN_ERR_ARGS; so does a query id outside [0, n).
+ */
+int knn_exact_fp64_noalloc(const float* points, int64_t n, int32_t d, int32_t k, int32_t metric,
+                           const int64_t* queries, int64_t nq, int32_t* out_idx,
+                           double* out_dist, void* stream);
+
+/*
  * knn_normalize_reference -- the reference's data normalisation
  * (normalizeDataStep1/2, euclideandistancematrixgpu.cu:19-85, run by calculate()
  * at :2869-2875) on host float32 [n][d] in place, on the GPU: subtract the
