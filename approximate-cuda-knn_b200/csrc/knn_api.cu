@@ -284,6 +284,45 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
   return KNN_OK;
 }
 
+// Mixed precision: BF16 tensor-core tiles select each point's best min(2k, 32)
+// approximate candidates over all trees; FP32 re-rank keeps the exact best k.
+int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, int trees,
+                  int depth, int metric, const int32_t* perm, const float* norms, Lists* L,
+                  int* err_flag, cudaStream_t st, knn::LaunchLog& log) {
+  const int kw = (k + 31) / 32;
+  const int kq = k <= 16 ? 2 * k : 32;
+  const int Kp = ((d + 63) / 64) * 64;
+  knn::UmmaLeafArgs a{};
+  a.X = X;
+  a.n = n;
+  a.d = d;
+  a.dpad = dpad;
+  a.k = k;
+  a.kq = kq;
+  a.trees = trees;
+  a.depth = depth;
+  a.metric = metric;
+  a.perm = perm;
+  a.norms = norms;
+  a.err = err_flag;
+  a.stream = st;
+  a.rkey = L->key[L->cur];
+  a.rid = L->id[L->cur];
+  int rc = C->get("Xb", (size_t)n * Kp * 2, &a.Xb);
+  if (!rc) rc = C->get("norms2", (size_t)n, &a.norms2);
+  if (!rc) rc = C->get("akey", (size_t)n * kq, &a.akey);
+  if (!rc) rc = C->get("aid", (size_t)n * kq, &a.aid);
+  if (rc) return rc;
+  knn::launch_init_lists(a.akey, a.aid, nullptr, n, kq, 1, st);
+  log.add();
+  rc = knn::leaf_stage_umma(a, log);
+  if (rc == KNN_ERR_UNSUPPORTED) return fail(rc, "tensor-core leaf stage: unsupported shape");
+  if (rc) return fail_cuda(cudaGetLastError(), "tensor-core leaf stage launch");
+  knn::launch_set_flags(L->flags[L->cur], n, k, kw, st);
+  log.add();
+  return KNN_OK;
+}
+
 int run_prop(const float* X, int64_t n, int d, int dpad, int k, int metric, const float* norms,
              const int32_t* order, Lists* L, bool with_flags, unsigned long long* counter,
              cudaStream_t st, knn::LaunchLog& log) {
@@ -367,8 +406,19 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
   Lists L;
   rc = get_lists(C, n, k, &L);
   if (rc) return rc;
-  rc = run_leaf(C, P.X, n, d, P.dpad, k, trees, T.depth, metric, T.perm, norms, &L,
-                stats ? counters : nullptr, st, log);
+  int* err_flag = nullptr;
+  rc = C->get("err_flag", 1, &err_flag);
+  if (rc) return rc;
+  KNN_CK(cudaMemsetAsync(err_flag, 0, sizeof(int), st));
+  const bool tensor_leaf = o.precision == KNN_PREC_BF16_RERANK && metric != KNN_METRIC_TAXICAB &&
+                           d <= 256 && k <= 32;
+  if (tensor_leaf) {
+    rc = run_leaf_umma(C, P.X, n, d, P.dpad, k, trees, T.depth, metric, T.perm, norms, &L,
+                       err_flag, st, log);
+  } else {
+    rc = run_leaf(C, P.X, n, d, P.dpad, k, trees, T.depth, metric, T.perm, norms, &L,
+                  stats ? counters : nullptr, st, log);
+  }
   if (rc) return rc;
   if (timed) KNN_CK(cudaEventRecord(C->ev[3], st));
 
@@ -397,7 +447,12 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
   KNN_CK(cudaPeekAtLastError());
 
   const bool async_ok = o.stream && o.outputs_on_device && !stats;
-  if (!async_ok) KNN_CK(cudaStreamSynchronize(st));
+  if (!async_ok) {
+    KNN_CK(cudaStreamSynchronize(st));
+    int host_err = 0;
+    KNN_CK(cudaMemcpy(&host_err, err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (host_err) return fail(KNN_ERR_TIMEOUT, "a tensor-core tile wait exceeded its iteration limit");
+  }
 
   if (stats) {
     const int32_t sz = stats->struct_size;
@@ -487,8 +542,7 @@ int knn_build_ex(knn_context* ctx, const void* points, int64_t n, int32_t d, int
   if (props < 0 || props > KNN_MAX_PROPS) return fail(KNN_ERR_ARGS, "props out of range");
   if (stats && stats->struct_size != (int32_t)sizeof(knn_stats))
     return fail(KNN_ERR_ARGS, "knn_stats.struct_size mismatch");
-  if (o.precision != KNN_PREC_FP32 || o.learned_splits)
-    return fail(KNN_ERR_UNSUPPORTED, "precision/learned mode not available in this build");
+  if (o.learned_splits) return fail(KNN_ERR_UNSUPPORTED, "learned splits not available in this build");
   rc = enter_device(&ctx, o);
   if (rc) return rc;
   return build_impl(ctx, points, n, d, k, trees, leaf, props, metric, seed, out_idx, out_dist, o,

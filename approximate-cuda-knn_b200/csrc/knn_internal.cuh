@@ -234,6 +234,56 @@ __device__ __forceinline__ void warp_list_insert(WarpList<KPL, K>& L, K ck, uint
   for (int r = KPL - 2; r >= 0; --r) warp_merge_pair(L.key[r], L.id[r], L.key[r + 1], L.id[r + 1]);
 }
 
+// Insert one warp-uniform candidate: entries from its rank on shift down one
+// slot and the last entry drops out.  ~10 instructions per register.
+template <int KPL, typename K>
+__device__ __forceinline__ void warp_list_insert_one(WarpList<KPL, K>& L, K ck, uint32_t ci) {
+  const int lane = threadIdx.x & 31;
+  int pos = 0;
+#pragma unroll
+  for (int r = 0; r < KPL; ++r) pos += __popc(__ballot_sync(0xFFFFFFFFu, cand_less(L.key[r], L.id[r], ck, ci)));
+#pragma unroll
+  for (int r = KPL - 1; r >= 0; --r) {
+    K up_k = __shfl_up_sync(0xFFFFFFFFu, L.key[r], 1);
+    uint32_t up_i = __shfl_up_sync(0xFFFFFFFFu, L.id[r], 1);
+    if (r > 0) {
+      const K pk = __shfl_sync(0xFFFFFFFFu, L.key[r - 1], 31);
+      const uint32_t pi = __shfl_sync(0xFFFFFFFFu, L.id[r - 1], 31);
+      if (lane == 0) {
+        up_k = pk;
+        up_i = pi;
+      }
+    }
+    const int e = r * 32 + lane;
+    if (e > pos) {
+      L.key[r] = up_k;
+      L.id[r] = up_i;
+    } else if (e == pos) {
+      L.key[r] = ck;
+      L.id[r] = ci;
+    }
+  }
+}
+
+// Insert the candidates of the lanes in `bal` (one per lane): one at a time
+// when there are few, else by bitonic sort + merge.
+template <int KPL, typename K>
+__device__ __forceinline__ void warp_list_insert_lanes(WarpList<KPL, K>& L, uint32_t bal, K ck,
+                                                       uint32_t ci, K inf_key) {
+  if (__popc(bal) <= 3) {
+    while (bal) {
+      const int src = __ffs(bal) - 1;
+      bal &= bal - 1;
+      const K k1 = __shfl_sync(0xFFFFFFFFu, ck, src);
+      const uint32_t i1 = __shfl_sync(0xFFFFFFFFu, ci, src);
+      warp_list_insert_one(L, k1, i1);
+    }
+  } else {
+    const bool mine = (bal >> (threadIdx.x & 31)) & 1u;
+    warp_list_insert(L, mine ? ck : inf_key, mine ? ci : kNoId);
+  }
+}
+
 // Entry e of the list (broadcast to all lanes).
 template <int KPL, typename K>
 __device__ __forceinline__ void warp_list_get(const WarpList<KPL, K>& L, int e, K& k, uint32_t& id) {

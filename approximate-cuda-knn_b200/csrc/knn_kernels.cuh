@@ -47,6 +47,24 @@ struct LeafArgs {
 };
 int leaf_stage(const LeafArgs& a, LaunchLog& log);
 
+// Mixed-precision leaf stage (BF16 tensor-core tiles + FP32 re-rank).
+struct UmmaLeafArgs {
+  const float* X;        // padded float32 rows
+  int64_t n;
+  int d, dpad, k, kq, trees, depth, metric;
+  const int32_t* perm;   // [trees][n]
+  const float* norms;    // [n] FP32 norms (COSINE) or null
+  void* Xb;              // [n][Kp] bf16 scratch (Kp = d rounded up to 64)
+  float* norms2;         // [n] scratch
+  float* akey;           // [n][kq] approximate lists (in: empty)
+  uint32_t* aid;
+  float* rkey;           // [n][k] out: exact keys, sorted
+  uint32_t* rid;
+  int* err;              // set when a bounded wait expires
+  cudaStream_t stream;
+};
+int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log);
+
 struct PropArgs {
   const float* X;
   int64_t n;

@@ -1,0 +1,432 @@
+// Initial k-NN over leaf blocks on the 5th-generation tensor cores (tcgen05),
+// for EUCLIDEAN and COSINE: the mixed-precision leaf stage.
+//
+// Same blocks and same union-over-trees rule as the FP32 leaf stage (which
+// replaces findInitialStateOfAproximated*KNN, euclideandistancematrixgpu.cu:107-1031),
+// but every (query, candidate) key of a block comes from one BF16 GEMM tile:
+//     key ~= |x|^2 + |y|^2 - 2 x.y      (EUCLIDEAN, norms of the BF16 rows)
+//     key ~= 1 - x.y                     (COSINE, rows normalised before rounding)
+// with FP32 accumulation in tensor memory.  Each point keeps its best kq (2k,
+// at most 32) approximate candidates over all trees; k_rerank then recomputes
+// those kq keys exactly in FP32 (the reference's order) and keeps the best k.
+// When the BF16 products and FP32 sums are exact (integer data below 2^8 per
+// coordinate and 2^24 per sum, e.g. the integer-mixture workload) the result
+// equals the FP32 leaf stage bit for bit.
+//
+// Tile: 128 queries x 128 candidates x Kp (Kp = d rounded up to 64, <= 256).
+//   * operands: K-major, 128-byte swizzled shared-memory tiles (8-row atoms of
+//     1024 B), filled by cp.async from the BF16 copy through the tree's order;
+//   * MMA: tcgen05.mma.cta_group::1.kind::f16, M=128 N=128 K=16, issued by one
+//     thread, accumulator 128 lanes x 128 columns of tensor memory;
+//   * completion: tcgen05.commit -> mbarrier, waited with an iteration limit
+//     (on expiry the block records an error, drains, frees TMEM and returns);
+//   * epilogue: tcgen05.ld 32x32b.x32 by all 8 warps (warp w reads lane quarter
+//     w%4, column half w/4), keys to shared memory, then one warp per query
+//     row merges the row into that query's list in global memory.
+#include <cuda_bf16.h>
+
+#include "knn_internal.cuh"
+#include "knn_kernels.cuh"
+
+namespace knn {
+
+namespace {
+constexpr int kBM = 128;
+constexpr int kBN = 128;
+constexpr int kKC = 64;               // bf16 per 128-byte swizzled row
+constexpr int kChunkBytes = kBM * 128; // one 128 x 64 bf16 operand chunk
+constexpr uint32_t kTmemCols = 128;
+constexpr int kUThreads = 256;
+constexpr int kQPerWarp = kBM / (kUThreads / 32);  // 16
+constexpr int kKsStride = kBN + 1;
+// A 128x128x256 tile finishes in about a microsecond; 2^16 polls with 32 ns
+// sleeps (a few ms) is far beyond that, and keeps a failing launch short.
+constexpr uint32_t kSpinLimit = 1u << 16;
+
+// Instruction descriptor: D f32 (bits 4-5 = 1), A bf16 (7-9 = 1), B bf16
+// (10-12 = 1), A and B K-major (15, 16 = 0), N>>3 at 17-22, M>>4 at 24-28.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kBN >> 3) << 17) |
+                            ((uint32_t)(kBM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor, K-major, 128-byte swizzle: start address
+// (>>4) in bits 0-13, leading offset 1 (unused for swizzled K-major) at 16-29,
+// stride 1024 B (>>4 = 64) between 8-row atoms at 32-45, version 1 at 46-47,
+// base offset 0, layout type 2 (SWIZZLE_128B) at 61-63.
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)64 << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count));
+}
+
+// Non-blocking test of phase completion.  (try_wait may suspend the thread for
+// a system-dependent time per call, so counting try_wait calls bounds nothing;
+// test_wait never suspends.)
+__device__ __forceinline__ bool mbar_test_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for the phase with the given parity; false once kWaitNs of wall time
+// (globaltimer) have passed.
+constexpr uint64_t kWaitNs = 20ull * 1000 * 1000;  // 20 ms; a tile takes ~1 us
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0; it < kSpinLimit; ++it) {
+    if (mbar_test_wait(bar, parity)) return true;
+    if (it > 64) {
+      __nanosleep(256);
+      if (global_ns() - t0 > kWaitNs) return false;
+    }
+  }
+  return false;
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+        "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+        "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+// Stage `rows` gathered rows (ids in `ids`, <0: zero row) of the BF16 copy into
+// a K-major 128B-swizzled operand of Kp/64 chunks.
+__device__ __forceinline__ void stage_operand(unsigned char* op, const __nv_bfloat16* __restrict__ Xb,
+                                              int Kp, const int32_t* ids) {
+  const int units = kBM * (Kp / 8);  // 16-byte units
+  const uint32_t base = smem_u32(op);
+  for (int u = threadIdx.x; u < units; u += kUThreads) {
+    const int r = u / (Kp / 8);
+    const int c16 = u - r * (Kp / 8);  // 16-byte unit along K
+    const int chunk = c16 >> 3, w = c16 & 7;
+    const uint32_t dst = base + chunk * kChunkBytes + r * 128 + ((w ^ (r & 7)) << 4);
+    const int32_t id = ids[r];
+    const __nv_bfloat16* src = Xb + (size_t)(id < 0 ? 0 : id) * Kp + c16 * 8;
+    cp_async16(dst, src, id < 0 ? 0 : 16);
+  }
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+
+}  // namespace
+
+// One block per (leaf, 128-query tile).  Prologue, MMA issue, bounded wait and
+// tensor-memory epilogue follow the single-tile sequence checked on its own
+// against a CPU product; the per-row merge is the FP32 leaf kernel's (each
+// query's list is read, merged with the tile row and written back).
+template <int METRIC>
+__global__ void __launch_bounds__(kUThreads, 1)
+    k_leaf_tc(const __nv_bfloat16* __restrict__ Xb, int Kp, int64_t n, int k, int kq, int depth,
+              int qtiles, const int32_t* __restrict__ perm, const float* __restrict__ norms2,
+              float* __restrict__ akey, uint32_t* __restrict__ aid, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int nchunks = Kp / kKC;
+  unsigned char* opA = smem;
+  unsigned char* opB = opA + nchunks * kChunkBytes;
+  float* Ks = reinterpret_cast<float*>(opB + nchunks * kChunkBytes);
+  int32_t* qid = reinterpret_cast<int32_t*>(Ks + kBM * kKsStride);
+  int32_t* cid = qid + kBM;
+  float* qn = reinterpret_cast<float*>(cid + kBN);
+  float* cn = qn + kBM;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(cn + kBN);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+  int* status = reinterpret_cast<int*>(tmem_slot + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t leaf = blockIdx.x / qtiles;
+  const int qt = (int)(blockIdx.x - leaf * qtiles);
+  const int64_t lo = node_lo(n, depth, leaf), hi = node_lo(n, depth, leaf + 1);
+  const int nq = (int)(hi - lo);
+  const int q0 = qt * kBM;
+  if (q0 >= nq) return;  // whole block, before any barrier or allocation
+  const int mq = min(kBM, nq - q0);
+  int bl = depth;
+  int64_t bj = leaf;
+  while (bl > 0 && node_lo(n, bl, bj + 1) - node_lo(n, bl, bj) < k + 1) {
+    --bl;
+    bj >>= 1;
+  }
+  const int64_t blo = node_lo(n, bl, bj), bhi = node_lo(n, bl, bj + 1);
+  const int nb = (int)(bhi - blo);
+  const float kInf = __int_as_float(0x7F800000);
+  const uint32_t bar = smem_u32(mbar);
+
+  if (warp == 0) {
+    if (lane == 0) {
+      mbar_init(bar, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+      *status = 0;
+    }
+    __syncwarp();
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid < kBM) {
+    const int32_t id = tid < mq ? perm[lo + q0 + tid] : -1;
+    qid[tid] = id;
+    qn[tid] = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
+  }
+  __syncthreads();
+  stage_operand(opA, Xb, Kp, qid);
+
+  uint32_t phase = 0;
+  for (int c0 = 0; c0 < nb; c0 += kBN) {
+    const int mc = min(kBN, nb - c0);
+    if (tid < kBN) {
+      const int32_t id = tid < mc ? perm[blo + c0 + tid] : -1;
+      cid[tid] = id;
+      cn[tid] = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
+    }
+    __syncthreads();
+    stage_operand(opB, Xb, Kp, cid);
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    if (tid == 0) {
+      if (*reinterpret_cast<volatile int*>(err) != 0) {
+        *status = 2;  // another block failed: issue nothing more
+      } else {
+        const uint32_t a0 = smem_u32(opA), b0 = smem_u32(opB);
+        for (int ch = 0; ch < nchunks; ++ch)
+#pragma unroll
+          for (int kk = 0; kk < kKC / 16; ++kk) {
+            const uint32_t off = ch * kChunkBytes + kk * 32;
+            umma_bf16(tmem, desc_sw128(a0 + off), desc_sw128(b0 + off), (ch | kk) != 0 ? 1u : 0u);
+          }
+        umma_commit(bar);
+        if (!mbar_wait_bounded(bar, phase)) {
+          *status = 1;
+          atomicExch(err, 1);
+          mbar_wait_bounded(bar, phase);  // let the MMAs drain before TMEM is freed
+        }
+      }
+    }
+    __syncthreads();
+    phase ^= 1u;
+    const int stat = *status;
+    if (stat != 0) break;  // uniform: read after the barrier
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    {
+      const int quarter = warp & 3, half = warp >> 2;
+      const int r = quarter * 32 + lane;
+      const bool rv = r < mq;
+      const int32_t myid = qid[r];
+      const float myn = qn[r];
+#pragma unroll 1
+      for (int cc = 0; cc < 2; ++cc) {
+        const int col0 = half * 64 + cc * 32;
+        uint32_t v[32];
+        tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)col0, v);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int c = col0 + j;
+          const float dot = __uint_as_float(v[j]);
+          const float key = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[c]))
+                                                           : __fsub_rn(1.f, dot);
+          Ks[r * kKsStride + c] = (rv && c < mc && cid[c] != myid) ? key : kInf;
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    // merge each query row of the tile into that query's list
+    for (int qq = warp; qq < mq; qq += kUThreads / 32) {
+      const uint32_t i = (uint32_t)qid[qq];
+      WarpList<1> L;
+      L.key[0] = lane < kq ? akey[(size_t)i * kq + lane] : kInf;
+      L.id[0] = lane < kq ? aid[(size_t)i * kq + lane] : kNoId;
+      for (int cb = 0; cb < mc; cb += 32) {
+        const int c = cb + lane;
+        const bool inrange = c < mc;
+        const float ck = inrange ? Ks[qq * kKsStride + c] : kInf;
+        const uint32_t ci = inrange ? (uint32_t)cid[c] : kNoId;
+        float tk;
+        uint32_t ti;
+        warp_list_get(L, kq - 1, tk, ti);
+        bool pass = inrange && ck < kInf && cand_less(ck, ci, tk, ti);
+        if (!__any_sync(0xFFFFFFFFu, pass)) continue;
+        const bool dup = warp_list_contains(L, ci, kq);
+        pass = pass && !dup;
+        if (!__any_sync(0xFFFFFFFFu, pass)) continue;
+        warp_list_insert(L, pass ? ck : kInf, pass ? ci : kNoId);
+      }
+      if (lane < kq) {
+        akey[(size_t)i * kq + lane] = L.key[0];
+        aid[(size_t)i * kq + lane] = L.id[0];
+      }
+    }
+    __syncthreads();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    __syncwarp();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(*tmem_slot), "r"(kTmemCols));
+  }
+}
+
+// BF16 operand copy: rows of Kp bf16 (zero padded), COSINE rows divided by
+// their FP32 norm first; norms2 = |row|^2 of the BF16 values (EUCLIDEAN).
+__global__ void k_to_bf16(const float* __restrict__ X, int64_t n, int d, int dpad, int Kp, int metric,
+                          const float* __restrict__ norms, __nv_bfloat16* __restrict__ Xb,
+                          float* __restrict__ norms2) {
+  const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  float scale = 1.f;
+  if (metric == KNN_METRIC_COSINE) {
+    const float nr = norms[row];
+    scale = nr > 0.f ? __frcp_rn(nr) : 0.f;
+  }
+  float s = 0.f;
+  for (int c = lane; c < Kp; c += 32) {
+    const float v = c < d ? X[(size_t)row * dpad + c] : 0.f;
+    const __nv_bfloat16 b = __float2bfloat16_rn(metric == KNN_METRIC_COSINE ? __fmul_rn(v, scale) : v);
+    Xb[(size_t)row * Kp + c] = b;
+    const float f = __bfloat162float(b);
+    s = __fmaf_rn(f, f, s);
+  }
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) s = __fadd_rn(s, __shfl_xor_sync(0xFFFFFFFFu, s, off));
+  if (lane == 0) norms2[row] = s;
+}
+
+// Exact FP32 keys (the reference's order) of each point's kq approximate
+// candidates; the best k become the list, all flagged new.  One warp per point.
+template <int METRIC>
+__global__ void __launch_bounds__(256) k_rerank(const float* __restrict__ X, int64_t n, int d, int dpad,
+                                                int k, int kq, const float* __restrict__ norms,
+                                                const uint32_t* __restrict__ aid,
+                                                float* __restrict__ rkey, uint32_t* __restrict__ rid) {
+  extern __shared__ __align__(16) float rsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+  float* xq = rsm + (size_t)warp * (dpad + 32 * 65);
+  float* rows = xq + dpad;
+  if (i >= n) return;
+  const float kInf = __int_as_float(0x7F800000);
+  for (int c = lane; c < dpad; c += 32) xq[c] = X[(size_t)i * dpad + c];
+  const uint32_t cj = lane < kq ? aid[(size_t)i * kq + lane] : kNoId;
+  const bool valid = cj != kNoId;
+  float total = 0.f, part = 0.f;
+  for (int cd = 0; cd < d; cd += 64) {
+    __syncwarp();
+    // stage 32 rows x 64 dims, padded stride 65 (conflict-free per-lane reads)
+    for (int r = 0; r < 32; ++r) {
+      const uint32_t id = __shfl_sync(0xFFFFFFFFu, cj, r);
+      for (int c = lane; c < 64; c += 32) {
+        const int dim = cd + c;
+        rows[r * 65 + c] = (id != kNoId && dim < dpad) ? X[(size_t)id * dpad + dim] : 0.f;
+      }
+    }
+    __syncwarp();
+    const int lim = min(64, d - cd);
+    for (int c = 0; c < lim; ++c) part = acc_step<METRIC>(xq[cd + c], rows[lane * 65 + c], part);
+    if (((cd + 64) & 255) == 0 || cd + 64 >= d) {
+      total = __fadd_rn(total, part);
+      part = 0.f;
+    }
+  }
+  float key = total;
+  if (METRIC == KNN_METRIC_COSINE) key = valid ? cosine_key(total, norms[i], norms[cj]) : kInf;
+  if (!valid) key = kInf;
+  float kk = key;
+  uint32_t ii = valid ? cj : kNoId;
+  warp_bitonic_sort32(kk, ii);
+  if (lane < k) {
+    rkey[(size_t)i * k + lane] = kk;
+    rid[(size_t)i * k + lane] = ii;
+  }
+}
+
+size_t umma_smem_bytes(int Kp) {
+  return 1024 + 2 * (size_t)(Kp / kKC) * kChunkBytes + (size_t)kBM * kKsStride * 4 +
+         (size_t)(kBM + kBN) * 8 + 64;
+}
+
+int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
+  const int Kp = ((a.d + kKC - 1) / kKC) * kKC;
+  if (Kp > 256 || a.kq > 32 || a.kq < a.k) return KNN_ERR_UNSUPPORTED;
+  cudaStream_t st = a.stream;
+  __nv_bfloat16* Xb = static_cast<__nv_bfloat16*>(a.Xb);
+  // operand copy
+  k_to_bf16<<<(unsigned)((a.n * 32 + 255) / 256), 256, 0, st>>>(a.X, a.n, a.d, a.dpad, Kp, a.metric,
+                                                                 a.norms, Xb, a.norms2);
+  log.add();
+  const size_t smem = umma_smem_bytes(Kp);
+  const int64_t leaves = int64_t(1) << a.depth;
+  const int64_t maxleaf = (a.n + leaves - 1) / leaves;
+  const int qtiles = (int)((maxleaf + kBM - 1) / kBM);
+  for (int t = 0; t < a.trees; ++t) {
+    const int32_t* perm = a.perm + (size_t)t * a.n;
+    if (a.metric == KNN_METRIC_EUCLIDEAN) {
+      cudaFuncSetAttribute(k_leaf_tc<KNN_METRIC_EUCLIDEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_leaf_tc<KNN_METRIC_EUCLIDEAN><<<(unsigned)(leaves * qtiles), kUThreads, smem, st>>>(
+          Xb, Kp, a.n, a.k, a.kq, a.depth, qtiles, perm, a.norms2, a.akey, a.aid, a.err);
+    } else {
+      cudaFuncSetAttribute(k_leaf_tc<KNN_METRIC_COSINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_leaf_tc<KNN_METRIC_COSINE><<<(unsigned)(leaves * qtiles), kUThreads, smem, st>>>(
+          Xb, Kp, a.n, a.k, a.kq, a.depth, qtiles, perm, a.norms2, a.akey, a.aid, a.err);
+    }
+    log.add();
+  }
+  const size_t rsm = (size_t)8 * (a.dpad + 32 * 65) * sizeof(float);
+  const unsigned rgrid = (unsigned)((a.n + 7) / 8);
+  if (a.metric == KNN_METRIC_EUCLIDEAN) {
+    cudaFuncSetAttribute(k_rerank<KNN_METRIC_EUCLIDEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm);
+    k_rerank<KNN_METRIC_EUCLIDEAN><<<rgrid, 256, rsm, st>>>(a.X, a.n, a.d, a.dpad, a.k, a.kq, a.norms, a.aid, a.rkey, a.rid);
+  } else {
+    cudaFuncSetAttribute(k_rerank<KNN_METRIC_COSINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm);
+    k_rerank<KNN_METRIC_COSINE><<<rgrid, 256, rsm, st>>>(a.X, a.n, a.d, a.dpad, a.k, a.kq, a.norms, a.aid, a.rkey, a.rid);
+  }
+  log.add();
+  return cudaPeekAtLastError() == cudaSuccess ? KNN_OK : KNN_ERR_CUDA;
+}
+
+}  // namespace knn

@@ -1,0 +1,79 @@
+"""Mixed-precision leaf stage (BF16 tcgen05 tiles + FP32 re-rank of the best
+min(2k, 32) candidates) against the plain FP32 path and the oracle.
+
+* Integer coordinates in [0, 255] with d * 255^2 < 2^24: every BF16 product and
+  FP32 sum of |x|^2 + |y|^2 - 2 x.y is exact, so the mixed path must return the
+  plain path's graph bit for bit (which is the oracle's).
+* Float data: every returned distance is the exact FP32 key of its pair (the
+  re-rank), and recall against the FP64 exact graph stays within 0.02 of the
+  plain path's."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import load_package, recall_at_k
+
+pytestmark = pytest.mark.gpu
+
+
+def _ints(n, d, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    centres = rng.uniform(0, 255, size=(12, d))
+    x = centres[rng.integers(0, 12, n)] + rng.normal(0, 20, size=(n, d))
+    return np.clip(np.rint(x), 0, 255).astype(np.float32)
+
+
+@pytest.fixture(scope="module")
+def lib():
+    acknn = load_package()
+    acknn.load_library()
+    return acknn
+
+
+@pytest.mark.parametrize("n,d,k,trees,leaf,props", [
+    (20000, 128, 16, 4, 64, 0),
+    (20000, 128, 16, 4, 64, 2),
+    (30000, 128, 16, 3, 512, 1),
+    (9000, 200, 10, 2, 300, 1),     # Kp = 256, three 128-query tiles per leaf
+    (5000, 64, 8, 3, 40, 1),        # Kp = 64, short blocks
+    (4000, 96, 24, 2, 130, 1),      # kq = 32 for k > 16
+])
+def test_mixed_equals_plain_on_exact_integer_data(lib, oracle, n, d, k, trees, leaf, props):
+    x = _ints(n, d, n + d)
+    mi, md = lib.knn_build(x, k, trees, leaf, props, 0, seed=4, precision=lib.PREC_BF16_RERANK)
+    pi, pd = lib.knn_build(x, k, trees, leaf, props, 0, seed=4)
+    np.testing.assert_array_equal(mi, pi)
+    np.testing.assert_array_equal(md.view(np.uint32), pd.view(np.uint32))
+    oi, od = oracle.knn_build(x, k, trees, leaf, props, 0, seed=4)
+    np.testing.assert_array_equal(mi, oi)
+
+
+@pytest.mark.parametrize("metric", [0, 2])
+def test_mixed_float_data_exact_keys_and_recall(lib, oracle, metric):
+    n, d, k = 12000, 48, 10
+    x = lib.workloads.gaussian_mixture(n, d, 20, seed=7)
+    mi, md = lib.knn_build(x, k, 6, 200, 2, metric, seed=1, precision=lib.PREC_BF16_RERANK)
+    pi, pd = lib.knn_build(x, k, 6, 200, 2, metric, seed=1)
+    # sorted rows, no self, unique neighbours
+    assert np.all(np.diff(md, axis=1) >= 0)
+    assert not np.any(mi == np.arange(n)[:, None])
+    # returned distances are the exact FP32 keys of their pairs
+    for i in range(0, n, 997):
+        for s in range(k):
+            key = oracle.pair_key(x[i], x[mi[i, s]], metric)
+            want = np.sqrt(np.float32(key)) if metric == 0 else np.float32(key)
+            assert md[i, s] == want
+    q = np.arange(0, n, 5)
+    ei, _ = oracle.exact(x, k, q, metric)
+    rm = recall_at_k(mi[q], ei)
+    rp = recall_at_k(pi[q], ei)
+    assert rm >= rp - 0.02, (rm, rp)
+
+
+def test_taxicab_request_falls_back_to_fp32(lib):
+    x = _ints(3000, 32, 3)
+    a = lib.knn_build(x, 6, 2, 40, 1, 1, precision=lib.PREC_BF16_RERANK)
+    b = lib.knn_build(x, 6, 2, 40, 1, 1)
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
