@@ -234,6 +234,27 @@ __device__ __forceinline__ void warp_list_insert(WarpList<KPL, K>& L, K ck, uint
   for (int r = KPL - 2; r >= 0; --r) warp_merge_pair(L.key[r], L.id[r], L.key[r + 1], L.id[r + 1]);
 }
 
+// One-register list (32 entries, ascending across lanes): insert the
+// warp-uniform candidate (c, i).  The lanes whose entry is greater than the
+// candidate form a suffix; its first lane takes the candidate, the suffix
+// shifts up one lane and lane 31's entry drops out.
+__device__ __forceinline__ void warp_insert1(float& lk, uint32_t& li, float c, uint32_t i) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t after = __ballot_sync(0xFFFFFFFFu, cand_less(c, i, lk, li));
+  const float uk = __shfl_up_sync(0xFFFFFFFFu, lk, 1);
+  const uint32_t ui = __shfl_up_sync(0xFFFFFFFFu, li, 1);
+  if (after) {
+    const int pos = __ffs(after) - 1;
+    if (lane > pos) {
+      lk = uk;
+      li = ui;
+    } else if (lane == pos) {
+      lk = c;
+      li = i;
+    }
+  }
+}
+
 // Insert one warp-uniform candidate: entries from its rank on shift down one
 // slot and the last entry drops out.  ~10 instructions per register.
 template <int KPL, typename K>

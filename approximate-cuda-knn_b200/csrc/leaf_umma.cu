@@ -20,9 +20,11 @@
 //     thread, accumulator 128 lanes x 128 columns of tensor memory;
 //   * completion: tcgen05.commit -> mbarrier, waited with an iteration limit
 //     (on expiry the block records an error, drains, frees TMEM and returns);
-//   * epilogue: tcgen05.ld 32x32b.x32 by all 8 warps (warp w reads lane quarter
-//     w%4, column half w/4), keys to shared memory, then one warp per query
-//     row merges the row into that query's list in global memory.
+//   * epilogue: per 64-column round, tcgen05.ld 32x32b.x32 by all 8 warps (warp
+//     w reads lane quarter w%4, 32 columns), keys filtered against each row's
+//     current last entry, then one warp per row inserts the row's few
+//     survivors into that query's sorted list (held in shared memory for the
+//     whole block) with one ballot and one lane shift each.
 #include <cuda_bf16.h>
 
 #include "knn_internal.cuh"
@@ -37,8 +39,9 @@ constexpr int kKC = 64;               // bf16 per 128-byte swizzled row
 constexpr int kChunkBytes = kBM * 128; // one 128 x 64 bf16 operand chunk
 constexpr uint32_t kTmemCols = 128;
 constexpr int kUThreads = 256;
-constexpr int kQPerWarp = kBM / (kUThreads / 32);  // 16
-constexpr int kKsStride = kBN + 1;
+constexpr int kRound = 64;          // tile columns per epilogue round
+constexpr int kRS = kRound + 1;      // key-tile row stride
+constexpr int kLS = 33;              // list row stride (row owners hit distinct banks)
 // A 128x128x256 tile finishes in about a microsecond; 2^16 polls with 32 ns
 // sleeps (a few ms) is far beyond that, and keeps a failing launch short.
 constexpr uint32_t kSpinLimit = 1u << 16;
@@ -151,10 +154,13 @@ __device__ __forceinline__ void stage_operand(unsigned char* op, const __nv_bflo
 
 }  // namespace
 
-// One block per (leaf, 128-query tile).  Prologue, MMA issue, bounded wait and
-// tensor-memory epilogue follow the single-tile sequence checked on its own
-// against a CPU product; the per-row merge is the FP32 leaf kernel's (each
-// query's list is read, merged with the tile row and written back).
+// One block per (leaf, 128-query tile).  The 128 queries' lists stay in shared
+// memory for the whole loop over candidate tiles (read once, written once);
+// each 128x128 tensor-core tile is emptied in two 64-column rounds: epilogue
+// (tcgen05.ld, approximate key, filter against the row's current last entry)
+// then a per-row merge of the survivors.  Prologue, MMA issue, bounded wait
+// and the tensor-memory loads follow the single-tile sequence that was checked
+// on its own against a CPU product.
 template <int METRIC>
 __global__ void __launch_bounds__(kUThreads, 1)
     k_leaf_tc(const __nv_bfloat16* __restrict__ Xb, int Kp, int64_t n, int k, int kq, int depth,
@@ -165,12 +171,15 @@ __global__ void __launch_bounds__(kUThreads, 1)
   const int nchunks = Kp / kKC;
   unsigned char* opA = smem;
   unsigned char* opB = opA + nchunks * kChunkBytes;
-  float* Ks = reinterpret_cast<float*>(opB + nchunks * kChunkBytes);
-  int32_t* qid = reinterpret_cast<int32_t*>(Ks + kBM * kKsStride);
+  float* Ks = reinterpret_cast<float*>(opB + nchunks * kChunkBytes);  // [128][kRS] keys of one round
+  float* Lk = Ks + kBM * kRS;                                          // [128][kLS] list keys
+  uint32_t* Li = reinterpret_cast<uint32_t*>(Lk + kBM * kLS);         // [128][kLS] list ids
+  int32_t* qid = reinterpret_cast<int32_t*>(Li + kBM * kLS);
   int32_t* cid = qid + kBM;
   float* qn = reinterpret_cast<float*>(cid + kBN);
   float* cn = qn + kBM;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(cn + kBN);
+  int* cnt = reinterpret_cast<int*>(cn + kBN);  // survivors of each row in the current round
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(cnt + kBM);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
   int* status = reinterpret_cast<int*>(tmem_slot + 1);
 
@@ -210,6 +219,13 @@ __global__ void __launch_bounds__(kUThreads, 1)
     qn[tid] = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
   }
   __syncthreads();
+  for (int e = tid; e < kBM * 32; e += kUThreads) {
+    const int r = e >> 5, s = e & 31;
+    const int32_t id = qid[r];
+    const bool live = id >= 0 && s < kq;
+    Lk[r * kLS + s] = live ? akey[(size_t)id * kq + s] : kInf;
+    Li[r * kLS + s] = live ? aid[(size_t)id * kq + s] : kNoId;
+  }
   stage_operand(opA, Xb, Kp, qid);
 
   uint32_t phase = 0;
@@ -219,6 +235,7 @@ __global__ void __launch_bounds__(kUThreads, 1)
       const int32_t id = tid < mc ? perm[blo + c0 + tid] : -1;
       cid[tid] = id;
       cn[tid] = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
+      cnt[tid] = 0;
     }
     __syncthreads();
     stage_operand(opB, Xb, Kp, cid);
@@ -249,59 +266,77 @@ __global__ void __launch_bounds__(kUThreads, 1)
     }
     __syncthreads();
     phase ^= 1u;
-    const int stat = *status;
-    if (stat != 0) break;  // uniform: read after the barrier
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    {
-      const int quarter = warp & 3, half = warp >> 2;
-      const int r = quarter * 32 + lane;
-      const bool rv = r < mq;
-      const int32_t myid = qid[r];
-      const float myn = qn[r];
-#pragma unroll 1
-      for (int cc = 0; cc < 2; ++cc) {
-        const int col0 = half * 64 + cc * 32;
+    if (*status != 0) break;  // uniform: read after the barrier
+
+    for (int rb = 0; rb < mc; rb += kRound) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      {
+        const int quarter = warp & 3, half = warp >> 2;
+        const int r = quarter * 32 + lane;
+        const int col0 = rb + half * 32;
         uint32_t v[32];
         tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)col0, v);
+        const bool rv = r < mq;
+        const int32_t myid = qid[r];
+        const float myn = qn[r];
+        const float tk = Lk[r * kLS + kq - 1];
+        const uint32_t ti = Li[r * kLS + kq - 1];
+        int survivors = 0;
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
           const int c = col0 + j;
           const float dot = __uint_as_float(v[j]);
           const float key = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[c]))
                                                            : __fsub_rn(1.f, dot);
-          Ks[r * kKsStride + c] = (rv && c < mc && cid[c] != myid) ? key : kInf;
+          // only keys that can still enter the row's list survive
+          const bool s = rv && c < mc && cid[c] != myid && cand_less(key, (uint32_t)cid[c], tk, ti);
+          Ks[r * kRS + half * 32 + j] = s ? key : kInf;
+          survivors += s ? 1 : 0;
         }
+        if (survivors) atomicAdd(&cnt[r], survivors);
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      __syncthreads();
+      // one warp per query row with survivors: list one entry per lane; each
+      // survivor is checked against the list ids by one ballot and placed by
+      // warp_insert1
+      for (int qq = warp; qq < mq; qq += kUThreads / 32) {
+        if (cnt[qq] == 0) continue;
+        float lk = Lk[qq * kLS + lane];
+        uint32_t li = Li[qq * kLS + lane];
+        for (int cb = 0; cb < kRound; cb += 32) {
+          const float ck = Ks[qq * kRS + cb + lane];
+          const int c = rb + cb + lane;
+          const uint32_t ci = c < mc ? (uint32_t)cid[c] : kNoId;
+          uint32_t bal = __ballot_sync(0xFFFFFFFFu, ck < kInf);
+          while (bal) {
+            const int src = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const float k1 = __shfl_sync(0xFFFFFFFFu, ck, src);
+            const uint32_t i1 = __shfl_sync(0xFFFFFFFFu, ci, src);
+            const float tk = __shfl_sync(0xFFFFFFFFu, lk, kq - 1);
+            const uint32_t ti = __shfl_sync(0xFFFFFFFFu, li, kq - 1);
+            const bool dup = __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
+            if (!dup && cand_less(k1, i1, tk, ti)) warp_insert1(lk, li, k1, i1);
+          }
+        }
+        Lk[qq * kLS + lane] = lk;
+        Li[qq * kLS + lane] = li;
+        __syncwarp();
+        if (lane == 0) cnt[qq] = 0;
+      }
+      __syncthreads();
+    }
+  }
+  if (*status == 0) {
+    for (int e = tid; e < kBM * 32; e += kUThreads) {
+      const int r = e >> 5, s = e & 31;
+      const int32_t id = qid[r];
+      if (id >= 0 && s < kq) {
+        akey[(size_t)id * kq + s] = Lk[r * kLS + s];
+        aid[(size_t)id * kq + s] = Li[r * kLS + s];
       }
     }
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    // merge each query row of the tile into that query's list
-    for (int qq = warp; qq < mq; qq += kUThreads / 32) {
-      const uint32_t i = (uint32_t)qid[qq];
-      WarpList<1> L;
-      L.key[0] = lane < kq ? akey[(size_t)i * kq + lane] : kInf;
-      L.id[0] = lane < kq ? aid[(size_t)i * kq + lane] : kNoId;
-      for (int cb = 0; cb < mc; cb += 32) {
-        const int c = cb + lane;
-        const bool inrange = c < mc;
-        const float ck = inrange ? Ks[qq * kKsStride + c] : kInf;
-        const uint32_t ci = inrange ? (uint32_t)cid[c] : kNoId;
-        float tk;
-        uint32_t ti;
-        warp_list_get(L, kq - 1, tk, ti);
-        bool pass = inrange && ck < kInf && cand_less(ck, ci, tk, ti);
-        if (!__any_sync(0xFFFFFFFFu, pass)) continue;
-        const bool dup = warp_list_contains(L, ci, kq);
-        pass = pass && !dup;
-        if (!__any_sync(0xFFFFFFFFu, pass)) continue;
-        warp_list_insert(L, pass ? ck : kInf, pass ? ci : kNoId);
-      }
-      if (lane < kq) {
-        akey[(size_t)i * kq + lane] = L.key[0];
-        aid[(size_t)i * kq + lane] = L.id[0];
-      }
-    }
-    __syncthreads();
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
@@ -386,8 +421,9 @@ __global__ void __launch_bounds__(256) k_rerank(const float* __restrict__ X, int
 }
 
 size_t umma_smem_bytes(int Kp) {
-  return 1024 + 2 * (size_t)(Kp / kKC) * kChunkBytes + (size_t)kBM * kKsStride * 4 +
-         (size_t)(kBM + kBN) * 8 + 64;
+  // alignment slack + A + B + round keys + lists + (qid, cid, qn, cn) + cnt + barrier words
+  return 1024 + 2 * (size_t)(Kp / kKC) * kChunkBytes + (size_t)kBM * kRS * 4 + (size_t)kBM * kLS * 8 +
+         (size_t)(kBM + kBN) * 8 + (size_t)kBM * 4 + 64;
 }
 
 int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
