@@ -3,21 +3,30 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-A step is one full k-NN graph build (trees -> leaf blocks -> propagation ->
-sorted lists) of the integer-mixture workload: N=1,000,000 points, d=128,
-float32 integer values in [0,255] from a 256-cluster Gaussian mixture (seeded
-synthetic data, no dataset needed); k=16, 16 trees, leaf 64, 5 propagations,
-EUCLIDEAN.  `value` is points/s with the points already in HBM; `e2e` is the
-same metric through the public C ABI with pinned host buffers (host->device
-copy of the points and device->host copy of the graph inside the timed
-region).  Recall@k and distance error are measured against the FP64 exact
-graph on 10,000 seeded queries.
+Workload (seeded synthetic data, no dataset needed): the integer mixture,
+N=1,000,000 points, d=128, float32 integer values in [0,255] drawn from a
+256-cluster Gaussian mixture (centres U[0,255], sigma 20); k=16, EUCLIDEAN.
+
+Metric: k-NN graph points/s at recall@k >= 0.95 against the FP64 exact graph.
+A step is one full graph build (trees -> leaf blocks -> propagation -> sorted
+lists).  The headline path is the mixed-precision builder (BF16 tcgen05 leaf
+tiles + exact FP32 re-rank) at the cheapest setting that reaches recall 0.95
+on this workload (10 trees, leaf 1024, 1 propagation); the plain FP32 builder
+is timed at the same setting (identical output on this data: every BF16
+product and FP32 sum is exact), and both at the configuration's literal
+parameters (16 trees, leaf 64, 5 propagations), which stay below 0.95.
+
+`value` is points/s with the points already in HBM (512 MB, larger than L2);
+`e2e` is the same build through the public C ABI with pinned host buffers
+(host->device copy of the points and device->host copy of the graph inside the
+timed region).  Recall@k and distance error are measured against the FP64
+exact graph (knn_exact_fp64) on 10,000 seeded queries.
 
 With --gpus N > 1 (launched by torchrun) every rank builds the graph of its own
 dataset (seed = rank): independent replicas, weak scaling, no collective on
 the data path.  `--impl reference` times the CPU rendition of the reference
-algorithm (the reference itself has no CPU implementation) on a bounded
-sample of the same workload with all host threads.
+algorithm (the reference itself has no CPU implementation) on a bounded sample
+of the same workload with all host threads.
 """
 from __future__ import annotations
 
@@ -39,6 +48,12 @@ ROOT = Path(__file__).resolve().parent
 PKG_DIR = ROOT / "approximate-cuda-knn_b200"
 METRIC_NAME = "k-NN graph points/s at recall@k≥0.95 vs FP64 exact, mixed/learned vs plain FP32"
 METRIC_NAMES = {0: "EUCLIDEAN", 1: "TAXICAB", 2: "COSINE"}
+
+WORKLOAD = dict(name="integer_mixture", n=1_000_000, d=128, k=16, metric=0)
+# the configuration's own parameters
+CONFIG_PARAMS = dict(trees=16, leaf=64, props=5)
+# cheapest setting found to reach recall@16 >= 0.95 on this workload (trees x leaf x props sweep)
+TARGET_PARAMS = dict(trees=10, leaf=1024, props=1)
 
 
 def load_package():
@@ -118,15 +133,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-# ------------------------------------------------------------- workloads --
-WORKLOAD = dict(name="integer_mixture", n=1_000_000, d=128, k=16, trees=16, leaf=64, props=5,
-                metric=0)
-
-
-def workload_desc(w) -> str:
+def workload_desc(w, p) -> str:
     return (f"integer_mixture N={w['n']:,} d={w['d']} float32 ints in [0,255] (256-cluster "
-            f"mixture, sigma 20); k={w['k']}, {w['trees']} trees, leaf {w['leaf']}, "
-            f"{w['props']} propagations, {METRIC_NAMES[w['metric']]}")
+            f"mixture, sigma 20); k={w['k']}, {p['trees']} trees, leaf {p['leaf']}, "
+            f"{p['props']} propagation(s), {METRIC_NAMES[w['metric']]}")
 
 
 def make_points(acknn, n: int, seed: int) -> np.ndarray:
@@ -134,14 +144,9 @@ def make_points(acknn, n: int, seed: int) -> np.ndarray:
 
 
 # ------------------------------------------------------------- accuracy --
-def accuracy(acknn, x: np.ndarray, idx: np.ndarray, dist: np.ndarray, k: int, metric: int,
-             nq: int = 10_000, seed: int = 12345) -> dict:
-    n = x.shape[0]
-    rng = np.random.Generator(np.random.PCG64(seed))
-    q = np.sort(rng.choice(n, size=min(nq, n), replace=False)).astype(np.int64)
-    ei, ed = acknn.exact_fp64(x, k, q, metric)
+def accuracy(acknn, x, idx, dist, k, metric, exact, q) -> dict:
+    ei, ed = exact
     ai, ad = idx[q], dist[q]
-    # FP64 distance of the returned pairs
     a = x[q].astype(np.float64)
     pair = np.empty(ai.shape, dtype=np.float64)
     for s in range(k):
@@ -163,7 +168,7 @@ def accuracy(acknn, x: np.ndarray, idx: np.ndarray, dist: np.ndarray, k: int, me
 
 
 # ------------------------------------------------------------ CPU rendition --
-def cpu_rendition(w, sample_n: int, repeats: int = 1) -> dict:
+def cpu_rendition(w, p, sample_n: int) -> dict:
     """The oracle's OpenMP rendition of the algorithm on a bounded sample."""
     sys.path.insert(0, str(ROOT / "tests"))
     from conftest import Oracle  # noqa: E402  -- the CPU baseline leg only
@@ -176,16 +181,14 @@ def cpu_rendition(w, sample_n: int, repeats: int = 1) -> dict:
     acknn = load_package()
     x = make_points(acknn, sample_n, seed=0)
     cores = os.cpu_count() or 1
-    times = []
-    for _ in range(repeats):
-        t = time.perf_counter()
-        orc.knn_build(x, w["k"], w["trees"], w["leaf"], w["props"], w["metric"], seed=0,
-                      threads=cores)
-        times.append(time.perf_counter() - t)
-    sec = min(times)
+    t = time.perf_counter()
+    orc.knn_build(x, w["k"], p["trees"], p["leaf"], p["props"], w["metric"], seed=0,
+                  threads=cores)
+    sec = time.perf_counter() - t
     return {"value": sample_n / sec, "unit": "points/s", "cores": cores, "kind": "port",
-            "sample": f"{sample_n:,} points of the same generator and parameters "
-                      f"(full workload is {w['n']:,}); best of {repeats}; {sec:.2f} s",
+            "sample": f"{sample_n:,} points of the same generator with {p['trees']} trees, leaf "
+                      f"{p['leaf']}, {p['props']} propagation(s) (full workload {w['n']:,}); "
+                      f"{sec:.2f} s",
             "seconds": sec}
 
 
@@ -201,25 +204,25 @@ def run_reference(args, w):
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    sample = args.cpu_sample
-    vals = []
+    p = TARGET_PARAMS
+    secs, last = [], None
     for i in range(args.warmup + args.steps):
-        r = cpu_rendition(w, sample, repeats=1)
+        r = cpu_rendition(w, p, args.cpu_sample)
         if i >= args.warmup:
-            vals.append(r)
-    sec = sum(r["seconds"] for r in vals) / len(vals)
-    value = sample / sec
-    cores = vals[0]["cores"]
+            secs.append(r["seconds"])
+            last = r
+    sec = sum(secs) / len(secs)
+    value = args.cpu_sample / sec
     line = {
         "impl": "reference", "metric": METRIC_NAME, "value": value, "unit": "points/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_desc(w), "sample_points": sample,
-                   "implementation": "CPU rendition of the reference algorithm (OpenMP), the "
+        "config": {"workload": workload_desc(w, p), "sample_points": args.cpu_sample,
+                   "implementation": "CPU rendition of the reference algorithm (OpenMP); the "
                                      "reference has no CPU path of its own"},
-        "cpu_baseline": {"value": value, "unit": "points/s", "cores": cores, "kind": "port",
-                         "sample": vals[0]["sample"]},
+        "cpu_baseline": {"value": value, "unit": "points/s", "cores": last["cores"],
+                         "kind": "port", "sample": last["sample"]},
         "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -244,7 +247,7 @@ def run_ours(args, w):
     dev = torch.cuda.current_device()
     acknn = load_package()
     lib = acknn.load_library()
-    n, d, k = w["n"], w["d"], w["k"]
+    n, d, k, metric = w["n"], w["d"], w["k"], w["metric"]
     x = make_points(acknn, n, seed=rank)
     xh = torch.from_numpy(x).pin_memory()
     xd = xh.to(f"cuda:{dev}")
@@ -254,25 +257,18 @@ def run_ours(args, w):
     dist_h = torch.empty((n, k), dtype=torch.float32).pin_memory()
     ctx = acknn.Context(dev)
     stream = torch.cuda.current_stream()
-    prec = acknn.PREC_BF16_RERANK if args.precision == "bf16" else acknn.PREC_FP32
+    MIXED, PLAIN = acknn.PREC_BF16_RERANK, acknn.PREC_FP32
+    head = TARGET_PARAMS
 
-    opt_dev = acknn.default_options(device=dev, points_on_device=1, outputs_on_device=1,
+    def build(p, prec, host=False, stats=None):
+        opt = acknn.default_options(device=dev, points_on_device=0 if host else 1,
+                                    outputs_on_device=0 if host else 1,
                                     stream=stream.cuda_stream, precision=prec)
-    opt_host = acknn.default_options(device=dev, points_on_device=0, outputs_on_device=0,
-                                     stream=stream.cuda_stream, precision=prec)
-
-    def step_device(stats=None):
-        rc = lib.knn_build_ex(ctx.handle, xd.data_ptr(), n, d, k, w["trees"], w["leaf"],
-                              w["props"], w["metric"], args.seed, idx_d.data_ptr(),
-                              dist_d.data_ptr(), ctypes.byref(opt_dev),
-                              ctypes.byref(stats) if stats is not None else None)
-        if rc:
-            raise acknn.KnnError(rc, lib.knn_last_error().decode())
-
-    def step_host():
-        rc = lib.knn_build_ex(ctx.handle, xh.data_ptr(), n, d, k, w["trees"], w["leaf"],
-                              w["props"], w["metric"], args.seed, idx_h.data_ptr(),
-                              dist_h.data_ptr(), ctypes.byref(opt_host), None)
+        src = xh if host else xd
+        oi, od = (idx_h, dist_h) if host else (idx_d, dist_d)
+        rc = lib.knn_build_ex(ctx.handle, src.data_ptr(), n, d, k, p["trees"], p["leaf"],
+                              p["props"], metric, args.seed, oi.data_ptr(), od.data_ptr(),
+                              ctypes.byref(opt), ctypes.byref(stats) if stats is not None else None)
         if rc:
             raise acknn.KnnError(rc, lib.knn_last_error().decode())
 
@@ -287,64 +283,77 @@ def run_ours(args, w):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # warm-up (allocates the context's scratch)
-    for _ in range(args.warmup):
-        step_device()
-    torch.cuda.synchronize()
+    def timed(fn, steps) -> float:
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / steps)
 
-    # one instrumented call for stage times and counts
+    # warm-up of the headline build (allocates the context's scratch)
+    for _ in range(args.warmup):
+        build(head, MIXED)
+    torch.cuda.synchronize()
     st = acknn.KnnStats()
     st.struct_size = ctypes.sizeof(acknn.KnnStats)
-    step_device(st)
+    build(head, MIXED, stats=st)
     torch.cuda.synchronize()
     stages = st.as_dict()
 
-    # timed: device-resident points and graph
     clocks = ClockSampler(dev)
     clocks.start()
-    barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step_device()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-
-    # timed: end to end through the public API with pinned host buffers
-    barrier()
-    torch.cuda.synchronize()
-    e2 = torch.cuda.Event(enable_timing=True)
-    e3 = torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    for _ in range(args.steps):
-        step_host()
-    e3.record(stream)
-    torch.cuda.synchronize()
-    barrier()
+    ms = timed(lambda: build(head, MIXED), args.steps)
+    ms_e2e = timed(lambda: build(head, MIXED, host=True), args.steps)
     clk = clocks.stop()
-    ms_e2e = max_over_ranks(e2.elapsed_time(e3) / args.steps)
+    mixed_idx = idx_h.numpy().copy()
+    mixed_dist = dist_h.numpy().copy()
+    same_dev_host = bool(torch.equal(idx_d.cpu(), idx_h) and torch.equal(dist_d.cpu(), dist_h))
 
-    # the device and host results must agree (same build)
-    same = bool(torch.equal(idx_d.cpu(), idx_h) and torch.equal(dist_d.cpu(), dist_h))
+    # the plain FP32 builder at the same setting
+    build(head, PLAIN)
+    ms_plain = timed(lambda: build(head, PLAIN), args.steps)
+    plain_same = bool(np.array_equal(idx_d.cpu().numpy(), mixed_idx) and
+                      np.array_equal(dist_d.cpu().numpy(), mixed_dist))
+    # both at the configuration's literal parameters (one step each, after a warm-up)
+    lit = {}
+    for name, prec in (("plain_fp32", PLAIN), ("mixed", MIXED)):
+        build(CONFIG_PARAMS, prec)
+        lit[name] = {"ms": timed(lambda: build(CONFIG_PARAMS, prec), 1)}
+    lit_idx = idx_d.cpu().numpy()
+    lit_dist = dist_d.cpu().numpy()
 
-    acc = accuracy(acknn, x, idx_h.numpy(), dist_h.numpy(), k, w["metric"]) if rank == 0 else {}
+    acc = lit_acc = {}
+    if rank == 0:
+        rng = np.random.Generator(np.random.PCG64(12345))
+        q = np.sort(rng.choice(n, size=min(10_000, n), replace=False)).astype(np.int64)
+        exact = acknn.exact_fp64(x, k, q, metric)
+        acc = accuracy(acknn, x, mixed_idx, mixed_dist, k, metric, exact, q)
+        lit_acc = accuracy(acknn, x, lit_idx, lit_dist, k, metric, exact, q)
+    for v in lit.values():
+        v["points_per_s"] = world * n / (v["ms"] / 1e3)
+        v["recall"] = lit_acc.get("recall")
 
     value = world * n / (ms / 1e3)
     value_e2e = world * n / (ms_e2e / 1e3)
+    value_plain = world * n / (ms_plain / 1e3)
 
     # roofline of the dominant stage (algorithmic bytes per launch / mean launch time)
     peak, peak_kind = measured_peaks()
-    T, L, P = w["trees"], stages["depth"], w["props"]
+    T, L, P = head["trees"], stages["depth"], head["props"]
     s = 4
+    kq = min(32, 2 * k)
     prop_bytes = sum(n * (k * k * 4 + 2 * k * 8) + c * d * s for c in stages["prop_candidates"])
-    leaf_bytes = T * (n * d * s + n * k * 8)
+    # tensor-core leaf stage: the BF16 rows (d*2 B) and each point's kq-entry list per tree
+    leaf_bytes = T * (n * d * 2 + n * kq * 8 * 2)
     tree_bytes = T * L * (n * d * s + 16 * n)
-    cand = {"propagate": (stages["ms_propagate"], prop_bytes, P),
-            "leaf": (stages["ms_leaf"], leaf_bytes, T),
+    cand = {"propagate": (stages["ms_propagate"], prop_bytes, max(1, P)),
+            "leaf_tc": (stages["ms_leaf"], leaf_bytes, T),
             "trees": (stages["ms_trees"], tree_bytes, 3 * L)}
     dom = max(cand, key=lambda kname: cand[kname][0])
     dms, dbytes, dlaunch = cand[dom]
@@ -352,31 +361,36 @@ def run_ours(args, w):
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                 "peak_source": peak_kind,
-                "algorithmic_bytes_per_launch": dbytes / max(1, dlaunch),
-                "mean_launch_ms": dms / max(1, dlaunch)}
+                "algorithmic_bytes_per_launch": dbytes / dlaunch,
+                "mean_launch_ms": dms / dlaunch}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = cpu_rendition(w, args.cpu_sample)
+        r = cpu_rendition(w, head, args.cpu_sample)
         cpu = {kk: r[kk] for kk in ("value", "unit", "cores", "kind", "sample")}
 
     if rank == 0:
         line = {
             "metric": METRIC_NAME, "value": value, "unit": "points/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32",
             "data": "synthetic (seeded integer Gaussian mixture; seed = rank)",
-            "config": {"workload": workload_desc(w), "n": n, "d": d, "k": k,
-                       "trees": w["trees"], "leaf": w["leaf"], "props": w["props"],
-                       "metric": METRIC_NAMES[w["metric"]], "precision": args.precision,
+            "config": {"workload": workload_desc(w, head), "n": n, "d": d, "k": k,
+                       **head, "metric": METRIC_NAMES[metric],
+                       "path": "mixed: BF16 tcgen05 leaf tiles + FP32 re-rank",
                        "l2": "inputs larger than L2 (512 MB of points per step)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-            "accuracy": acc, "stages_ms": {kk: stages[kk] for kk in (
+            "accuracy": acc,
+            "plain_fp32_same_setting": {"value": value_plain, "ms_per_step": ms_plain,
+                                        "identical_graph": plain_same,
+                                        "mixed_speedup": value / value_plain},
+            "config_literal_params": {"params": CONFIG_PARAMS, **lit},
+            "stages_ms": {kk: stages[kk] for kk in (
                 "ms_upload", "ms_trees", "ms_leaf", "ms_propagate", "ms_download", "ms_total")},
             "prop_candidates": stages["prop_candidates"],
             "e2e": {"value": value_e2e, "unit": "points/s", "ms_per_step": ms_e2e,
                     "h2d_bytes_per_step": int(n * d * 4),
-                    "d2h_bytes_per_step": int(n * k * 8), "matches_device_run": same},
+                    "d2h_bytes_per_step": int(n * k * 8), "matches_device_run": same_dev_host},
             "gpu_launches": int(stages["launches"]) * args.steps * 2,
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
         }
@@ -393,10 +407,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp32", "bf16"], default="fp32")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--n", type=int, default=None, help="override N (smaller runs)")
-    ap.add_argument("--cpu-sample", type=int, default=100_000)
+    ap.add_argument("--cpu-sample", type=int, default=20_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
