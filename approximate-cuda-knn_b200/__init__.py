@@ -106,6 +106,7 @@ EXPORTS = {
     "knn_version": (ctypes.c_int, []),
     "knn_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "knn_last_error": (ctypes.c_char_p, []),
+    "knn_device_capability": (ctypes.c_int, [_I32, _P, _P]),
     "knn_context_create": (_P, [_I32]),
     "knn_context_destroy": (None, [_P]),
     "knn_context_scratch_bytes": (_I64, [_P]),

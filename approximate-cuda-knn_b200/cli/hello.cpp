@@ -1,0 +1,239 @@
+// hello -- drop-in command line of the k-NN graph builder.
+//
+//   hello <input_file> <output_file> <k> <trees> <leaf_size> <propagations>
+//         <EUCLIDEAN|TAXICAB|COSINE> <gpu_id[,gpu_id...]> <cluster: T/F> [--debug]
+//
+// Same argument order, messages and exit codes as the reference's main.cpp
+// (main.cpp:8-124): 1 wrong argument count, 2 unknown metric, 3 device not
+// present, 4 compute capability 1.x, 5 no CUDA GPU, 7 input not readable,
+// 8 initialisation failed, 9 deinitialisation failed.  Input is the reference's
+// CSV (README.md:31-47, loadData euclideandistancematrixgpu.cu:2712-2757), parsed
+// here by several threads; output is its binary layout (saveResultToResultFile,
+// .cu:2908-2978) with the VALIDATION and DEBUG side files.  The points are
+// normalised as the reference's calculate() does (.cu:2869-2875) before the
+// graph is built by knn_build on the first listed device.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "knn.h"
+
+namespace {
+
+void usage() {
+  std::cout << "Wrong number of arguments!\n";
+  std::cout << "Proper launching: hello.exe <input_file> <output_file> <number_of_neighbours> "
+               "<number_of_trees> <number_of_elements_in_leaf> <number_of_propagations> "
+               "<distance_Algorithm> <id_gpu> <cluster: T/F> <--debug>\n";
+  std::cout << "Example launching: hello.exe input.csv output.csv 2 10 10 10 EUCLIDEAN 1 T\n";
+  std::cout << "Example launching: hello.exe input.csv output.csv 2 10 10 10 EUCLIDEAN 1 T --debug\n";
+  std::cout << "Available distance algorithms: EUCLIDEAN TAXICAB COSINE\n";
+  std::cout << "Attention!\n";
+  std::cout << "Delimeter -> ,\n";
+  std::cout << "If file has cluster (at the end of line) you should run program with cluster set "
+               "T, otherwise F\n";
+}
+
+// One CSV point line: tokens split on ',' (empty tokens skipped, as strtok
+// does), each parsed like atof (leading blanks, longest numeric prefix, 0 when
+// none) and narrowed to float; with `klaster` the last token is the cluster id.
+void parse_line(const char* s, const char* e, int d, bool klaster, float* row) {
+  std::vector<std::pair<const char*, const char*>> toks;
+  const char* p = s;
+  while (p < e) {
+    while (p < e && *p == ',') ++p;
+    if (p >= e) break;
+    const char* q = p;
+    while (q < e && *q != ',') ++q;
+    toks.emplace_back(p, q);
+    p = q;
+  }
+  size_t nfeat = toks.size();
+  if (klaster && nfeat > 0) --nfeat;
+  char buf[128];
+  for (size_t i = 0; i < nfeat && (int)i < d; ++i) {
+    size_t len = std::min<size_t>(toks[i].second - toks[i].first, sizeof(buf) - 1);
+    std::memcpy(buf, toks[i].first, len);
+    buf[len] = 0;
+    row[i] = (float)std::atof(buf);
+  }
+}
+
+bool load_csv(const std::string& path, int64_t n, int d, bool klaster, std::vector<float>& x) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f.is_open()) return false;
+  std::stringstream ss;
+  ss << f.rdbuf();
+  const std::string text = ss.str();
+  // skip the two header lines, then index the point lines
+  size_t pos = 0;
+  for (int h = 0; h < 2 && pos < text.size(); ++h) {
+    size_t nl = text.find('\n', pos);
+    pos = nl == std::string::npos ? text.size() : nl + 1;
+  }
+  std::vector<std::pair<size_t, size_t>> lines;
+  lines.reserve((size_t)n);
+  while (pos < text.size() && (int64_t)lines.size() < n) {
+    size_t nl = text.find('\n', pos);
+    size_t end = nl == std::string::npos ? text.size() : nl;
+    lines.emplace_back(pos, end);
+    pos = end + 1;
+  }
+  x.assign((size_t)n * d, 0.0f);
+  const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  const size_t per = (lines.size() + hw - 1) / hw;
+  for (unsigned t = 0; t < hw; ++t) {
+    const size_t a = t * per, b = std::min(lines.size(), a + per);
+    if (a >= b) break;
+    pool.emplace_back([&, a, b] {
+      for (size_t i = a; i < b; ++i)
+        parse_line(text.data() + lines[i].first, text.data() + lines[i].second, d, klaster,
+                   x.data() + i * d);
+    });
+  }
+  for (auto& th : pool) th.join();
+  return true;
+}
+
+bool save_result(const std::string& out, const std::vector<int32_t>& idx, const std::vector<float>& dist,
+                 int64_t n, int k, int metric, bool debug) {
+  std::ofstream ofs(out, std::ofstream::trunc | std::ofstream::binary);
+  std::ofstream dbg;
+  if (debug) dbg.open(out + "DEBUG", std::ofstream::trunc | std::ofstream::binary);
+  std::ofstream val(out + "VALIDATION", std::ofstream::trunc | std::ofstream::binary);
+  if (!ofs.is_open()) {
+    std::cout << "Can not open the file for saving result.\n";
+    return false;
+  }
+  ofs << n << ";" << k << ";" << sizeof(int64_t) << "\n";
+  const int64_t magic = 0x01020304;
+  ofs.write(reinterpret_cast<const char*>(&magic), sizeof(magic));
+  std::vector<char> rec((size_t)k * 8);
+  for (int64_t i = 0; i < n; ++i) {
+    for (int s = 0; s < k; ++s) {
+      const float dv = dist[(size_t)i * k + s];
+      // stored distance: L2, sqrt(L1) (.cu:567-570), or cosine similarity (.cu:1007)
+      float stored = dv;
+      if (metric == KNN_METRIC_TAXICAB) stored = std::sqrt(dv);
+      else if (metric == KNN_METRIC_COSINE) stored = (float)(1.0 - (double)dv);
+      const int32_t id = idx[(size_t)i * k + s];
+      std::memcpy(rec.data() + (size_t)s * 8, &id, 4);
+      std::memcpy(rec.data() + (size_t)s * 8 + 4, &stored, 4);
+      if (dbg.is_open()) dbg << "NEAR: <" << i << ", " << id << ">(" << stored << ") ";
+    }
+    ofs.write(rec.data(), (std::streamsize)rec.size());
+    if (dbg.is_open()) dbg << ";\n";
+  }
+  if (val.is_open()) val << "Everything is OK.";
+  return true;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc != 10 && argc != 11) {
+    usage();
+    return 1;
+  }
+  const std::string input = argv[1], output = argv[2];
+  const int k = std::atoi(argv[3]);
+  const int trees = std::atoi(argv[4]);
+  const int leaf = std::atoi(argv[5]);
+  const int props = std::atoi(argv[6]);
+  const std::string mname = argv[7];
+  int metric;
+  if (mname == "EUCLIDEAN") metric = KNN_METRIC_EUCLIDEAN;
+  else if (mname == "TAXICAB") metric = KNN_METRIC_TAXICAB;
+  else if (mname == "COSINE") metric = KNN_METRIC_COSINE;
+  else {
+    std::cout << "Wrong distance algorithm!\n";
+    std::cout << "Available distance algorithms: EUCLIDEAN TAXICAB COSINE\n";
+    return 2;
+  }
+  std::vector<int> devices;
+  {
+    std::string list = argv[8];
+    size_t p = 0;
+    while (p <= list.size()) {
+      size_t q = list.find(',', p);
+      if (q == std::string::npos) q = list.size();
+      if (q > p) devices.push_back(std::atoi(list.substr(p, q - p).c_str()));
+      p = q + 1;
+    }
+  }
+  for (int dev : devices) {
+    int32_t major = 0, minor = 0;
+    const int rc = knn_device_capability(dev, &major, &minor);
+    if (rc != KNN_OK) {
+      std::cout << "Device with id " << dev << " is not located in this computer\n";
+      return 3;
+    }
+    if (major == 1) {
+      std::cout << "Device with id " << dev
+                << " can not be use because Compute Capability. Required at least 2.0 Compute "
+                   "Capability, your GPU has "
+                << major << "." << minor << "\n";
+      return 4;
+    }
+    if (major == 9999) {
+      std::cout << "This computer does not have any GPU with CUDA\n";
+      return 5;
+    }
+  }
+  const bool klaster = std::string(argv[9]) == "T";
+  const bool debug = argc == 11 && std::string(argv[10]) == "--debug";
+
+  std::ifstream head(input);
+  if (!head.is_open()) {
+    std::cout << "Error opening the file\n";
+    return 7;
+  }
+  std::string line;
+  std::getline(head, line);
+  const int64_t n = std::atoi(line.c_str());
+  std::getline(head, line);
+  const int d = std::atoi(line.c_str());
+  head.close();
+
+  std::vector<float> x;
+  if (devices.empty() || n < 1 || d < 1 || !load_csv(input, n, d, klaster, x)) {
+    std::cout << "Initialization failed.\n";
+    return 8;
+  }
+  std::cout << "The datafile has been opened\n";
+  std::cout << "I begin analysis.\n";
+  knn_options opt;
+  knn_default_options(&opt);
+  opt.device = devices[0];
+  std::vector<int32_t> idx((size_t)n * (k > 0 ? k : 1));
+  std::vector<float> dist((size_t)n * (k > 0 ? k : 1));
+  const auto t0 = std::chrono::steady_clock::now();
+  int rc = knn_normalize_reference(x.data(), n, d);
+  if (rc == KNN_OK)
+    rc = knn_build_ex(nullptr, x.data(), n, d, k, trees, leaf, props, metric, 0, idx.data(),
+                      dist.data(), &opt, nullptr);
+  const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (rc != KNN_OK) {
+    std::cout << "k-NN graph build failed: " << knn_status_string(rc) << " (" << knn_last_error() << ")\n";
+    return 8;
+  }
+  std::cout << "The device " << devices[0] << ": has done task in: " << ms << " ms\n";
+  std::cout << "I am writing the solution to a file.\n";
+  if (!save_result(output, idx, dist, n, k, metric, debug)) {
+    std::cout << "Deinitialization failed.\n";
+    return 9;
+  }
+  std::cout << "The end\n";
+  return 0;
+}

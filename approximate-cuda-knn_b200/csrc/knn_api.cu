@@ -497,6 +497,23 @@ void knn_default_options(knn_options* opt) {
 
 int knn_version(void) { return 100; }
 
+int knn_device_capability(int32_t device, int32_t* major, int32_t* minor) {
+  if (!major || !minor) return fail(KNN_ERR_ARGS, "NULL pointer");
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(KNN_ERR_NO_DEVICE, "no CUDA device");
+  }
+  if (device < 0 || device >= count) return fail(KNN_ERR_ARGS, "device ordinal out of range");
+  cudaDeviceProp p;
+  e = cudaGetDeviceProperties(&p, device);
+  if (e != cudaSuccess) return fail_cuda(e, "cudaGetDeviceProperties");
+  *major = p.major;
+  *minor = p.minor;
+  return KNN_OK;
+}
+
 const char* knn_status_string(int status) {
   switch (status) {
     case KNN_OK: return "ok";

@@ -373,7 +373,9 @@ __global__ void k_to_bf16(const float* __restrict__ X, int64_t n, int d, int dpa
 }
 
 // Exact FP32 keys (the reference's order) of each point's kq approximate
-// candidates; the best k become the list, all flagged new.  One warp per point.
+// candidates; the best k become the list, all flagged new.  One warp per point:
+// the candidate rows are staged 64 dims at a time by 16-byte cp.async into an
+// xor-swizzled tile (lane r reads row r conflict-free), one lane per candidate.
 template <int METRIC>
 __global__ void __launch_bounds__(256) k_rerank(const float* __restrict__ X, int64_t n, int d, int dpad,
                                                 int k, int kq, const float* __restrict__ norms,
@@ -382,31 +384,45 @@ __global__ void __launch_bounds__(256) k_rerank(const float* __restrict__ X, int
   extern __shared__ __align__(16) float rsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
-  float* xq = rsm + (size_t)warp * (dpad + 32 * 65);
+  float* xq = rsm + (size_t)warp * (dpad + 32 * 64 + 32);
   float* rows = xq + dpad;
+  uint32_t* ids = reinterpret_cast<uint32_t*>(rows + 32 * 64);
   if (i >= n) return;
   const float kInf = __int_as_float(0x7F800000);
-  for (int c = lane; c < dpad; c += 32) xq[c] = X[(size_t)i * dpad + c];
+  const float4* xr = reinterpret_cast<const float4*>(X + (size_t)i * dpad);
+  for (int c = lane; c < (dpad >> 2); c += 32) reinterpret_cast<float4*>(xq)[c] = xr[c];
   const uint32_t cj = lane < kq ? aid[(size_t)i * kq + lane] : kNoId;
   const bool valid = cj != kNoId;
+  ids[lane] = cj;
+  __syncwarp();
   float total = 0.f, part = 0.f;
+  const int half = lane >> 4, c4 = lane & 15;
   for (int cd = 0; cd < d; cd += 64) {
-    __syncwarp();
-    // stage 32 rows x 64 dims, padded stride 65 (conflict-free per-lane reads)
-    for (int r = 0; r < 32; ++r) {
-      const uint32_t id = __shfl_sync(0xFFFFFFFFu, cj, r);
-      for (int c = lane; c < 64; c += 32) {
-        const int dim = cd + c;
-        rows[r * 65 + c] = (id != kNoId && dim < dpad) ? X[(size_t)id * dpad + dim] : 0.f;
-      }
+    const int dim = cd + 4 * c4;
+    for (int r = half; r < 32; r += 2) {
+      const uint32_t id = ids[r];
+      const bool ok = id != kNoId && dim < dpad;
+      const float* src = X + (size_t)(id != kNoId ? id : 0) * dpad + (dim < dpad ? dim : 0);
+      cp_async16(smem_u32(rows + r * 64 + ((c4 ^ (r & 7)) << 2)), src, ok ? 16 : 0);
     }
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncwarp();
     const int lim = min(64, d - cd);
-    for (int c = 0; c < lim; ++c) part = acc_step<METRIC>(xq[cd + c], rows[lane * 65 + c], part);
+    const float* myrow = rows + lane * 64;
+    for (int q4 = 0; q4 < (lim + 3) >> 2; ++q4) {
+      const float4 cv = *reinterpret_cast<const float4*>(myrow + ((q4 ^ (lane & 7)) << 2));
+      const float4 qv = *reinterpret_cast<const float4*>(xq + cd + 4 * q4);
+      part = acc_step<METRIC>(qv.x, cv.x, part);
+      part = acc_step<METRIC>(qv.y, cv.y, part);
+      part = acc_step<METRIC>(qv.z, cv.z, part);
+      part = acc_step<METRIC>(qv.w, cv.w, part);
+    }
     if (((cd + 64) & 255) == 0 || cd + 64 >= d) {
       total = __fadd_rn(total, part);
       part = 0.f;
     }
+    __syncwarp();
   }
   float key = total;
   if (METRIC == KNN_METRIC_COSINE) key = valid ? cosine_key(total, norms[i], norms[cj]) : kInf;
@@ -452,7 +468,7 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
     }
     log.add();
   }
-  const size_t rsm = (size_t)8 * (a.dpad + 32 * 65) * sizeof(float);
+  const size_t rsm = (size_t)8 * (a.dpad + 32 * 64 + 32) * sizeof(float);
   const unsigned rgrid = (unsigned)((a.n + 7) / 8);
   if (a.metric == KNN_METRIC_EUCLIDEAN) {
     cudaFuncSetAttribute(k_rerank<KNN_METRIC_EUCLIDEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm);

@@ -105,6 +105,11 @@ int knn_version(void);
 const char* knn_status_string(int status);
 const char* knn_last_error(void);
 
+/* Compute capability of `device`: KNN_OK, KNN_ERR_NO_DEVICE when the machine
+ * has no CUDA device, KNN_ERR_ARGS when the ordinal does not exist.  Serves the
+ * CLI's device check (main.cpp:53-70). */
+int knn_device_capability(int32_t device, int32_t* major, int32_t* minor);
+
 /* Context owning device scratch, stream and events on `device` (-1: current).
  * Returns NULL on failure (see knn_last_error). */
 knn_context* knn_context_create(int32_t device);
