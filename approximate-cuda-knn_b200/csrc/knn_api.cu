@@ -226,6 +226,8 @@ int run_trees(knn_context* C, const float* X, int64_t n, int d, int dpad, int tr
   a.seed = seed;
   int rc = C->get("perm", (size_t)trees * n, &a.perm);
   if (!rc) rc = C->get("perm_alt", (size_t)trees * n, &a.perm_alt);
+  if (!rc) rc = C->get("perm_inv", (size_t)trees * n, &a.inv);
+  if (!rc) rc = C->get("perm_node", (size_t)trees * n, &a.node);
   if (!rc) rc = C->get("keys", (size_t)trees * n, &a.keys);
   const size_t dir_nodes = depth > 0 ? ((size_t)1 << (depth - 1)) : 1;
   if (!rc) rc = C->get("dirs", (size_t)trees * dir_nodes * dpad, &a.dirs);

@@ -28,6 +28,8 @@ struct TreeArgs {
   uint64_t seed;
   int32_t* perm;      // [trees][n] out: leaf order
   int32_t* perm_alt;  // [trees][n] scratch
+  int32_t* inv;       // [trees][n] scratch: position of each point
+  int32_t* node;      // [trees][n] scratch: node of each point at the current level
   uint64_t* keys;     // [trees][n] scratch
   float* dirs;        // [trees][2^(depth-1)][dpad] scratch
   cudaStream_t stream;

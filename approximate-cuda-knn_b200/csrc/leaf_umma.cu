@@ -27,6 +27,8 @@
 //     whole block) with one ballot and one lane shift each.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "knn_internal.cuh"
 #include "knn_kernels.cuh"
 
@@ -40,7 +42,11 @@ constexpr int kChunkBytes = kBM * 128; // one 128 x 64 bf16 operand chunk
 constexpr uint32_t kTmemCols = 128;
 constexpr int kUThreads = 256;
 constexpr int kRound = 64;          // tile columns per epilogue round
-constexpr int kRS = kRound + 1;      // key-tile row stride
+// Round keys live in the B-operand region once the tile's MMA has completed:
+// 128 rows x 64 floats (32 KB), column index xor-swizzled by the row at 32-float
+// granularity so that row-parallel writes and column-parallel reads hit distinct banks.
+constexpr int kKsBytes = kBM * kRound * 4;
+__device__ __forceinline__ int ks_at(int r, int c) { return r * kRound + (c ^ (r & 31)); }
 constexpr int kLS = 33;              // list row stride (row owners hit distinct banks)
 // A 128x128x256 tile finishes in about a microsecond; 2^16 polls with 32 ns
 // sleeps (a few ms) is far beyond that, and keeps a failing launch short.
@@ -162,7 +168,7 @@ __device__ __forceinline__ void stage_operand(unsigned char* op, const __nv_bflo
 // and the tensor-memory loads follow the single-tile sequence that was checked
 // on its own against a CPU product.
 template <int METRIC>
-__global__ void __launch_bounds__(kUThreads, 1)
+__global__ void __launch_bounds__(kUThreads, 2)
     k_leaf_tc(const __nv_bfloat16* __restrict__ Xb, int Kp, int64_t n, int k, int kq, int depth,
               int qtiles, const int32_t* __restrict__ perm, const float* __restrict__ norms2,
               float* __restrict__ akey, uint32_t* __restrict__ aid, int* __restrict__ err) {
@@ -171,8 +177,9 @@ __global__ void __launch_bounds__(kUThreads, 1)
   const int nchunks = Kp / kKC;
   unsigned char* opA = smem;
   unsigned char* opB = opA + nchunks * kChunkBytes;
-  float* Ks = reinterpret_cast<float*>(opB + nchunks * kChunkBytes);  // [128][kRS] keys of one round
-  float* Lk = Ks + kBM * kRS;                                          // [128][kLS] list keys
+  const int bbytes = max(nchunks * kChunkBytes, kKsBytes);
+  float* Ks = reinterpret_cast<float*>(opB);                           // round keys (reuses B)
+  float* Lk = reinterpret_cast<float*>(opB + bbytes);                  // [128][kLS] list keys
   uint32_t* Li = reinterpret_cast<uint32_t*>(Lk + kBM * kLS);         // [128][kLS] list ids
   int32_t* qid = reinterpret_cast<int32_t*>(Li + kBM * kLS);
   int32_t* cid = qid + kBM;
@@ -290,7 +297,7 @@ __global__ void __launch_bounds__(kUThreads, 1)
                                                            : __fsub_rn(1.f, dot);
           // only keys that can still enter the row's list survive
           const bool s = rv && c < mc && cid[c] != myid && cand_less(key, (uint32_t)cid[c], tk, ti);
-          Ks[r * kRS + half * 32 + j] = s ? key : kInf;
+          Ks[ks_at(r, half * 32 + j)] = s ? key : kInf;
           survivors += s ? 1 : 0;
         }
         if (survivors) atomicAdd(&cnt[r], survivors);
@@ -305,7 +312,7 @@ __global__ void __launch_bounds__(kUThreads, 1)
         float lk = Lk[qq * kLS + lane];
         uint32_t li = Li[qq * kLS + lane];
         for (int cb = 0; cb < kRound; cb += 32) {
-          const float ck = Ks[qq * kRS + cb + lane];
+          const float ck = Ks[ks_at(qq, cb + lane)];
           const int c = rb + cb + lane;
           const uint32_t ci = c < mc ? (uint32_t)cid[c] : kNoId;
           uint32_t bal = __ballot_sync(0xFFFFFFFFu, ck < kInf);
@@ -437,8 +444,9 @@ __global__ void __launch_bounds__(256) k_rerank(const float* __restrict__ X, int
 }
 
 size_t umma_smem_bytes(int Kp) {
-  // alignment slack + A + B + round keys + lists + (qid, cid, qn, cn) + cnt + barrier words
-  return 1024 + 2 * (size_t)(Kp / kKC) * kChunkBytes + (size_t)kBM * kRS * 4 + (size_t)kBM * kLS * 8 +
+  // alignment slack + A + B (also the round keys) + lists + (qid, cid, qn, cn) + cnt + barrier words
+  const size_t bbytes = std::max((size_t)(Kp / kKC) * kChunkBytes, (size_t)kKsBytes);
+  return 1024 + (size_t)(Kp / kKC) * kChunkBytes + bbytes + (size_t)kBM * kLS * 8 +
          (size_t)(kBM + kBN) * 8 + (size_t)kBM * 4 + 64;
 }
 

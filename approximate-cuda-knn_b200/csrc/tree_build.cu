@@ -49,31 +49,36 @@ __global__ void k_directions(const float* __restrict__ X, int dpad, int64_t n, i
   }
 }
 
-// Keys of every (tree, position): (orderable projection << 32) | id.
+// Keys of every (tree, position): (orderable projection << 32) | id, computed
+// point-major: a group of G lanes takes one point, reads its row once (the
+// re-reads for the other trees hit L1) and projects it on the direction of the
+// node it occupies in each tree (recorded by the previous level's split).  The
+// rows thus cross HBM once per level instead of once per tree and level; the
+// directions (a few MB per level) come from L2.
 template <int G>
 __global__ void __launch_bounds__(256) k_project(const float* __restrict__ X, int dpad, int64_t n,
                                                  int level, int trees,
-                                                 const int32_t* __restrict__ perm,
+                                                 const int32_t* __restrict__ inv,
+                                                 const int32_t* __restrict__ node,
                                                  const float* __restrict__ dirs,
                                                  uint64_t* __restrict__ keys) {
   const int64_t nodes = int64_t(1) << level;
-  const int64_t total = (int64_t)trees * n;
   constexpr int PER_WARP = 32 / G;
   const int lane = threadIdx.x & 31;
   const int gl = lane % G;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * PER_WARP;
-       base < total; base += warps * PER_WARP) {
-    const int64_t gi = base + lane / G;
-    const bool valid = gi < total;
-    const int64_t g = valid ? gi : total - 1;
-    const int t = (int)(g / n);
-    const int64_t p = g - (int64_t)t * n;
-    const int64_t j = node_of(n, level, p);
-    const int32_t id = perm[g];
-    const float proj = group_project<G>(X + (size_t)id * dpad,
-                                        dirs + ((size_t)t * nodes + j) * dpad, dpad, gl);
-    if (valid && gl == 0) keys[g] = proj_key(proj, (uint32_t)id);
+       base < n; base += warps * PER_WARP) {
+    const int64_t i0 = base + lane / G;
+    const bool valid = i0 < n;
+    const int64_t i = valid ? i0 : n - 1;
+    const float* row = X + (size_t)i * dpad;
+    for (int t = 0; t < trees; ++t) {
+      const int64_t p = inv[(size_t)t * n + i];
+      const int64_t j = node[(size_t)t * n + i];
+      const float proj = group_project<G>(row, dirs + ((size_t)t * nodes + j) * dpad, dpad, gl);
+      if (valid && gl == 0) keys[(size_t)t * n + p] = proj_key(proj, (uint32_t)i);
+    }
   }
 }
 
@@ -171,12 +176,15 @@ __device__ __forceinline__ int64_t block_excl_scan(int64_t v, int64_t* warp_sums
 }
 
 // One block per (tree, node) of `level`: median select + stable partition of
-// the node's positions into perm_out.  SMEM_KEYS: node keys staged in shared
+// the node's positions into perm_out, keeping the inverse permutation `inv`
+// (point id -> position) and each point's node of the next level current.  SMEM_KEYS: node keys staged in shared
 // memory (count <= kSplitSmemKeys).
 template <bool SMEM_KEYS>
 __global__ void __launch_bounds__(1024) k_split(int64_t n, int level, const uint64_t* __restrict__ keys,
                                                 const int32_t* __restrict__ perm,
-                                                int32_t* __restrict__ perm_out) {
+                                                int32_t* __restrict__ perm_out,
+                                                int32_t* __restrict__ inv,
+                                                int32_t* __restrict__ node) {
   extern __shared__ uint64_t dyn_keys[];
   __shared__ uint32_t hist[256];
   __shared__ uint64_t sh[4];
@@ -192,7 +200,11 @@ __global__ void __launch_bounds__(1024) k_split(int64_t n, int level, const uint
   const int32_t* Pin = perm + (size_t)t * n + lo;
   int32_t* Pout = perm_out + (size_t)t * n + lo;
   if (cnt < 2 || nl <= 0 || nl >= cnt) {
-    for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) Pout[i] = Pin[i];
+    for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+      const int32_t id = Pin[i];
+      Pout[i] = id;
+      node[(size_t)t * n + id] = (int32_t)(lo + i < mid ? 2 * j : 2 * j + 1);
+    }
     return;
   }
   const uint64_t* KS = K;
@@ -223,7 +235,12 @@ __global__ void __launch_bounds__(1024) k_split(int64_t n, int level, const uint
       const int64_t p = p0 + e;
       if (p < cnt) {
         const int64_t dst = f[e] ? before : nl + (p - before);
-        if (dst >= 0 && dst < cnt) Pout[dst] = Pin[p];  // exactly nl keys are below the pivot
+        if (dst >= 0 && dst < cnt) {  // exactly nl keys are below the pivot
+          const int32_t id = Pin[p];
+          Pout[dst] = id;
+          inv[(size_t)t * n + id] = (int32_t)(lo + dst);
+          node[(size_t)t * n + id] = (int32_t)(f[e] ? 2 * j : 2 * j + 1);
+        }
         before += f[e];
       }
     }
@@ -246,7 +263,9 @@ int tree_build(const TreeArgs& a, LaunchLog& log) {
   }
   // identity order for every tree
   k_iota<<<(unsigned)((a.trees * n + 255) / 256), 256, 0, st>>>(a.perm, n, a.trees);
-  log.add();
+  k_iota<<<(unsigned)((a.trees * n + 255) / 256), 256, 0, st>>>(a.inv, n, a.trees);
+  cudaMemsetAsync(a.node, 0, sizeof(int32_t) * (size_t)a.trees * n, st);  // all in the root
+  log.add(2);
   int32_t* cur = a.perm;
   int32_t* alt = a.perm_alt;
   const int G = proj_group(a.d);
@@ -255,17 +274,16 @@ int tree_build(const TreeArgs& a, LaunchLog& log) {
     const int64_t segs = nodes * a.trees;
     k_directions<<<(unsigned)((segs + 7) / 8), 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur,
                                                              a.dirs, a.seed);
-    const int64_t total = (int64_t)a.trees * n;
     const int per_block = 8 * (32 / G);
-    int64_t blocks = (total + per_block - 1) / per_block;
+    int64_t blocks = (n + per_block - 1) / per_block;
     if (blocks > 148LL * 64) blocks = 148LL * 64;
     switch (G) {
-      case 1: k_project<1><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur, a.dirs, a.keys); break;
-      case 2: k_project<2><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur, a.dirs, a.keys); break;
-      case 4: k_project<4><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur, a.dirs, a.keys); break;
-      case 8: k_project<8><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur, a.dirs, a.keys); break;
-      case 16: k_project<16><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur, a.dirs, a.keys); break;
-      default: k_project<32><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur, a.dirs, a.keys); break;
+      case 1: k_project<1><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, a.inv, a.node, a.dirs, a.keys); break;
+      case 2: k_project<2><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, a.inv, a.node, a.dirs, a.keys); break;
+      case 4: k_project<4><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, a.inv, a.node, a.dirs, a.keys); break;
+      case 8: k_project<8><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, a.inv, a.node, a.dirs, a.keys); break;
+      case 16: k_project<16><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, a.inv, a.node, a.dirs, a.keys); break;
+      default: k_project<32><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, a.inv, a.node, a.dirs, a.keys); break;
     }
     const int64_t maxcnt = (n + nodes - 1) / nodes;
     int threads = (int)((maxcnt + 3) / 4);
@@ -273,9 +291,9 @@ int tree_build(const TreeArgs& a, LaunchLog& log) {
     if (threads < 64) threads = 64;
     if (threads > 1024) threads = 1024;
     if (maxcnt <= kSplitSmemKeys) {
-      k_split<true><<<(unsigned)segs, threads, (size_t)maxcnt * sizeof(uint64_t), st>>>(n, l, a.keys, cur, alt);
+      k_split<true><<<(unsigned)segs, threads, (size_t)maxcnt * sizeof(uint64_t), st>>>(n, l, a.keys, cur, alt, a.inv, a.node);
     } else {
-      k_split<false><<<(unsigned)segs, threads, 0, st>>>(n, l, a.keys, cur, alt);
+      k_split<false><<<(unsigned)segs, threads, 0, st>>>(n, l, a.keys, cur, alt, a.inv, a.node);
     }
     log.add(3);
     int32_t* tmp = cur;
