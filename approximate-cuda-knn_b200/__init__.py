@@ -64,7 +64,9 @@ class KnnOptions(ctypes.Structure):
         ("timing", ctypes.c_int32),
         ("ld", ctypes.c_int64),
         ("stream", ctypes.c_void_p),
-        ("reserved", ctypes.c_int32 * 8),
+        ("mlp_sample", ctypes.c_int32),
+        ("mlp_steps", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 6),
     ]
 
 
@@ -83,14 +85,16 @@ class KnnStats(ctypes.Structure):
         ("leaf_pairs", ctypes.c_int64),
         ("prop_candidates", ctypes.c_int64 * MAX_PROPS),
         ("ms_prop_iter", ctypes.c_float * MAX_PROPS),
-        ("reserved", ctypes.c_int64 * 8),
+        ("ms_learn", ctypes.c_float),
+        ("reserved_pad", ctypes.c_int32),
+        ("reserved", ctypes.c_int64 * 7),
     ]
 
     def as_dict(self) -> dict:
         n = self.props_run
         return {
             "depth": self.depth, "ms_total": self.ms_total, "ms_upload": self.ms_upload,
-            "ms_trees": self.ms_trees, "ms_leaf": self.ms_leaf,
+            "ms_learn": self.ms_learn, "ms_trees": self.ms_trees, "ms_leaf": self.ms_leaf,
             "ms_propagate": self.ms_propagate, "ms_download": self.ms_download,
             "launches": self.launches, "leaf_pairs": self.leaf_pairs,
             "prop_candidates": [self.prop_candidates[i] for i in range(n)],
@@ -119,6 +123,10 @@ EXPORTS = {
     "knn_exact_fp64": (ctypes.c_int, [_P, _P, _I64, _I32, _I32, _I32, _P, _I64, _P, _P, _P]),
     "knn_normalize_reference": (ctypes.c_int, [_P, _I64, _I32]),
     "knn_exact_fp64_noalloc": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _P, _I64, _P, _P, _P]),
+    "knn_mlp_param_count": (_I64, [_I32]),
+    "knn_mlp_loss_grad": (ctypes.c_int, [_P, _I32, _P, _I32, ctypes.c_float, _P, _P]),
+    "knn_mlp_train": (ctypes.c_int, [_P, _P, _I64, _I32, _I32, _I32, _U64, _P, _P, _P, _P, _P]),
+    "knn_mlp_embed": (ctypes.c_int, [_P, _P, _I64, _I32, _I32, _P, _P, _P, _P, _P]),
 }
 
 _lib_handle = None
@@ -172,18 +180,21 @@ def default_options(**kw) -> KnnOptions:
 
 def knn_build(points, k: int, trees: int, leaf: int, props: int, metric: int = 0,
               seed: int = 0, precision: int = PREC_FP32, learned: bool = False,
-              stats: bool = False, context=None):
+              stats: bool = False, context=None, mlp_sample: int = 0, mlp_steps: int = 0):
     """k-NN graph of ``points`` ([n, d] float32/float16, host memory).
 
-    Returns ``(idx int32 [n, k], dist float32 [n, k])`` sorted by (distance,
-    index), plus a stats dict when ``stats``."""
+    ``learned`` builds the trees on the learned split network's embedding
+    (trained on a sample of ``mlp_sample`` points for ``mlp_steps`` steps; 0
+    picks the library default).  Returns ``(idx int32 [n, k], dist float32
+    [n, k])`` sorted by (distance, index), plus a stats dict when ``stats``."""
     x = _points(points)
     n, d = x.shape
     lib = load_library()
     idx = np.empty((n, k), dtype=np.int32)
     dist = np.empty((n, k), dtype=np.float32)
     opt = default_options(dtype=F16 if x.dtype == np.float16 else F32, precision=precision,
-                          learned_splits=int(bool(learned)))
+                          learned_splits=int(bool(learned)), mlp_sample=mlp_sample,
+                          mlp_steps=mlp_steps)
     st = KnnStats()
     st.struct_size = ctypes.sizeof(KnnStats)
     rc = lib.knn_build_ex(context, _ptr(x), n, d, k, trees, leaf, props, metric, seed,
@@ -238,6 +249,61 @@ def exact_fp64(points, k: int, queries, metric: int = 0):
     _check(load_library().knn_exact_fp64(None, _ptr(x), n, d, k, metric, _ptr(q), q.shape[0],
                                          _ptr(idx), _ptr(dist), None))
     return idx, dist
+
+
+MLP_HIDDEN, MLP_EMBED = 256, 64
+
+
+def mlp_param_count(d: int) -> int:
+    """Length of the learned split network's parameter vector (W1, b1, W2, b2)."""
+    return int(load_library().knn_mlp_param_count(d))
+
+
+def mlp_loss_grad(params: np.ndarray, rows: np.ndarray, margin: float = 1.0):
+    """Mean triplet loss and gradient on the GPU for standardised rows
+    [3B, d] (anchors, positives, negatives): (loss, grad float32)."""
+    rows = np.ascontiguousarray(rows, dtype=np.float32)
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    d = rows.shape[1]
+    if rows.shape[0] % 3:
+        raise ValueError("rows must hold 3*batch rows")
+    grad = np.empty(mlp_param_count(d), dtype=np.float32)
+    loss = np.zeros(1, dtype=np.float32)
+    _check(load_library().knn_mlp_loss_grad(_ptr(params), d, _ptr(rows), rows.shape[0] // 3,
+                                            ctypes.c_float(margin), _ptr(grad), _ptr(loss)))
+    return float(loss[0]), grad
+
+
+def mlp_train(points, k: int, metric: int = 0, seed: int = 0, mlp_sample: int = 0,
+              mlp_steps: int = 0):
+    """Train the split network as a learned build would:
+    (params, mean, inv_std, loss_curve)."""
+    x = _points(points)
+    n, d = x.shape
+    steps = mlp_steps if mlp_steps > 0 else 300
+    params = np.empty(mlp_param_count(d), dtype=np.float32)
+    mean = np.empty(d, dtype=np.float32)
+    inv_std = np.empty(d, dtype=np.float32)
+    curve = np.empty(steps, dtype=np.float32)
+    opt = default_options(dtype=F16 if x.dtype == np.float16 else F32, mlp_sample=mlp_sample,
+                          mlp_steps=mlp_steps)
+    _check(load_library().knn_mlp_train(None, _ptr(x), n, d, k, metric, seed, ctypes.byref(opt),
+                                        _ptr(params), _ptr(mean), _ptr(inv_std), _ptr(curve)))
+    return params, mean, inv_std, curve
+
+
+def mlp_embed(points, params, mean, inv_std, metric: int = 0) -> np.ndarray:
+    """f(points) on the GPU, float32 [n, 64] (COSINE feeds the unit rows)."""
+    x = _points(points)
+    n, d = x.shape
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    mean = np.ascontiguousarray(mean, dtype=np.float32)
+    inv_std = np.ascontiguousarray(inv_std, dtype=np.float32)
+    out = np.empty((n, MLP_EMBED), dtype=np.float32)
+    opt = default_options(dtype=F16 if x.dtype == np.float16 else F32)
+    _check(load_library().knn_mlp_embed(None, _ptr(x), n, d, metric, _ptr(params), _ptr(mean),
+                                        _ptr(inv_std), ctypes.byref(opt), _ptr(out)))
+    return out
 
 
 def normalize_reference(points: np.ndarray) -> np.ndarray:

@@ -352,6 +352,110 @@ int run_prop(const float* X, int64_t n, int d, int dpad, int k, int metric, cons
   return KNN_OK;
 }
 
+// Learned split network (mlp.cu): the plain graph of a strided sample of the
+// points trains the MLP; the trees are then built on the embeddings of all
+// points.  Sample graph: 8 trees, leaf 128, 2 propagations, 2k neighbours (at
+// most 32), plain FP32.
+constexpr int kMlpSampleDefault = 65536;
+constexpr int kMlpStepsDefault = 300;
+constexpr int kMlpBatch = 1024;
+constexpr float kMlpLr = 1e-3f;
+constexpr float kMlpMargin = 1.0f;
+constexpr int kMlpGraphTrees = 8, kMlpGraphLeaf = 128, kMlpGraphProps = 2;
+constexpr int64_t kMlpEmbedChunk = 65536;
+constexpr uint64_t kMlpSeedSalt = 0x6C6561726E656421ull;
+
+struct Learned {
+  float* params = nullptr;
+  float* mean = nullptr;
+  float* inv_std = nullptr;
+  float* loss = nullptr;
+  int steps = 0;
+};
+
+int learn_network(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, int metric,
+                  uint64_t seed, const knn_options& o, cudaStream_t st, Learned* Lr, knn::LaunchLog& log) {
+  int64_t ns = o.mlp_sample > 0 ? o.mlp_sample : kMlpSampleDefault;
+  if (ns > n) ns = n;
+  int gk = 2 * k;
+  if (gk > 32) gk = 32;
+  if (gk < 2) gk = 2;
+  if (ns <= gk) return fail(KNN_ERR_ARGS, "learned splits: too few points for the training graph");
+  const int steps = o.mlp_steps > 0 ? o.mlp_steps : kMlpStepsDefault;
+  const uint64_t lseed = knn::splitmix64(seed ^ kMlpSeedSalt);
+
+  float* Xs = nullptr;
+  int rc = C->get("mlp_Xs", (size_t)ns * dpad, &Xs);
+  if (rc) return rc;
+  knn::launch_gather_sample(X, n, dpad, ns, Xs, st);
+  log.add();
+  float* norms = nullptr;
+  if (metric == KNN_METRIC_COSINE) {
+    rc = C->get("mlp_norms", (size_t)ns, &norms);
+    if (rc) return rc;
+    knn::launch_norms(Xs, ns, d, dpad, norms, st);
+    log.add();
+  }
+  Trees T;
+  rc = run_trees(C, Xs, ns, d, dpad, kMlpGraphTrees, kMlpGraphLeaf, lseed, st, &T, log);
+  if (rc) return rc;
+  Lists L;
+  rc = get_lists(C, ns, gk, &L);
+  if (!rc) rc = run_leaf(C, Xs, ns, d, dpad, gk, kMlpGraphTrees, T.depth, metric, T.perm, norms, &L, nullptr, st, log);
+  for (int p = 0; !rc && p < kMlpGraphProps; ++p)
+    rc = run_prop(Xs, ns, d, dpad, gk, metric, norms, T.perm, &L, true, nullptr, st, log);
+  if (rc) return rc;
+  int32_t* graph = nullptr;
+  float* gdist = nullptr;
+  rc = C->get("mlp_graph", (size_t)ns * gk, &graph);
+  if (!rc) rc = C->get("mlp_gdist", (size_t)ns * gk, &gdist);
+  if (rc) return rc;
+  knn::launch_finalize(L.key[L.cur], L.id[L.cur], ns, gk, metric, gdist, graph, st);
+  log.add();
+
+  knn::MlpTrainArgs a{};
+  a.Xs = Xs;
+  a.norms = norms;
+  a.ns = ns;
+  a.d = d;
+  a.dpad = dpad;
+  a.graph = graph;
+  a.gk = gk;
+  a.steps = steps;
+  a.batch = kMlpBatch;
+  a.lr = kMlpLr;
+  a.margin = kMlpMargin;
+  a.seed = lseed;
+  a.stream = st;
+  rc = C->get("mlp_params", knn::mlp_param_count(d), &a.params);
+  if (!rc) rc = C->get("mlp_mean", (size_t)d, &a.mean);
+  if (!rc) rc = C->get("mlp_inv_std", (size_t)d, &a.inv_std);
+  if (!rc) rc = C->get("mlp_loss", (size_t)steps, &a.loss);
+  if (!rc) rc = C->get("mlp_ws", knn::mlp_train_ws_floats(d, kMlpBatch), &a.ws);
+  if (rc) return rc;
+  rc = knn::mlp_train(a, log);
+  if (rc) return fail_cuda(cudaGetLastError(), "learned split training launch");
+  Lr->params = a.params;
+  Lr->mean = a.mean;
+  Lr->inv_std = a.inv_std;
+  Lr->loss = a.loss;
+  Lr->steps = steps;
+  return KNN_OK;
+}
+
+int embed_points(knn_context* C, const float* X, const float* norms, int64_t n, int d, int dpad,
+                 const float* params, const float* mean, const float* inv_std, cudaStream_t st, float** Z,
+                 knn::LaunchLog& log) {
+  float* ws = nullptr;
+  const int64_t chunk = n < kMlpEmbedChunk ? n : kMlpEmbedChunk;
+  int rc = C->get("mlp_Z", (size_t)n * knn::kMlpEmbed, Z);
+  if (!rc) rc = C->get("mlp_embed_ws", knn::mlp_embed_ws_floats(d, chunk), &ws);
+  if (rc) return rc;
+  rc = knn::mlp_embed(X, norms, n, d, dpad, params, mean, inv_std, ws, chunk, *Z, st, log);
+  if (rc) return fail_cuda(cudaGetLastError(), "learned split embedding launch");
+  return KNN_OK;
+}
+
 int resolve_options(const knn_options* opt, knn_options* o) {
   knn_default_options(o);
   if (opt) {
@@ -361,6 +465,8 @@ int resolve_options(const knn_options* opt, knn_options* o) {
   }
   if (o->dtype < 0 || o->dtype > 2) return fail(KNN_ERR_ARGS, "unknown dtype");
   if (o->precision < 0 || o->precision > 1) return fail(KNN_ERR_ARGS, "unknown precision mode");
+  if (o->learned_splits < 0 || o->learned_splits > 1) return fail(KNN_ERR_ARGS, "learned_splits must be 0 or 1");
+  if (o->mlp_sample < 0 || o->mlp_steps < 0) return fail(KNN_ERR_ARGS, "negative learned-split setting");
   return KNN_OK;
 }
 
@@ -401,7 +507,18 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
   if (timed) KNN_CK(cudaEventRecord(C->ev[1], st));
 
   Trees T;
-  rc = run_trees(C, P.X, n, d, P.dpad, trees, leaf, seed, st, &T, log);
+  if (o.learned_splits) {
+    // Trees on the learned 64-dim embedding; leaf and propagation on X.
+    Learned Lr;
+    rc = learn_network(C, P.X, n, d, P.dpad, k, metric, seed, o, st, &Lr, log);
+    float* Z = nullptr;
+    if (!rc) rc = embed_points(C, P.X, norms, n, d, P.dpad, Lr.params, Lr.mean, Lr.inv_std, st, &Z, log);
+    if (rc) return rc;
+    if (timed) KNN_CK(cudaEventRecord(C->ev[6], st));
+    rc = run_trees(C, Z, n, knn::kMlpEmbed, knn::kMlpEmbed, trees, leaf, seed, st, &T, log);
+  } else {
+    rc = run_trees(C, P.X, n, d, P.dpad, trees, leaf, seed, st, &T, log);
+  }
   if (rc) return rc;
   if (timed) KNN_CK(cudaEventRecord(C->ev[2], st));
 
@@ -466,7 +583,13 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
     stats->ms_total = ms;
     KNN_CK(cudaEventElapsedTime(&ms, C->ev[0], C->ev[1]));
     stats->ms_upload = ms;
-    KNN_CK(cudaEventElapsedTime(&ms, C->ev[1], C->ev[2]));
+    if (o.learned_splits) {
+      KNN_CK(cudaEventElapsedTime(&ms, C->ev[1], C->ev[6]));
+      stats->ms_learn = ms;
+      KNN_CK(cudaEventElapsedTime(&ms, C->ev[6], C->ev[2]));
+    } else {
+      KNN_CK(cudaEventElapsedTime(&ms, C->ev[1], C->ev[2]));
+    }
     stats->ms_trees = ms;
     KNN_CK(cudaEventElapsedTime(&ms, C->ev[2], C->ev[3]));
     stats->ms_leaf = ms;
@@ -561,7 +684,6 @@ int knn_build_ex(knn_context* ctx, const void* points, int64_t n, int32_t d, int
   if (props < 0 || props > KNN_MAX_PROPS) return fail(KNN_ERR_ARGS, "props out of range");
   if (stats && stats->struct_size != (int32_t)sizeof(knn_stats))
     return fail(KNN_ERR_ARGS, "knn_stats.struct_size mismatch");
-  if (o.learned_splits) return fail(KNN_ERR_UNSUPPORTED, "learned splits not available in this build");
   rc = enter_device(&ctx, o);
   if (rc) return rc;
   return build_impl(ctx, points, n, d, k, trees, leaf, props, metric, seed, out_idx, out_dist, o,
@@ -743,6 +865,110 @@ int knn_normalize_reference(float* points, int64_t n, int32_t d) {
   knn::launch_normalize_reference(X, n, d, st);
   KNN_CK(cudaPeekAtLastError());
   KNN_CK(cudaMemcpyAsync(points, X, sizeof(float) * (size_t)n * d, cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaStreamSynchronize(st));
+  return KNN_OK;
+}
+
+int64_t knn_mlp_param_count(int32_t d) {
+  if (d < 1) return fail(KNN_ERR_ARGS, "d must be >= 1");
+  return (int64_t)knn::mlp_param_count(d);
+}
+
+int knn_mlp_loss_grad(const float* params, int32_t d, const float* rows, int32_t batch, float margin,
+                      float* grad, float* loss) {
+  if (!params || !rows || !grad || !loss) return fail(KNN_ERR_ARGS, "NULL pointer");
+  if (d < 1 || batch < 1) return fail(KNN_ERR_ARGS, "d and batch must be >= 1");
+  knn_context* ctx = nullptr;
+  knn_options o;
+  knn_default_options(&o);
+  int rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  cudaStream_t st = ctx->stream;
+  knn::LaunchLog log;
+  const size_t np = knn::mlp_param_count(d);
+  const size_t nr = (size_t)3 * batch * d;
+  float *dp = nullptr, *dr = nullptr, *dg = nullptr, *ws = nullptr, *dl = nullptr;
+  rc = ctx->get("mlpg_params", np, &dp);
+  if (!rc) rc = ctx->get("mlpg_rows", nr, &dr);
+  if (!rc) rc = ctx->get("mlpg_grad", np, &dg);
+  if (!rc) rc = ctx->get("mlpg_ws", knn::mlp_fwd_bwd_ws_floats(d, batch), &ws);
+  if (!rc) rc = ctx->get("mlpg_loss", 1, &dl);
+  if (rc) return rc;
+  KNN_CK(cudaMemcpyAsync(dp, params, sizeof(float) * np, cudaMemcpyHostToDevice, st));
+  KNN_CK(cudaMemcpyAsync(dr, rows, sizeof(float) * nr, cudaMemcpyHostToDevice, st));
+  KNN_CK(cudaMemsetAsync(dl, 0, sizeof(float), st));
+  rc = knn::mlp_loss_grad(dp, d, dr, batch, margin, dg, ws, dl, st, log);
+  if (rc) return fail_cuda(cudaGetLastError(), "learned split gradient launch");
+  KNN_CK(cudaMemcpyAsync(grad, dg, sizeof(float) * np, cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaMemcpyAsync(loss, dl, sizeof(float), cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaStreamSynchronize(st));
+  return KNN_OK;
+}
+
+int knn_mlp_train(knn_context* ctx, const void* points, int64_t n, int32_t d, int32_t k, int32_t metric,
+                  uint64_t seed, const knn_options* opt, float* params, float* mean, float* inv_std,
+                  float* loss_curve) {
+  knn_options o;
+  int rc = resolve_options(opt, &o);
+  if (rc) return rc;
+  rc = check_common(points, n, d, k, metric);
+  if (rc) return rc;
+  if (!params || !mean || !inv_std) return fail(KNN_ERR_ARGS, "output pointer is NULL");
+  rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  cudaStream_t st = o.stream ? static_cast<cudaStream_t>(o.stream) : ctx->stream;
+  knn::LaunchLog log;
+  Prepared P;
+  rc = prepare_points(ctx, points, n, d, o, st, &P, log);
+  if (rc) return rc;
+  Learned Lr;
+  rc = learn_network(ctx, P.X, n, d, P.dpad, k, metric, seed, o, st, &Lr, log);
+  if (rc) return rc;
+  KNN_CK(cudaMemcpyAsync(params, Lr.params, sizeof(float) * knn::mlp_param_count(d), cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaMemcpyAsync(mean, Lr.mean, sizeof(float) * (size_t)d, cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaMemcpyAsync(inv_std, Lr.inv_std, sizeof(float) * (size_t)d, cudaMemcpyDeviceToHost, st));
+  if (loss_curve)
+    KNN_CK(cudaMemcpyAsync(loss_curve, Lr.loss, sizeof(float) * (size_t)Lr.steps, cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaStreamSynchronize(st));
+  return KNN_OK;
+}
+
+int knn_mlp_embed(knn_context* ctx, const void* points, int64_t n, int32_t d, int32_t metric,
+                  const float* params, const float* mean, const float* inv_std, const knn_options* opt,
+                  float* out) {
+  knn_options o;
+  int rc = resolve_options(opt, &o);
+  if (rc) return rc;
+  if (!points || !params || !mean || !inv_std || !out) return fail(KNN_ERR_ARGS, "NULL pointer");
+  if (n < 1 || n >= (int64_t)INT32_MAX || d < 1) return fail(KNN_ERR_ARGS, "size out of range");
+  if (metric < 0 || metric > 2) return fail(KNN_ERR_ARGS, "unknown metric");
+  rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  cudaStream_t st = o.stream ? static_cast<cudaStream_t>(o.stream) : ctx->stream;
+  knn::LaunchLog log;
+  Prepared P;
+  rc = prepare_points(ctx, points, n, d, o, st, &P, log);
+  if (rc) return rc;
+  const size_t np = knn::mlp_param_count(d);
+  float *dp = nullptr, *dm = nullptr, *ds = nullptr;
+  rc = ctx->get("mlpe_params", np, &dp);
+  if (!rc) rc = ctx->get("mlpe_mean", (size_t)d, &dm);
+  if (!rc) rc = ctx->get("mlpe_inv_std", (size_t)d, &ds);
+  if (rc) return rc;
+  KNN_CK(cudaMemcpyAsync(dp, params, sizeof(float) * np, cudaMemcpyHostToDevice, st));
+  KNN_CK(cudaMemcpyAsync(dm, mean, sizeof(float) * (size_t)d, cudaMemcpyHostToDevice, st));
+  KNN_CK(cudaMemcpyAsync(ds, inv_std, sizeof(float) * (size_t)d, cudaMemcpyHostToDevice, st));
+  float* norms = nullptr;
+  if (metric == KNN_METRIC_COSINE) {
+    rc = ctx->get("norms", (size_t)n, &norms);
+    if (rc) return rc;
+    knn::launch_norms(P.X, n, d, P.dpad, norms, st);
+  }
+  float* Z = nullptr;
+  rc = embed_points(ctx, P.X, norms, n, d, P.dpad, dp, dm, ds, st, &Z, log);
+  if (rc) return rc;
+  KNN_CK(cudaMemcpyAsync(out, Z, sizeof(float) * (size_t)n * knn::kMlpEmbed,
+                         o.outputs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
   KNN_CK(cudaStreamSynchronize(st));
   return KNN_OK;
 }

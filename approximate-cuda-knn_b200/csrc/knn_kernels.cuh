@@ -84,6 +84,42 @@ struct PropArgs {
 };
 int propagate_step(const PropArgs& a, LaunchLog& log);
 
+// Learned split network d -> kMlpHidden -> kMlpEmbed (mlp.cu).  Parameter
+// vector: W1 [H][d], b1 [H], W2 [E][H], b2 [E].
+constexpr int kMlpHidden = 256;
+constexpr int kMlpEmbed = 64;
+
+struct MlpTrainArgs {
+  const float* Xs;       // [ns][dpad] sample rows
+  const float* norms;    // [ns] row norms (COSINE: the input is the unit row) or null
+  int64_t ns;
+  int d, dpad;
+  const int32_t* graph;  // [ns][gk] k-NN graph of the sample (sample-local ids), rank order
+  int gk;
+  int steps, batch;      // Adam steps, triplets per step
+  float lr, margin;
+  uint64_t seed;
+  float* params;         // out: [mlp_param_count(d)]
+  float* mean;           // out: [d]
+  float* inv_std;        // out: [d]
+  float* loss;           // out: [steps] mean triplet loss per step
+  float* ws;             // [mlp_train_ws_floats(d, batch)]
+  cudaStream_t stream;
+};
+size_t mlp_param_count(int d);
+size_t mlp_fwd_bwd_ws_floats(int d, int B);
+size_t mlp_train_ws_floats(int d, int B);
+size_t mlp_embed_ws_floats(int d, int64_t chunk);
+int mlp_train(const MlpTrainArgs& a, LaunchLog& log);
+// Z [n][kMlpEmbed] = f(X) in chunks of `chunk` rows; norms [n] (COSINE) or null.
+int mlp_embed(const float* X, const float* norms, int64_t n, int d, int dpad, const float* params,
+              const float* mean, const float* inv_std, float* ws, int64_t chunk, float* Z, cudaStream_t st,
+              LaunchLog& log);
+// One forward + backward of the triplet loss over 3B standardised rows.
+int mlp_loss_grad(const float* params, int d, const float* rows, int B, float margin, float* grad, float* ws,
+                  float* loss, cudaStream_t st, LaunchLog& log);
+void launch_gather_sample(const float* X, int64_t n, int dpad, int64_t ns, float* Xs, cudaStream_t st);
+
 // Helpers (knn_misc.cu).
 void launch_init_lists(float* key, uint32_t* id, uint32_t* flags, int64_t n, int k, int kw,
                        cudaStream_t st);

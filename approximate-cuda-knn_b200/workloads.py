@@ -78,6 +78,25 @@ def normalized_mixture(seed: int = 0, n: int = 10_000_000, d: int = 96,
     return out
 
 
+def scaled_directions(seed: int = 0, n: int = 200_000, d: int = 64, clusters: int = 100,
+                      sigma: float = 0.3, scale_lo: float = 0.1, scale_hi: float = 10.0) -> np.ndarray:
+    """Rows of :func:`normalized_mixture` (float32) each multiplied by a
+    log-uniform scale in [scale_lo, scale_hi].  COSINE neighbours are those of
+    the unit rows, while raw-coordinate geometry is dominated by the scales."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    centres = rng.standard_normal((clusters, d), dtype=np.float32)
+    labels = rng.integers(0, clusters, size=n)
+    out = np.empty((n, d), dtype=np.float32)
+    lo, hi = math.log(scale_lo), math.log(scale_hi)
+    for s in range(0, n, _CHUNK):
+        e = min(n, s + _CHUNK)
+        x = centres[labels[s:e]] + np.float32(sigma) * rng.standard_normal((e - s, d), dtype=np.float32)
+        x /= np.linalg.norm(x, axis=1, keepdims=True)
+        x *= np.exp(rng.uniform(lo, hi, size=(e - s, 1))).astype(np.float32)
+        out[s:e] = x
+    return out
+
+
 def batch_dataset(seed: int) -> np.ndarray:
     """One member of the 256-dataset batch: N log-uniform in [1e3, 2e5],
     d uniform over {32, 64, 128, 256}, 16-cluster mixture (centres U[-10,10]^d,

@@ -72,7 +72,9 @@ typedef struct knn_options {
   int32_t timing;            /* 1: record per-stage device times in knn_stats         */
   int64_t ld;                /* row stride of `points` in elements; 0 means d         */
   void* stream;              /* cudaStream_t; NULL: the context's own stream          */
-  int32_t reserved[8];
+  int32_t mlp_sample;        /* learned splits: points in the training sample (0: 65536) */
+  int32_t mlp_steps;         /* learned splits: Adam steps (0: 300)                      */
+  int32_t reserved[6];
 } knn_options;
 
 typedef struct knn_stats {
@@ -89,7 +91,9 @@ typedef struct knn_stats {
   int64_t leaf_pairs;        /* (query, candidate) keys evaluated by the leaf stage     */
   int64_t prop_candidates[KNN_MAX_PROPS]; /* keys evaluated per propagation iteration  */
   float ms_prop_iter[KNN_MAX_PROPS];      /* device time per propagation iteration     */
-  int64_t reserved[8];
+  float ms_learn;            /* learned splits: sample graph, training and embedding    */
+  int32_t reserved_pad;
+  int64_t reserved[7];
 } knn_stats;
 
 typedef struct knn_context knn_context;
@@ -202,6 +206,45 @@ int knn_exact_fp64_noalloc(const float* points, int64_t n, int32_t d, int32_t k,
  * the reference).  Used by the CLI only; knn_build never normalises.
  */
 int knn_normalize_reference(float* points, int64_t n, int32_t d);
+
+/*
+ * Learned split network (options.learned_splits = 1).  No counterpart in the
+ * reference, whose split directions are differences of raw points
+ * (euclideandistancematrixgpu.cu:2138-2164).
+ *
+ *   f(x) = W2 gelu(W1 s(x) + b1) + b2,  s(x) = (u(x) - mean) * inv_std,
+ *   u(x) = x/|x| for COSINE (a zero row stays zero), else x,
+ *   gelu(a) = 0.5 a (1 + tanh(sqrt(2/pi) (a + 0.044715 a^3))),
+ *   W1 [256][d], b1 [256], W2 [64][256], b2 [64]; the parameter vector is
+ *   W1, b1, W2, b2 in that order, float32, knn_mlp_param_count(d) values.
+ *
+ * Training: the plain method builds a k-NN graph (2k neighbours, at most 32)
+ * of a strided sample of options.mlp_sample points; each Adam step takes 1024
+ * triplets (anchor, a graph neighbour of rank < k', a random point or a
+ * neighbour of rank >= k', k' = half the graph width) and minimises
+ *   mean max(0, margin + |f(a) - f(p)|^2 - |f(a) - f(n)|^2),  margin 1.
+ * knn_build_ex then builds the trees on the 64-dim embeddings f(x) (split
+ * directions f(x_p2) - f(x_p1)); leaf blocks and propagation rank the
+ * original points as before.
+ */
+#define KNN_MLP_HIDDEN 256
+#define KNN_MLP_EMBED 64
+int64_t knn_mlp_param_count(int32_t d);
+/* Mean triplet loss and its gradient for one batch: rows host float32
+ * [3*batch][d], already standardised, anchors then positives then negatives;
+ * grad host float32 [knn_mlp_param_count(d)]; loss host float32 [1]. */
+int knn_mlp_loss_grad(const float* params, int32_t d, const float* rows, int32_t batch, float margin,
+                      float* grad, float* loss);
+/* Train the network as knn_build_ex does for these points (host outputs:
+ * params, mean [d], inv_std [d], loss_curve [steps] or NULL). */
+int knn_mlp_train(knn_context* ctx, const void* points, int64_t n, int32_t d, int32_t k, int32_t metric,
+                  uint64_t seed, const knn_options* opt, float* params, float* mean, float* inv_std,
+                  float* loss_curve);
+/* out [n][64] = f(points) (host, or device with options.outputs_on_device);
+ * for KNN_METRIC_COSINE the network input is the unit row x/|x|. */
+int knn_mlp_embed(knn_context* ctx, const void* points, int64_t n, int32_t d, int32_t metric,
+                  const float* params, const float* mean, const float* inv_std, const knn_options* opt,
+                  float* out);
 
 #ifdef __cplusplus
 }

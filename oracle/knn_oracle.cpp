@@ -7,7 +7,10 @@
 //   points -> random-projection trees -> leaf-block all-pairs k-NN
 //          -> neighbour-of-neighbour propagation (Jacobi) -> k-NN graph
 //
-// plus an FP64 exact brute-force k-NN used as the recall / distance-error judge.
+// plus an FP64 exact brute-force k-NN used as the recall / distance-error judge,
+// and the learned split network's forward pass and triplet-loss gradient in
+// FP64 (no reference counterpart; the tests pin it by central finite
+// differences, then use it as the judge of the GPU backward kernels).
 //
 // Parity: the reference ships no tests, golden vectors or fixtures, and its GPU
 // output is non-deterministic (atomic scatter order, atomic tie fill, unstable
@@ -481,6 +484,116 @@ int oracle_pair_dist_fp64(const float* X, int64_t n, int32_t d, int32_t metric,
       s = den == 0.0 ? 1.0 : 1.0 - s / den;
     }
     out[p] = s;
+  }
+  return 0;
+}
+
+// ---- learned split network, FP64 -------------------------------------------
+// f(x) = W2 gelu(W1 x + b1) + b2 on already-standardised rows x [d];
+// params = W1 [256][d], b1 [256], W2 [64][256], b2 [64].
+static const int kOH = 256, kOE = 64;
+
+static double o_gelu(double a) {
+  const double c = 0.7978845608028654, u = c * (a + 0.044715 * a * a * a);
+  return 0.5 * a * (1.0 + std::tanh(u));
+}
+static double o_gelu_grad(double a) {
+  const double c = 0.7978845608028654, u = c * (a + 0.044715 * a * a * a), t = std::tanh(u);
+  return 0.5 * (1.0 + t) + 0.5 * a * (1.0 - t * t) * c * (1.0 + 3.0 * 0.044715 * a * a);
+}
+
+// Z [m][64] = f(rows) for m rows [m][d].
+int oracle_mlp_forward(const float* params, int32_t d, const float* rows, int64_t m, double* Z) {
+  const float* W1 = params;
+  const float* b1 = W1 + (size_t)kOH * d;
+  const float* W2 = b1 + kOH;
+  const float* b2 = W2 + (size_t)kOE * kOH;
+  std::vector<double> g(kOH);
+  for (int64_t r = 0; r < m; ++r) {
+    const float* x = rows + r * d;
+    for (int h = 0; h < kOH; ++h) {
+      double a = b1[h];
+      for (int c = 0; c < d; ++c) a += (double)W1[(size_t)h * d + c] * x[c];
+      g[h] = o_gelu(a);
+    }
+    for (int e = 0; e < kOE; ++e) {
+      double z = b2[e];
+      for (int h = 0; h < kOH; ++h) z += (double)W2[(size_t)e * kOH + h] * g[h];
+      Z[r * kOE + e] = z;
+    }
+  }
+  return 0;
+}
+
+// Mean triplet loss over B triplets of rows [3B][d] (anchors, positives,
+// negatives) and its gradient with respect to params.
+int oracle_mlp_loss_grad(const float* params, int32_t d, const float* rows, int32_t B, double margin,
+                         double* grad, double* loss, double* hinge) {
+  const float* W1 = params;
+  const float* W2 = W1 + (size_t)kOH * d + kOH;
+  const size_t np = (size_t)kOH * d + kOH + (size_t)kOE * kOH + kOE;
+  double* gW1 = grad;
+  double* gb1 = gW1 + (size_t)kOH * d;
+  double* gW2 = gb1 + kOH;
+  double* gb2 = gW2 + (size_t)kOE * kOH;
+  std::fill(grad, grad + np, 0.0);
+  const int R = 3 * B;
+  std::vector<double> A((size_t)R * kOH), G((size_t)R * kOH), Z((size_t)R * kOE), dZ((size_t)R * kOE, 0.0);
+  const float* b1 = W1 + (size_t)kOH * d;
+  const float* b2 = W2 + (size_t)kOE * kOH;
+  for (int r = 0; r < R; ++r) {
+    const float* x = rows + (size_t)r * d;
+    for (int h = 0; h < kOH; ++h) {
+      double a = b1[h];
+      for (int c = 0; c < d; ++c) a += (double)W1[(size_t)h * d + c] * x[c];
+      A[(size_t)r * kOH + h] = a;
+      G[(size_t)r * kOH + h] = o_gelu(a);
+    }
+    for (int e = 0; e < kOE; ++e) {
+      double z = b2[e];
+      for (int h = 0; h < kOH; ++h) z += (double)W2[(size_t)e * kOH + h] * G[(size_t)r * kOH + h];
+      Z[(size_t)r * kOE + e] = z;
+    }
+  }
+  double L = 0.0;
+  for (int b = 0; b < B; ++b) {
+    const double* za = &Z[(size_t)b * kOE];
+    const double* zp = &Z[(size_t)(B + b) * kOE];
+    const double* zn = &Z[(size_t)(2 * B + b) * kOE];
+    double dap = 0, dan = 0;
+    for (int e = 0; e < kOE; ++e) {
+      dap += (za[e] - zp[e]) * (za[e] - zp[e]);
+      dan += (za[e] - zn[e]) * (za[e] - zn[e]);
+    }
+    const double l = margin + dap - dan;
+    if (hinge) hinge[b] = l;
+    if (l <= 0) continue;
+    L += l / B;
+    const double s = 2.0 / B;
+    for (int e = 0; e < kOE; ++e) {
+      const double u = za[e] - zp[e], w = za[e] - zn[e];
+      dZ[(size_t)b * kOE + e] += s * (u - w);
+      dZ[(size_t)(B + b) * kOE + e] += -s * u;
+      dZ[(size_t)(2 * B + b) * kOE + e] += s * w;
+    }
+  }
+  *loss = L;
+  std::vector<double> dA(kOH);
+  for (int r = 0; r < R; ++r) {
+    const double* dz = &dZ[(size_t)r * kOE];
+    for (int e = 0; e < kOE; ++e) {
+      gb2[e] += dz[e];
+      for (int h = 0; h < kOH; ++h) gW2[(size_t)e * kOH + h] += dz[e] * G[(size_t)r * kOH + h];
+    }
+    for (int h = 0; h < kOH; ++h) {
+      double s = 0;
+      for (int e = 0; e < kOE; ++e) s += dz[e] * W2[(size_t)e * kOH + h];
+      dA[h] = s * o_gelu_grad(A[(size_t)r * kOH + h]);
+      gb1[h] += dA[h];
+    }
+    const float* x = rows + (size_t)r * d;
+    for (int h = 0; h < kOH; ++h)
+      for (int c = 0; c < d; ++c) gW1[(size_t)h * d + c] += dA[h] * x[c];
   }
   return 0;
 }

@@ -50,6 +50,8 @@ class Oracle:
             "oracle_knn_build": (ctypes.c_int, [P, I64, I32, I32, I32, I32, I32, I32, U64, P, P, I32]),
             "oracle_exact_knn": (ctypes.c_int, [P, I64, I32, I32, I32, P, I64, P, P, I32]),
             "oracle_pair_dist_fp64": (ctypes.c_int, [P, I64, I32, I32, P, P, I64, P]),
+            "oracle_mlp_forward": (ctypes.c_int, [P, I32, P, I64, P]),
+            "oracle_mlp_loss_grad": (ctypes.c_int, [P, I32, P, I32, ctypes.c_double, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -132,6 +134,28 @@ class Oracle:
         x = self._x(x)
         v = self._x(v)
         return self.lib.oracle_project(x.ctypes.data, v.ctypes.data, x.shape[0])
+
+    def mlp_forward(self, params, rows):
+        """FP64 f(rows) of the learned split network: [m, 64]."""
+        p = self._x(params)
+        r = self._x(rows)
+        z = np.empty((r.shape[0], 64), dtype=np.float64)
+        assert self.lib.oracle_mlp_forward(p.ctypes.data, r.shape[1], r.ctypes.data, r.shape[0],
+                                           z.ctypes.data) == 0
+        return z
+
+    def mlp_loss_grad(self, params, rows, margin=1.0):
+        """FP64 (loss, grad, per-triplet hinge argument) of the triplet loss."""
+        p = self._x(params)
+        r = self._x(rows)
+        b = r.shape[0] // 3
+        grad = np.empty(p.shape[0], dtype=np.float64)
+        loss = np.zeros(1, dtype=np.float64)
+        hinge = np.empty(b, dtype=np.float64)
+        assert self.lib.oracle_mlp_loss_grad(p.ctypes.data, r.shape[1], r.ctypes.data, b, margin,
+                                             grad.ctypes.data, loss.ctypes.data,
+                                             hinge.ctypes.data) == 0
+        return float(loss[0]), grad, hinge
 
 
 @pytest.fixture(scope="session")
