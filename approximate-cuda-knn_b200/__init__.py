@@ -101,6 +101,18 @@ class KnnStats(ctypes.Structure):
         }
 
 
+class KnnDataset(ctypes.Structure):
+    _fields_ = [
+        ("points", ctypes.c_void_p),
+        ("n", ctypes.c_int64),
+        ("d", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("seed", ctypes.c_uint64),
+        ("out_idx", ctypes.c_void_p),
+        ("out_dist", ctypes.c_void_p),
+    ]
+
+
 _P = ctypes.c_void_p
 _I32, _I64, _U64 = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64
 
@@ -123,6 +135,7 @@ EXPORTS = {
     "knn_exact_fp64": (ctypes.c_int, [_P, _P, _I64, _I32, _I32, _I32, _P, _I64, _P, _P, _P]),
     "knn_normalize_reference": (ctypes.c_int, [_P, _I64, _I32]),
     "knn_exact_fp64_noalloc": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _P, _I64, _P, _P, _P]),
+    "knn_build_batch": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _I32, _I32, _I32, _P, _P]),
     "knn_mlp_param_count": (_I64, [_I32]),
     "knn_mlp_loss_grad": (ctypes.c_int, [_P, _I32, _P, _I32, ctypes.c_float, _P, _P]),
     "knn_mlp_train": (ctypes.c_int, [_P, _P, _I64, _I32, _I32, _I32, _U64, _P, _P, _P, _P, _P]),
@@ -202,6 +215,39 @@ def knn_build(points, k: int, trees: int, leaf: int, props: int, metric: int = 0
                           ctypes.byref(st) if stats else None)
     _check(rc)
     return (idx, dist, st.as_dict()) if stats else (idx, dist)
+
+
+def knn_build_batch(datasets, k: int, trees: int, leaf: int, props: int, metric: int = 0,
+                    seeds=None, precision: int = PREC_FP32, stats: bool = False, context=None):
+    """k-NN graphs of many independent point sets in one call.
+
+    ``datasets``: sequence of [n_i, d_i] arrays (all float32 or all float16);
+    ``seeds``: one seed per set (default 0).  Returns a list of ``(idx, dist)``
+    per set (ids local to the set), plus a stats dict when ``stats``."""
+    xs = [_points(x) for x in datasets]
+    if len({x.dtype for x in xs}) > 1:
+        raise ValueError("all datasets must share one element type")
+    seeds = [0] * len(xs) if seeds is None else list(seeds)
+    outs = []
+    arr = (KnnDataset * max(1, len(xs)))()
+    for i, x in enumerate(xs):
+        n, d = x.shape
+        idx = np.empty((n, k), dtype=np.int32)
+        dist = np.empty((n, k), dtype=np.float32)
+        outs.append((idx, dist))
+        arr[i].points = _ptr(x)
+        arr[i].n = n
+        arr[i].d = d
+        arr[i].seed = int(seeds[i])
+        arr[i].out_idx = _ptr(idx)
+        arr[i].out_dist = _ptr(dist)
+    f16 = bool(xs) and xs[0].dtype == np.float16
+    opt = default_options(dtype=F16 if f16 else F32, precision=precision)
+    st = KnnStats()
+    st.struct_size = ctypes.sizeof(KnnStats)
+    _check(load_library().knn_build_batch(context, arr, len(xs), k, trees, leaf, props, metric,
+                                          ctypes.byref(opt), ctypes.byref(st) if stats else None))
+    return (outs, st.as_dict()) if stats else outs
 
 
 def build_trees(points, trees: int, leaf: int, seed: int = 0) -> np.ndarray:

@@ -13,6 +13,8 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <vector>
+#include <algorithm>
 
 #include "knn_internal.cuh"
 #include "knn_kernels.cuh"
@@ -60,6 +62,17 @@ struct knn_context {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[8] = {};
   std::map<std::string, Buffer> bufs;
+  // Bumped whenever a buffer moves: captured graphs of older generations hold
+  // stale pointers and are not replayed.
+  uint64_t generation = 0;
+  // Captured batch pipelines by shape signature (see knn_build_batch).
+  struct Captured {
+    std::string sig;
+    uint64_t generation;
+    cudaGraphExec_t exec;
+  };
+  std::vector<Captured> graphs;
+  std::vector<std::string> seen;
 
   // Device buffer `name` of at least `bytes`; grows by reallocation.
   int get(const char* name, size_t bytes, void** out) {
@@ -78,6 +91,7 @@ struct knn_context {
         return fail_cuda(e, (std::string("cudaMalloc ") + name).c_str());
       }
       b.bytes = bytes;
+      ++generation;
     }
     *out = b.p;
     return KNN_OK;
@@ -97,6 +111,7 @@ struct knn_context {
   ~knn_context() {
     int cur = 0;
     if (cudaGetDevice(&cur) == cudaSuccess && cur != device) cudaSetDevice(device);
+    for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
     for (auto& kv : bufs)
       if (kv.second.p) cudaFree(kv.second.p);
     for (auto& e : ev)
@@ -212,32 +227,45 @@ struct Trees {
   int depth = 0;
 };
 
-int run_trees(knn_context* C, const float* X, int64_t n, int d, int dpad, int trees, int leaf,
-              uint64_t seed, cudaStream_t st, Trees* T, knn::LaunchLog& log) {
-  const int depth = knn::tree_depth(n, leaf);
-  if (depth > 30) return fail(KNN_ERR_ARGS, "tree too deep (n / leaf too large)");
+// Trees of a batch of segments (global positions), or of one point set.
+int run_trees_segs(knn_context* C, const float* X, int64_t ntot, int d, int dpad, int trees,
+                   const knn::SegView& segs, const knn::SegEntry* hsegs, int nseg, cudaStream_t st,
+                   Trees* T, knn::LaunchLog& log) {
   knn::TreeArgs a{};
   a.X = X;
-  a.n = n;
+  a.n = ntot;
   a.d = d;
   a.dpad = dpad;
   a.trees = trees;
-  a.depth = depth;
-  a.seed = seed;
-  int rc = C->get("perm", (size_t)trees * n, &a.perm);
-  if (!rc) rc = C->get("perm_alt", (size_t)trees * n, &a.perm_alt);
-  if (!rc) rc = C->get("perm_inv", (size_t)trees * n, &a.inv);
-  if (!rc) rc = C->get("perm_node", (size_t)trees * n, &a.node);
-  if (!rc) rc = C->get("keys", (size_t)trees * n, &a.keys);
-  const size_t dir_nodes = depth > 0 ? ((size_t)1 << (depth - 1)) : 1;
-  if (!rc) rc = C->get("dirs", (size_t)trees * dir_nodes * dpad, &a.dirs);
+  a.segs = segs;
+  a.hsegs = hsegs;
+  a.nseg = nseg;
+  int rc = C->get("perm", (size_t)trees * ntot, &a.perm);
+  if (!rc) rc = C->get("perm_alt", (size_t)trees * ntot, &a.perm_alt);
+  if (!rc) rc = C->get("perm_inv", (size_t)trees * ntot, &a.inv);
+  if (!rc) rc = C->get("perm_node", (size_t)trees * ntot, &a.node);
+  if (!rc) rc = C->get("keys", (size_t)trees * ntot, &a.keys);
+  if (!rc) rc = C->get("dirs", knn::tree_dir_nodes(hsegs, nseg, trees) * dpad, &a.dirs);
   if (rc) return rc;
   a.stream = st;
   rc = knn::tree_build(a, log);
   if (rc) return fail_cuda(cudaGetLastError(), "tree build launch");
   T->perm = a.perm;
-  T->depth = depth;
+  T->depth = hsegs[0].depth;
   return KNN_OK;
+}
+
+int run_trees(knn_context* C, const float* X, int64_t n, int d, int dpad, int trees, int leaf,
+              uint64_t seed, cudaStream_t st, Trees* T, knn::LaunchLog& log) {
+  const int depth = knn::tree_depth(n, leaf);
+  if (depth > 30) return fail(KNN_ERR_ARGS, "tree too deep (n / leaf too large)");
+  knn::SegEntry e{};
+  e.off = 0;
+  e.n = n;
+  e.seed = seed;
+  e.leaf_base = 0;
+  e.depth = depth;
+  return run_trees_segs(C, X, n, d, dpad, trees, knn::single_segment(n, seed, depth), &e, 1, st, T, log);
 }
 
 struct Lists {
@@ -259,8 +287,22 @@ int get_lists(knn_context* C, int64_t n, int k, Lists* L) {
   return rc;
 }
 
+// Where the leaves of every tree lie: segments, leaf blocks per tree, largest leaf.
+struct Layout {
+  knn::SegView segs;
+  int64_t leaves = 1, maxleaf = 1;
+};
+
+Layout single_layout(int64_t n, int depth) {
+  Layout y;
+  y.segs = knn::single_segment(n, 0, depth);
+  y.leaves = int64_t(1) << depth;
+  y.maxleaf = (n + y.leaves - 1) / y.leaves;
+  return y;
+}
+
 int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, int trees,
-             int depth, int metric, const int32_t* perm, const float* norms, Lists* L,
+             const Layout& lay, int metric, const int32_t* perm, const float* norms, Lists* L,
              unsigned long long* counter, cudaStream_t st, knn::LaunchLog& log) {
   const int kw = (k + 31) / 32;
   knn::launch_init_lists(L->key[L->cur], L->id[L->cur], L->flags[L->cur], n, k, kw, st);
@@ -272,7 +314,8 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
   a.dpad = dpad;
   a.k = k;
   a.trees = trees;
-  a.depth = depth;
+  a.segs = lay.segs;
+  a.leaves = lay.leaves;
   a.metric = metric;
   a.perm = perm;
   a.norms = norms;
@@ -289,7 +332,7 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
 // Mixed precision: BF16 tensor-core tiles select each point's best min(2k, 32)
 // approximate candidates over all trees; FP32 re-rank keeps the exact best k.
 int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, int trees,
-                  int depth, int metric, const int32_t* perm, const float* norms, Lists* L,
+                  const Layout& lay, int metric, const int32_t* perm, const float* norms, Lists* L,
                   int* err_flag, cudaStream_t st, knn::LaunchLog& log) {
   const int kw = (k + 31) / 32;
   const int kq = k <= 16 ? 2 * k : 32;
@@ -302,7 +345,9 @@ int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, in
   a.k = k;
   a.kq = kq;
   a.trees = trees;
-  a.depth = depth;
+  a.segs = lay.segs;
+  a.leaves = lay.leaves;
+  a.maxleaf = lay.maxleaf;
   a.metric = metric;
   a.perm = perm;
   a.norms = norms;
@@ -401,7 +446,9 @@ int learn_network(knn_context* C, const float* X, int64_t n, int d, int dpad, in
   if (rc) return rc;
   Lists L;
   rc = get_lists(C, ns, gk, &L);
-  if (!rc) rc = run_leaf(C, Xs, ns, d, dpad, gk, kMlpGraphTrees, T.depth, metric, T.perm, norms, &L, nullptr, st, log);
+  if (!rc)
+    rc = run_leaf(C, Xs, ns, d, dpad, gk, kMlpGraphTrees, single_layout(ns, T.depth), metric, T.perm, norms, &L,
+                  nullptr, st, log);
   for (int p = 0; !rc && p < kMlpGraphProps; ++p)
     rc = run_prop(Xs, ns, d, dpad, gk, metric, norms, T.perm, &L, true, nullptr, st, log);
   if (rc) return rc;
@@ -532,10 +579,10 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
   const bool tensor_leaf = o.precision == KNN_PREC_BF16_RERANK && metric != KNN_METRIC_TAXICAB &&
                            d <= 256 && k <= 32;
   if (tensor_leaf) {
-    rc = run_leaf_umma(C, P.X, n, d, P.dpad, k, trees, T.depth, metric, T.perm, norms, &L,
+    rc = run_leaf_umma(C, P.X, n, d, P.dpad, k, trees, single_layout(n, T.depth), metric, T.perm, norms, &L,
                        err_flag, st, log);
   } else {
-    rc = run_leaf(C, P.X, n, d, P.dpad, k, trees, T.depth, metric, T.perm, norms, &L,
+    rc = run_leaf(C, P.X, n, d, P.dpad, k, trees, single_layout(n, T.depth), metric, T.perm, norms, &L,
                   stats ? counters : nullptr, st, log);
   }
   if (rc) return rc;
@@ -603,6 +650,242 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
     KNN_CK(cudaMemcpy(host, counters, sizeof(host), cudaMemcpyDeviceToHost));
     stats->leaf_pairs = (int64_t)host[0];
     for (int p = 0; p < props && p < KNN_MAX_PROPS; ++p) stats->prop_candidates[p] = (int64_t)host[2 + p];
+  }
+  return KNN_OK;
+}
+
+// ------------------------------------------------------------------ batch --
+// Rows of one point set into the concatenated float32 array (dst already
+// offset), zero padded to dpad.
+int upload_rows(knn_context* C, const void* src, int64_t n, int d, int dtype, bool on_device, float* dst,
+                int dpad, cudaStream_t st, knn::LaunchLog& log) {
+  if (on_device) {
+    knn::launch_pad_rows(src, dtype, n, d, d, dst, dpad, st);
+    log.add();
+    return KNN_OK;
+  }
+  if (dtype == KNN_F32) {
+    KNN_CK(cudaMemcpy2DAsync(dst, (size_t)dpad * 4, src, (size_t)d * 4, (size_t)d * 4, (size_t)n,
+                             cudaMemcpyHostToDevice, st));
+    if (dpad != d)
+      KNN_CK(cudaMemset2DAsync(dst + d, (size_t)dpad * 4, 0, (size_t)(dpad - d) * 4, (size_t)n, st));
+    return KNN_OK;
+  }
+  void* stage = nullptr;
+  int rc = C->get("stage", (size_t)n * d * 2, &stage);
+  if (rc) return rc;
+  KNN_CK(cudaMemcpyAsync(stage, src, (size_t)n * d * 2, cudaMemcpyHostToDevice, st));
+  knn::launch_pad_rows(stage, dtype, n, d, d, dst, dpad, st);
+  log.add();
+  return KNN_OK;
+}
+
+// One group of datasets sharing d: concatenated rows, segment table sorted by
+// n descending, one launch per stage for all of them.
+struct BatchGroup {
+  int d = 0, dpad = 0;
+  int64_t ntot = 0;
+  std::vector<int> order;                 // dataset indices, n descending
+  std::vector<knn::SegEntry> hsegs;       // same order
+  int64_t leaves = 0, maxleaf = 1;
+};
+
+BatchGroup make_group(const knn_dataset* sets, std::vector<int> idx, int d, int leaf) {
+  BatchGroup g;
+  g.d = d;
+  g.dpad = round4(d);
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return sets[a].n > sets[b].n; });
+  g.order = idx;
+  for (int i : idx) {
+    knn::SegEntry e{};
+    e.off = g.ntot;
+    e.n = sets[i].n;
+    e.seed = sets[i].seed;
+    e.depth = knn::tree_depth(e.n, leaf);
+    e.leaf_base = g.leaves;
+    g.leaves += int64_t(1) << e.depth;
+    const int64_t ml = (e.n + (int64_t(1) << e.depth) - 1) >> e.depth;
+    if (ml > g.maxleaf) g.maxleaf = ml;
+    g.ntot += e.n;
+    g.hsegs.push_back(e);
+  }
+  return g;
+}
+
+// The device part of a group's build, from the uploaded rows and table to the
+// finalised [ntot][k] lists with local ids.  Stream-ordered launches only
+// (no allocation once the buffers exist), so it can be captured.
+int group_compute(knn_context* C, const BatchGroup& g, int k, int trees, int props, int metric, int precision,
+                  const float* X, const knn::SegEntry* dsegs, int32_t* seg_of, float* norms, int* err_flag,
+                  float* out_dist, int32_t* out_idx, cudaStream_t st, knn::LaunchLog& log) {
+  const int nseg = (int)g.hsegs.size();
+  knn::launch_fill_seg_of(dsegs, nseg, seg_of, st);
+  log.add();
+  if (metric == KNN_METRIC_COSINE) {
+    knn::launch_norms(X, g.ntot, g.d, g.dpad, norms, st);
+    log.add();
+  }
+  knn::SegView view;
+  view.table = dsegs;
+  view.seg_of = seg_of;
+  view.count = nseg;
+  view.n0 = g.ntot;
+  view.seed0 = 0;
+  view.depth0 = 0;
+  Trees T;
+  int rc = run_trees_segs(C, X, g.ntot, g.d, g.dpad, trees, view, g.hsegs.data(), nseg, st, &T, log);
+  if (rc) return rc;
+  Lists L;
+  rc = get_lists(C, g.ntot, k, &L);
+  if (rc) return rc;
+  Layout lay;
+  lay.segs = view;
+  lay.leaves = g.leaves;
+  lay.maxleaf = g.maxleaf;
+  const bool tensor_leaf = precision == KNN_PREC_BF16_RERANK && metric != KNN_METRIC_TAXICAB && g.d <= 256 &&
+                           k <= 32;
+  if (tensor_leaf)
+    rc = run_leaf_umma(C, X, g.ntot, g.d, g.dpad, k, trees, lay, metric, T.perm, norms, &L, err_flag, st, log);
+  else
+    rc = run_leaf(C, X, g.ntot, g.d, g.dpad, k, trees, lay, metric, T.perm, norms, &L, nullptr, st, log);
+  if (rc) return rc;
+  for (int p = 0; p < props; ++p) {
+    rc = run_prop(X, g.ntot, g.d, g.dpad, k, metric, norms, T.perm, &L, true, nullptr, st, log);
+    if (rc) return rc;
+  }
+  knn::launch_finalize_local(L.key[L.cur], L.id[L.cur], g.ntot, k, metric, seg_of, dsegs, out_dist, out_idx, st);
+  log.add();
+  KNN_CK(cudaPeekAtLastError());
+  return KNN_OK;
+}
+
+std::string group_signature(const BatchGroup& g, int k, int trees, int leaf, int props, int metric,
+                            int precision) {
+  std::string s = "d" + std::to_string(g.d) + ":k" + std::to_string(k) + ":t" + std::to_string(trees) + ":l" +
+                  std::to_string(leaf) + ":p" + std::to_string(props) + ":m" + std::to_string(metric) + ":q" +
+                  std::to_string(precision);
+  for (const auto& e : g.hsegs) s += ":" + std::to_string(e.n) + "/" + std::to_string(e.seed);
+  return s;
+}
+
+int batch_impl(knn_context* C, const knn_dataset* sets, int count, int32_t k, int32_t trees, int32_t leaf,
+               int32_t props, int32_t metric, const knn_options& o, knn_stats* stats, bool use_graphs) {
+  cudaStream_t st = o.stream ? static_cast<cudaStream_t>(o.stream) : C->stream;
+  knn::LaunchLog log;
+  const bool timed = stats != nullptr;
+  if (timed) KNN_CK(cudaEventRecord(C->ev[0], st));
+  std::map<int, std::vector<int>> by_d;
+  for (int i = 0; i < count; ++i) by_d[sets[i].d].push_back(i);
+  int max_depth = 0;
+  int* err_flag = nullptr;
+  int rc = C->get("err_flag", 1, &err_flag);
+  if (rc) return rc;
+  KNN_CK(cudaMemsetAsync(err_flag, 0, sizeof(int), st));
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  KNN_CK(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone || timed) use_graphs = false;
+
+  for (auto& kv : by_d) {
+    const BatchGroup g = make_group(sets, kv.second, kv.first, leaf);
+    for (const auto& e : g.hsegs)
+      if (e.depth > 30) return fail(KNN_ERR_ARGS, "tree too deep (n / leaf too large)");
+    if (g.hsegs[0].depth > max_depth) max_depth = g.hsegs[0].depth;
+    const int nseg = (int)g.hsegs.size();
+    // buffers (all allocated before anything is captured)
+    float *X = nullptr, *norms = nullptr, *od = nullptr;
+    int32_t *seg_of = nullptr, *oi = nullptr;
+    knn::SegEntry* dsegs = nullptr;
+    rc = C->get("bX", (size_t)g.ntot * g.dpad, &X);
+    if (!rc) rc = C->get("b_segs", (size_t)nseg, &dsegs);
+    if (!rc) rc = C->get("b_seg_of", (size_t)g.ntot, &seg_of);
+    if (!rc && metric == KNN_METRIC_COSINE) rc = C->get("norms", (size_t)g.ntot, &norms);
+    if (!rc) rc = C->get("b_out_dist", (size_t)g.ntot * k, &od);
+    if (!rc) rc = C->get("b_out_idx", (size_t)g.ntot * k, &oi);
+    if (rc) return rc;
+    // inputs
+    for (size_t a = 0; a < g.order.size(); ++a) {
+      const knn_dataset& ds = sets[g.order[a]];
+      rc = upload_rows(C, ds.points, ds.n, g.d, o.dtype, o.points_on_device != 0,
+                       X + (size_t)g.hsegs[a].off * g.dpad, g.dpad, st, log);
+      if (rc) return rc;
+    }
+    KNN_CK(cudaMemcpyAsync(dsegs, g.hsegs.data(), sizeof(knn::SegEntry) * nseg, cudaMemcpyHostToDevice, st));
+    // compute: replay a captured graph of this shape, capture it on its second
+    // sighting, or launch directly
+    const std::string sig = use_graphs ? group_signature(g, k, trees, leaf, props, metric, o.precision) : "";
+    bool done = false;
+    if (use_graphs) {
+      for (auto& cg : C->graphs)
+        if (cg.sig == sig && cg.generation == C->generation) {
+          KNN_CK(cudaGraphLaunch(cg.exec, st));
+          log.add(1);
+          done = true;
+          break;
+        }
+      if (!done && std::find(C->seen.begin(), C->seen.end(), sig) != C->seen.end()) {
+        const uint64_t gen0 = C->generation;
+        knn::LaunchLog glog;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        KNN_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int crc = group_compute(C, g, k, trees, props, metric, o.precision, X, dsegs, seg_of, norms,
+                                      err_flag, od, oi, st, glog);
+        cudaError_t e = cudaStreamEndCapture(st, &graph);
+        if (crc == KNN_OK && e == cudaSuccess && C->generation == gen0) e = cudaGraphInstantiate(&exec, graph, 0);
+        else if (e == cudaSuccess) e = cudaErrorStreamCaptureInvalidated;
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        if (e == cudaSuccess) {
+          // drop captures whose buffers have moved since, keep at most 16
+          std::vector<knn_context::Captured> keep;
+          for (auto& cg : C->graphs) {
+            if (cg.generation == C->generation && keep.size() < 15) keep.push_back(cg);
+            else cudaGraphExecDestroy(cg.exec);
+          }
+          C->graphs.swap(keep);
+          C->graphs.push_back({sig, C->generation, exec});
+          KNN_CK(cudaGraphLaunch(exec, st));
+          log.add(1);
+          done = true;
+        }
+      }
+      if (!done && std::find(C->seen.begin(), C->seen.end(), sig) == C->seen.end()) {
+        if (C->seen.size() >= 64) C->seen.erase(C->seen.begin());
+        C->seen.push_back(sig);
+      }
+    }
+    if (!done) {
+      rc = group_compute(C, g, k, trees, props, metric, o.precision, X, dsegs, seg_of, norms, err_flag, od, oi, st,
+                         log);
+      if (rc) return rc;
+    }
+    // outputs
+    const cudaMemcpyKind kind = o.outputs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    for (size_t a = 0; a < g.order.size(); ++a) {
+      const knn_dataset& ds = sets[g.order[a]];
+      const size_t off = (size_t)g.hsegs[a].off * k, cnt = (size_t)ds.n * k;
+      KNN_CK(cudaMemcpyAsync(ds.out_dist, od + off, sizeof(float) * cnt, kind, st));
+      KNN_CK(cudaMemcpyAsync(ds.out_idx, oi + off, sizeof(int32_t) * cnt, kind, st));
+    }
+  }
+  if (timed) KNN_CK(cudaEventRecord(C->ev[5], st));
+  const bool async_ok = o.stream && o.outputs_on_device && !stats;
+  if (!async_ok) {
+    KNN_CK(cudaStreamSynchronize(st));
+    int host_err = 0;
+    KNN_CK(cudaMemcpy(&host_err, err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (host_err) return fail(KNN_ERR_TIMEOUT, "a tensor-core tile wait exceeded its iteration limit");
+  }
+  if (stats) {
+    const int32_t sz = stats->struct_size;
+    std::memset(stats, 0, sizeof(knn_stats));
+    stats->struct_size = sz;
+    stats->depth = max_depth;
+    float ms = 0;
+    KNN_CK(cudaEventElapsedTime(&ms, C->ev[0], C->ev[5]));
+    stats->ms_total = ms;
+    stats->launches = log.count;
+    stats->props_run = props;
   }
   return KNN_OK;
 }
@@ -690,6 +973,35 @@ int knn_build_ex(knn_context* ctx, const void* points, int64_t n, int32_t d, int
                     stats);
 }
 
+int knn_build_batch(knn_context* ctx, const knn_dataset* sets, int32_t count, int32_t k, int32_t trees,
+                    int32_t leaf, int32_t props, int32_t metric, const knn_options* opt, knn_stats* stats) {
+  knn_options o;
+  int rc = resolve_options(opt, &o);
+  if (rc) return rc;
+  if (!sets || count < 1) return fail(KNN_ERR_ARGS, "no datasets");
+  if (k < 1 || k > KNN_MAX_K) return fail(KNN_ERR_ARGS, "k must be in 1..KNN_MAX_K");
+  if (metric < 0 || metric > 2) return fail(KNN_ERR_ARGS, "unknown metric");
+  if (trees < 1 || leaf < 1) return fail(KNN_ERR_ARGS, "trees and leaf must be >= 1");
+  if (props < 0 || props > KNN_MAX_PROPS) return fail(KNN_ERR_ARGS, "props out of range");
+  if (o.ld != 0) return fail(KNN_ERR_ARGS, "batches take contiguous rows (options.ld must be 0)");
+  if (o.learned_splits) return fail(KNN_ERR_UNSUPPORTED, "learned splits are not available for batches");
+  if (stats && stats->struct_size != (int32_t)sizeof(knn_stats))
+    return fail(KNN_ERR_ARGS, "knn_stats.struct_size mismatch");
+  std::map<int, int64_t> per_d;
+  for (int32_t i = 0; i < count; ++i) {
+    const knn_dataset& ds = sets[i];
+    if (!ds.points || !ds.out_idx || !ds.out_dist) return fail(KNN_ERR_ARGS, "dataset pointer is NULL");
+    if (ds.d < 1) return fail(KNN_ERR_ARGS, "dataset d must be >= 1");
+    if (ds.n < 1 || ds.n >= (int64_t)INT32_MAX) return fail(KNN_ERR_ARGS, "dataset n out of range");
+    if (ds.n <= k) return fail(KNN_ERR_N_LE_K, "a dataset has n <= k");
+    per_d[ds.d] += ds.n;
+    if (per_d[ds.d] >= (int64_t)INT32_MAX) return fail(KNN_ERR_ARGS, "too many points of one d in the batch");
+  }
+  rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  return batch_impl(ctx, sets, count, k, trees, leaf, props, metric, o, stats, true);
+}
+
 int knn_build_trees(knn_context* ctx, const float* points, int64_t n, int32_t d, int32_t trees,
                     int32_t leaf, uint64_t seed, int32_t* out_perm) {
   if (!points || !out_perm) return fail(KNN_ERR_ARGS, "NULL pointer");
@@ -742,7 +1054,8 @@ int knn_leaf_stage(knn_context* ctx, const float* points, int64_t n, int32_t d, 
   Lists L;
   rc = get_lists(ctx, n, k, &L);
   if (rc) return rc;
-  rc = run_leaf(ctx, P.X, n, d, P.dpad, k, trees, depth, metric, dperm, norms, &L, nullptr, st, log);
+  rc = run_leaf(ctx, P.X, n, d, P.dpad, k, trees, single_layout(n, depth), metric, dperm, norms, &L, nullptr, st,
+                log);
   if (rc) return rc;
   KNN_CK(cudaMemcpyAsync(out_key, L.key[L.cur], sizeof(float) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
   int32_t* di = nullptr;

@@ -64,6 +64,86 @@ inline int tree_depth(int64_t n, int leaf) {
   return l;
 }
 
+// ------------------------------------------------------------- segments --
+// A batch of independent point sets concatenated in one array.  Segment a
+// holds the global positions / ids [off, off + n) and its trees have `depth`
+// levels; ids in neighbour lists stay global while the batch is built.
+// Segments are sorted by n descending (so by depth descending): the segments
+// still splitting at level l are a prefix of the table.  leaf_base = leaves
+// per tree of the segments before this one.
+struct SegEntry {
+  int64_t off, n;
+  uint64_t seed;
+  int64_t leaf_base;
+  int32_t depth, pad;
+};
+
+struct SegView {
+  const SegEntry* table;  // device; null: one segment {0, n0, seed0, depth0}
+  const int32_t* seg_of;  // device [ntot]: segment of each point; null with one segment
+  int count;
+  int64_t n0;
+  uint64_t seed0;
+  int depth0;
+
+  __device__ __forceinline__ SegEntry get(int a) const {
+    if (table) return table[a];
+    SegEntry e;
+    e.off = 0;
+    e.n = n0;
+    e.seed = seed0;
+    e.leaf_base = 0;
+    e.depth = depth0;
+    e.pad = 0;
+    return e;
+  }
+  __device__ __forceinline__ int of(int64_t i) const { return seg_of ? seg_of[i] : 0; }
+  // The segment holding flat leaf index b (per tree); *j = the leaf in it.
+  __device__ __forceinline__ SegEntry leaf(int64_t b, int64_t* j) const {
+    if (!table) {
+      *j = b;
+      return get(0);
+    }
+    int lo = 0, hi = count - 1;  // last segment with leaf_base <= b
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (table[mid].leaf_base <= b) lo = mid;
+      else hi = mid - 1;
+    }
+    const SegEntry e = table[lo];
+    *j = b - e.leaf_base;
+    return e;
+  }
+};
+
+inline SegView single_segment(int64_t n, uint64_t seed, int depth) {
+  SegView v;
+  v.table = nullptr;
+  v.seg_of = nullptr;
+  v.count = 1;
+  v.n0 = n;
+  v.seed0 = seed;
+  v.depth0 = depth;
+  return v;
+}
+
+// Global positions of leaf j of segment e and of its block, the smallest
+// ancestor holding at least k+1 points (the climb of
+// euclideandistancematrixgpu.cu:87-105).
+__device__ __forceinline__ void leaf_block(const SegEntry& e, int64_t j, int k, int64_t* lo, int64_t* hi,
+                                           int64_t* blo, int64_t* bhi) {
+  *lo = e.off + node_lo(e.n, e.depth, j);
+  *hi = e.off + node_lo(e.n, e.depth, j + 1);
+  int bl = e.depth;
+  int64_t bj = j;
+  while (bl > 0 && node_lo(e.n, bl, bj + 1) - node_lo(e.n, bl, bj) < k + 1) {
+    --bl;
+    bj >>= 1;
+  }
+  *blo = e.off + node_lo(e.n, bl, bj);
+  *bhi = e.off + node_lo(e.n, bl, bj + 1);
+}
+
 // -------------------------------------------------------------- ordering --
 __host__ __device__ __forceinline__ uint32_t orderable(float f) {
 #ifdef __CUDA_ARCH__

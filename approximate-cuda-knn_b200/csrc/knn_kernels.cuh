@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "knn_internal.cuh"
+
 namespace knn {
 
 // Keys of a node staged in shared memory by k_split when it has at most this
@@ -20,26 +22,36 @@ __global__ void k_iota(int32_t* perm, int64_t n, int trees);
 
 // Points are row-major float32 [n][dpad], dpad % 4 == 0, zero padded, 16-byte
 // aligned rows.
+// Batches: n = total points of all segments; segs / hsegs describe them
+// (device view and host copy, sorted by n descending).
 struct TreeArgs {
   const float* X;
   int64_t n;
   int d, dpad;
-  int trees, depth;
-  uint64_t seed;
+  int trees;
+  SegView segs;
+  const SegEntry* hsegs;
+  int nseg;
   int32_t* perm;      // [trees][n] out: leaf order
   int32_t* perm_alt;  // [trees][n] scratch
   int32_t* inv;       // [trees][n] scratch: position of each point
   int32_t* node;      // [trees][n] scratch: node of each point at the current level
   uint64_t* keys;     // [trees][n] scratch
-  float* dirs;        // [trees][2^(depth-1)][dpad] scratch
+  float* dirs;        // [tree_dir_nodes(...)][dpad] scratch
   cudaStream_t stream;
 };
 int tree_build(const TreeArgs& a, LaunchLog& log);
+// Direction slots the deepest-populated level needs: max over levels l of
+// (segments still splitting at l) * trees * 2^l.
+size_t tree_dir_nodes(const SegEntry* hsegs, int nseg, int trees);
 
+// n = all points (a batch: of every segment); leaves = leaf blocks per tree.
 struct LeafArgs {
   const float* X;
   int64_t n;
-  int d, dpad, k, trees, depth, metric;
+  int d, dpad, k, trees, metric;
+  SegView segs;
+  int64_t leaves;
   const int32_t* perm;   // [trees][n]
   const float* norms;    // [n] (COSINE) or null
   float* rkey;           // [n][k] in/out, sorted
@@ -53,7 +65,9 @@ int leaf_stage(const LeafArgs& a, LaunchLog& log);
 struct UmmaLeafArgs {
   const float* X;        // padded float32 rows
   int64_t n;
-  int d, dpad, k, kq, trees, depth, metric;
+  int d, dpad, k, kq, trees, metric;
+  SegView segs;
+  int64_t leaves, maxleaf;  // leaf blocks per tree; points in the largest leaf
   const int32_t* perm;   // [trees][n]
   const float* norms;    // [n] FP32 norms (COSINE) or null
   void* Xb;              // [n][Kp] bf16 scratch (Kp = d rounded up to 64)
@@ -131,5 +145,10 @@ void launch_finalize(const float* key, const uint32_t* id, int64_t n, int k, int
                      float* out_dist, int32_t* out_idx, cudaStream_t st);
 void launch_keys_from_dist(const float* dist, int64_t count, int metric, float* key,
                            cudaStream_t st);
+// Batches (segments): local ids at finalisation; segment of every point.
+void launch_finalize_local(const float* key, const uint32_t* id, int64_t ntot, int k, int metric,
+                           const int32_t* seg_of, const SegEntry* segs, float* out_dist, int32_t* out_idx,
+                           cudaStream_t st);
+void launch_fill_seg_of(const SegEntry* segs, int count, int32_t* seg_of, cudaStream_t st);
 
 }  // namespace knn

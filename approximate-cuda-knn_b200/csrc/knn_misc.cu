@@ -64,6 +64,26 @@ __global__ void k_finalize(const float* __restrict__ key, const uint32_t* __rest
   }
 }
 
+// Batches: ids become local to their segment (the point's own), as above.
+__global__ void k_finalize_local(const float* __restrict__ key, const uint32_t* __restrict__ id,
+                                 int64_t ntot, int k, int metric, const int32_t* __restrict__ seg_of,
+                                 const SegEntry* __restrict__ segs, float* __restrict__ dist,
+                                 int32_t* __restrict__ idx) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < ntot * k) {
+    const int64_t off = segs[seg_of[g / k]].off;
+    const float kv = key[g];
+    dist[g] = metric == KNN_METRIC_EUCLIDEAN ? __fsqrt_rn(kv) : kv;
+    idx[g] = (int32_t)((int64_t)(id[g] & kIdMask) - off);
+  }
+}
+
+// seg_of[i] = segment of global position i; block per segment.
+__global__ void k_fill_seg_of(const SegEntry* __restrict__ segs, int32_t* __restrict__ seg_of) {
+  const SegEntry e = segs[blockIdx.x];
+  for (int64_t i = threadIdx.x; i < e.n; i += blockDim.x) seg_of[e.off + i] = (int32_t)blockIdx.x;
+}
+
 __global__ void k_keys_from_dist(const float* __restrict__ dist, int64_t count, int metric,
                                  float* __restrict__ key) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -101,6 +121,15 @@ void launch_pad_rows(const void* src, int dtype, int64_t n, int d, int64_t ld, f
 void launch_finalize(const float* key, const uint32_t* id, int64_t n, int k, int metric,
                      float* out_dist, int32_t* out_idx, cudaStream_t st) {
   k_finalize<<<blocks_for(n * k, 256), 256, 0, st>>>(key, id, n * k, metric, out_dist, out_idx);
+}
+void launch_finalize_local(const float* key, const uint32_t* id, int64_t ntot, int k, int metric,
+                           const int32_t* seg_of, const SegEntry* segs, float* out_dist, int32_t* out_idx,
+                           cudaStream_t st) {
+  k_finalize_local<<<blocks_for(ntot * k, 256), 256, 0, st>>>(key, id, ntot, k, metric, seg_of, segs, out_dist,
+                                                               out_idx);
+}
+void launch_fill_seg_of(const SegEntry* segs, int count, int32_t* seg_of, cudaStream_t st) {
+  k_fill_seg_of<<<(unsigned)count, 256, 0, st>>>(segs, seg_of);
 }
 void launch_keys_from_dist(const float* dist, int64_t count, int metric, float* key,
                            cudaStream_t st) {

@@ -26,7 +26,7 @@ constexpr int kSP = kTile + 4;
 
 template <int METRIC, int KPL>
 __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d, int dpad,
-                                              int64_t n, int k, int depth,
+                                              SegView segs, int k,
                                               const int32_t* __restrict__ perm,
                                               const float* __restrict__ norms,
                                               float* __restrict__ rkey, uint32_t* __restrict__ rid,
@@ -37,16 +37,10 @@ __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d
   __shared__ int32_t qid[kTile], cid[kTile];
   __shared__ float qnorm[kTile], cnorm[kTile];
 
-  const int64_t j = blockIdx.x;
-  const int64_t lo = node_lo(n, depth, j), hi = node_lo(n, depth, j + 1);
+  int64_t j, lo, hi, blo, bhi;
+  const SegEntry seg = segs.leaf(blockIdx.x, &j);
+  leaf_block(seg, j, k, &lo, &hi, &blo, &bhi);
   const int nq = (int)(hi - lo);
-  int bl = depth;
-  int64_t bj = j;
-  while (bl > 0 && node_lo(n, bl, bj + 1) - node_lo(n, bl, bj) < k + 1) {
-    --bl;
-    bj >>= 1;
-  }
-  const int64_t blo = node_lo(n, bl, bj), bhi = node_lo(n, bl, bj + 1);
   const int nb = (int)(bhi - blo);
 
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
@@ -179,15 +173,14 @@ __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d
 
 template <int METRIC>
 static void launch_leaf_metric(const LeafArgs& a, int t, int kpl) {
-  const int64_t leaves = int64_t(1) << a.depth;
   const int32_t* perm = a.perm + (size_t)t * a.n;
-  dim3 grid((unsigned)leaves);
+  dim3 grid((unsigned)a.leaves);
   if (kpl == 1)
-    k_leaf<METRIC, 1><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.n, a.k, a.depth, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 1><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
   else if (kpl == 2)
-    k_leaf<METRIC, 2><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.n, a.k, a.depth, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 2><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
   else
-    k_leaf<METRIC, 4><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.n, a.k, a.depth, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 4><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
 }
 
 // One launch per tree: a point sits in one leaf per tree, so the leaves of a

@@ -169,7 +169,7 @@ __device__ __forceinline__ void stage_operand(unsigned char* op, const __nv_bflo
 // on its own against a CPU product.
 template <int METRIC>
 __global__ void __launch_bounds__(kUThreads, 2)
-    k_leaf_tc(const __nv_bfloat16* __restrict__ Xb, int Kp, int64_t n, int k, int kq, int depth,
+    k_leaf_tc(const __nv_bfloat16* __restrict__ Xb, int Kp, SegView segs, int k, int kq,
               int qtiles, const int32_t* __restrict__ perm, const float* __restrict__ norms2,
               float* __restrict__ akey, uint32_t* __restrict__ aid, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -193,18 +193,13 @@ __global__ void __launch_bounds__(kUThreads, 2)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t leaf = blockIdx.x / qtiles;
   const int qt = (int)(blockIdx.x - leaf * qtiles);
-  const int64_t lo = node_lo(n, depth, leaf), hi = node_lo(n, depth, leaf + 1);
+  int64_t j, lo, hi, blo, bhi;
+  const SegEntry seg = segs.leaf(leaf, &j);
+  leaf_block(seg, j, k, &lo, &hi, &blo, &bhi);
   const int nq = (int)(hi - lo);
   const int q0 = qt * kBM;
   if (q0 >= nq) return;  // whole block, before any barrier or allocation
   const int mq = min(kBM, nq - q0);
-  int bl = depth;
-  int64_t bj = leaf;
-  while (bl > 0 && node_lo(n, bl, bj + 1) - node_lo(n, bl, bj) < k + 1) {
-    --bl;
-    bj >>= 1;
-  }
-  const int64_t blo = node_lo(n, bl, bj), bhi = node_lo(n, bl, bj + 1);
   const int nb = (int)(bhi - blo);
   const float kInf = __int_as_float(0x7F800000);
   const uint32_t bar = smem_u32(mbar);
@@ -460,19 +455,18 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
                                                                  a.norms, Xb, a.norms2);
   log.add();
   const size_t smem = umma_smem_bytes(Kp);
-  const int64_t leaves = int64_t(1) << a.depth;
-  const int64_t maxleaf = (a.n + leaves - 1) / leaves;
-  const int qtiles = (int)((maxleaf + kBM - 1) / kBM);
+  const int64_t leaves = a.leaves;
+  const int qtiles = (int)((a.maxleaf + kBM - 1) / kBM);
   for (int t = 0; t < a.trees; ++t) {
     const int32_t* perm = a.perm + (size_t)t * a.n;
     if (a.metric == KNN_METRIC_EUCLIDEAN) {
       cudaFuncSetAttribute(k_leaf_tc<KNN_METRIC_EUCLIDEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       k_leaf_tc<KNN_METRIC_EUCLIDEAN><<<(unsigned)(leaves * qtiles), kUThreads, smem, st>>>(
-          Xb, Kp, a.n, a.k, a.kq, a.depth, qtiles, perm, a.norms2, a.akey, a.aid, a.err);
+          Xb, Kp, a.segs, a.k, a.kq, qtiles, perm, a.norms2, a.akey, a.aid, a.err);
     } else {
       cudaFuncSetAttribute(k_leaf_tc<KNN_METRIC_COSINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       k_leaf_tc<KNN_METRIC_COSINE><<<(unsigned)(leaves * qtiles), kUThreads, smem, st>>>(
-          Xb, Kp, a.n, a.k, a.kq, a.depth, qtiles, perm, a.norms2, a.akey, a.aid, a.err);
+          Xb, Kp, a.segs, a.k, a.kq, qtiles, perm, a.norms2, a.akey, a.aid, a.err);
     }
     log.add();
   }

@@ -18,17 +18,21 @@
 
 namespace knn {
 
-// One warp per (tree, node): direction = x[b] - x[a].
-__global__ void k_directions(const float* __restrict__ X, int dpad, int64_t n, int level,
+// One warp per (active segment, tree, node) of `level`: direction
+// x[b] - x[a] of two member points.  Global positions index the perm rows.
+__global__ void k_directions(const float* __restrict__ X, int dpad, int64_t ntot, int level,
                              int trees, const int32_t* __restrict__ perm, float* __restrict__ dirs,
-                             uint64_t seed) {
+                             SegView segs, int active) {
   const int64_t nodes = int64_t(1) << level;
   const int64_t gw = (int64_t)(blockIdx.x * (blockDim.x >> 5)) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (gw >= nodes * trees) return;
-  const int t = (int)(gw / nodes);
-  const int64_t j = gw - (int64_t)t * nodes;
-  const int64_t lo = node_lo(n, level, j), hi = node_lo(n, level, j + 1);
+  if (gw >= nodes * trees * active) return;
+  const int a = (int)(gw / (nodes * trees));
+  const int64_t r = gw - (int64_t)a * nodes * trees;
+  const int t = (int)(r / nodes);
+  const int64_t j = r - (int64_t)t * nodes;
+  const SegEntry e = segs.get(a);
+  const int64_t lo = e.off + node_lo(e.n, level, j), hi = e.off + node_lo(e.n, level, j + 1);
   const int64_t cnt = hi - lo;
   float4* v4 = reinterpret_cast<float4*>(dirs + (size_t)gw * dpad);
   const int nc = dpad >> 2;
@@ -37,11 +41,11 @@ __global__ void k_directions(const float* __restrict__ X, int dpad, int64_t n, i
     return;
   }
   int64_t p1, p2;
-  pivot_positions(seed, t, level, j, cnt, &p1, &p2);
-  const int32_t a = perm[(size_t)t * n + lo + p1];
-  const int32_t b = perm[(size_t)t * n + lo + p2];
-  const float4* xa = reinterpret_cast<const float4*>(X + (size_t)a * dpad);
-  const float4* xb = reinterpret_cast<const float4*>(X + (size_t)b * dpad);
+  pivot_positions(e.seed, t, level, j, cnt, &p1, &p2);
+  const int32_t ia = perm[(size_t)t * ntot + lo + p1];
+  const int32_t ib = perm[(size_t)t * ntot + lo + p2];
+  const float4* xa = reinterpret_cast<const float4*>(X + (size_t)ia * dpad);
+  const float4* xb = reinterpret_cast<const float4*>(X + (size_t)ib * dpad);
   for (int c = lane; c < nc; c += 32) {
     float4 u = __ldg(xa + c), w = __ldg(xb + c);
     v4[c] = make_float4(__fsub_rn(w.x, u.x), __fsub_rn(w.y, u.y), __fsub_rn(w.z, u.z),
@@ -56,28 +60,33 @@ __global__ void k_directions(const float* __restrict__ X, int dpad, int64_t n, i
 // rows thus cross HBM once per level instead of once per tree and level; the
 // directions (a few MB per level) come from L2.
 template <int G>
-__global__ void __launch_bounds__(256) k_project(const float* __restrict__ X, int dpad, int64_t n,
+__global__ void __launch_bounds__(256) k_project(const float* __restrict__ X, int dpad, int64_t ntot,
                                                  int level, int trees,
                                                  const int32_t* __restrict__ inv,
                                                  const int32_t* __restrict__ node,
                                                  const float* __restrict__ dirs,
-                                                 uint64_t* __restrict__ keys) {
+                                                 uint64_t* __restrict__ keys, SegView segs, int active) {
   const int64_t nodes = int64_t(1) << level;
   constexpr int PER_WARP = 32 / G;
   const int lane = threadIdx.x & 31;
   const int gl = lane % G;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * PER_WARP;
-       base < n; base += warps * PER_WARP) {
+       base < ntot; base += warps * PER_WARP) {
     const int64_t i0 = base + lane / G;
-    const bool valid = i0 < n;
-    const int64_t i = valid ? i0 : n - 1;
+    const int64_t i = i0 < ntot ? i0 : ntot - 1;
+    int a = segs.of(i);
+    // every lane takes part in the group's shuffles; points of segments that
+    // stopped splitting project on a valid direction and store nothing
+    const bool valid = i0 < ntot && a < active;
+    if (a >= active) a = 0;
     const float* row = X + (size_t)i * dpad;
     for (int t = 0; t < trees; ++t) {
-      const int64_t p = inv[(size_t)t * n + i];
-      const int64_t j = node[(size_t)t * n + i];
-      const float proj = group_project<G>(row, dirs + ((size_t)t * nodes + j) * dpad, dpad, gl);
-      if (valid && gl == 0) keys[(size_t)t * n + p] = proj_key(proj, (uint32_t)i);
+      const int64_t p = inv[(size_t)t * ntot + i];
+      const int64_t j = valid ? node[(size_t)t * ntot + i] : 0;
+      const float proj =
+          group_project<G>(row, dirs + (((size_t)a * trees + t) * nodes + j) * dpad, dpad, gl);
+      if (valid && gl == 0) keys[(size_t)t * ntot + p] = proj_key(proj, (uint32_t)i);
     }
   }
 }
@@ -175,12 +184,15 @@ __device__ __forceinline__ int64_t block_excl_scan(int64_t v, int64_t* warp_sums
   return r;
 }
 
-// One block per (tree, node) of `level`: median select + stable partition of
-// the node's positions into perm_out, keeping the inverse permutation `inv`
-// (point id -> position) and each point's node of the next level current.  SMEM_KEYS: node keys staged in shared
-// memory (count <= kSplitSmemKeys).
+// One block per (active segment, tree, node) of `level`: median select +
+// stable partition of the node's positions into perm_out, keeping the inverse
+// permutation `inv` (point id -> global position) and each point's node of the
+// next level current.  Blocks past the active ones copy the whole range of a
+// (segment, tree) that no longer splits, so both perm buffers stay complete.
+// SMEM_KEYS: node keys staged in shared memory (count <= kSplitSmemKeys).
 template <bool SMEM_KEYS>
-__global__ void __launch_bounds__(1024) k_split(int64_t n, int level, const uint64_t* __restrict__ keys,
+__global__ void __launch_bounds__(1024) k_split(int64_t ntot, int level, int trees, SegView segs, int active,
+                                                const uint64_t* __restrict__ keys,
                                                 const int32_t* __restrict__ perm,
                                                 int32_t* __restrict__ perm_out,
                                                 int32_t* __restrict__ inv,
@@ -191,19 +203,33 @@ __global__ void __launch_bounds__(1024) k_split(int64_t n, int level, const uint
   __shared__ int64_t warp_sums[33];
   const int64_t nodes = int64_t(1) << level;
   const int64_t s = blockIdx.x;
-  const int t = (int)(s / nodes);
-  const int64_t j = s - (int64_t)t * nodes;
-  const int64_t lo = node_lo(n, level, j), hi = node_lo(n, level, j + 1);
-  const int64_t mid = node_lo(n, level + 1, 2 * j + 1);
+  const int64_t split_blocks = (int64_t)active * trees * nodes;
+  if (s >= split_blocks) {  // copy a finished (segment, tree)
+    const int64_t c = s - split_blocks;
+    const int a = active + (int)(c / trees);
+    const int t = (int)(c % trees);
+    const SegEntry e = segs.get(a);
+    const int32_t* Pin = perm + (size_t)t * ntot + e.off;
+    int32_t* Pout = perm_out + (size_t)t * ntot + e.off;
+    for (int64_t i = threadIdx.x; i < e.n; i += blockDim.x) Pout[i] = Pin[i];
+    return;
+  }
+  const int a = (int)(s / (nodes * trees));
+  const int64_t r = s - (int64_t)a * nodes * trees;
+  const int t = (int)(r / nodes);
+  const int64_t j = r - (int64_t)t * nodes;
+  const SegEntry e = segs.get(a);
+  const int64_t lo = e.off + node_lo(e.n, level, j), hi = e.off + node_lo(e.n, level, j + 1);
+  const int64_t mid = e.off + node_lo(e.n, level + 1, 2 * j + 1);
   const int64_t cnt = hi - lo, nl = mid - lo;
-  const uint64_t* K = keys + (size_t)t * n + lo;
-  const int32_t* Pin = perm + (size_t)t * n + lo;
-  int32_t* Pout = perm_out + (size_t)t * n + lo;
+  const uint64_t* K = keys + (size_t)t * ntot + lo;
+  const int32_t* Pin = perm + (size_t)t * ntot + lo;
+  int32_t* Pout = perm_out + (size_t)t * ntot + lo;
   if (cnt < 2 || nl <= 0 || nl >= cnt) {
     for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) {
       const int32_t id = Pin[i];
       Pout[i] = id;
-      node[(size_t)t * n + id] = (int32_t)(lo + i < mid ? 2 * j : 2 * j + 1);
+      node[(size_t)t * ntot + id] = (int32_t)(lo + i < mid ? 2 * j : 2 * j + 1);
     }
     return;
   }
@@ -223,25 +249,25 @@ __global__ void __launch_bounds__(1024) k_split(int64_t n, int level, const uint
     bool f[ITEMS];
     int c = 0;
 #pragma unroll
-    for (int e = 0; e < ITEMS; ++e) {
-      const int64_t p = p0 + e;
-      f[e] = p < cnt && KS[p] < pivot;
-      c += f[e];
+    for (int q = 0; q < ITEMS; ++q) {
+      const int64_t p = p0 + q;
+      f[q] = p < cnt && KS[p] < pivot;
+      c += f[q];
     }
     int64_t total;
     int64_t before = block_excl_scan(c, warp_sums, &total) + left_base;
 #pragma unroll
-    for (int e = 0; e < ITEMS; ++e) {
-      const int64_t p = p0 + e;
+    for (int q = 0; q < ITEMS; ++q) {
+      const int64_t p = p0 + q;
       if (p < cnt) {
-        const int64_t dst = f[e] ? before : nl + (p - before);
+        const int64_t dst = f[q] ? before : nl + (p - before);
         if (dst >= 0 && dst < cnt) {  // exactly nl keys are below the pivot
           const int32_t id = Pin[p];
           Pout[dst] = id;
-          inv[(size_t)t * n + id] = (int32_t)(lo + dst);
-          node[(size_t)t * n + id] = (int32_t)(f[e] ? 2 * j : 2 * j + 1);
+          inv[(size_t)t * ntot + id] = (int32_t)(lo + dst);
+          node[(size_t)t * ntot + id] = (int32_t)(f[q] ? 2 * j : 2 * j + 1);
         }
-        before += f[e];
+        before += f[q];
       }
     }
     left_base += total;
@@ -249,9 +275,20 @@ __global__ void __launch_bounds__(1024) k_split(int64_t n, int level, const uint
 }
 
 // ------------------------------------------------------------------ host --
+size_t tree_dir_nodes(const SegEntry* hsegs, int nseg, int trees) {
+  size_t best = 1;
+  const int maxdepth = hsegs[0].depth;
+  for (int l = 0; l < maxdepth; ++l) {
+    int active = 0;
+    while (active < nseg && hsegs[active].depth > l) ++active;
+    const size_t v = (size_t)active * (size_t)trees << l;
+    if (v > best) best = v;
+  }
+  return best;
+}
+
 int tree_build(const TreeArgs& a, LaunchLog& log) {
-  const int64_t n = a.n;
-  const int depth = a.depth;
+  const int64_t ntot = a.n;
   cudaStream_t st = a.stream;
   static bool attr_set[64] = {false};
   int dev = 0;
@@ -262,38 +299,43 @@ int tree_build(const TreeArgs& a, LaunchLog& log) {
     attr_set[dev & 63] = true;
   }
   // identity order for every tree
-  k_iota<<<(unsigned)((a.trees * n + 255) / 256), 256, 0, st>>>(a.perm, n, a.trees);
-  k_iota<<<(unsigned)((a.trees * n + 255) / 256), 256, 0, st>>>(a.inv, n, a.trees);
-  cudaMemsetAsync(a.node, 0, sizeof(int32_t) * (size_t)a.trees * n, st);  // all in the root
+  k_iota<<<(unsigned)((a.trees * ntot + 255) / 256), 256, 0, st>>>(a.perm, ntot, a.trees);
+  k_iota<<<(unsigned)((a.trees * ntot + 255) / 256), 256, 0, st>>>(a.inv, ntot, a.trees);
+  cudaMemsetAsync(a.node, 0, sizeof(int32_t) * (size_t)a.trees * ntot, st);  // all in the root
   log.add(2);
   int32_t* cur = a.perm;
   int32_t* alt = a.perm_alt;
   const int G = proj_group(a.d);
-  for (int l = 0; l < depth; ++l) {
+  const int maxdepth = a.hsegs[0].depth;
+  for (int l = 0; l < maxdepth; ++l) {
+    int active = 0;
+    while (active < a.nseg && a.hsegs[active].depth > l) ++active;
     const int64_t nodes = int64_t(1) << l;
-    const int64_t segs = nodes * a.trees;
-    k_directions<<<(unsigned)((segs + 7) / 8), 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, cur,
-                                                             a.dirs, a.seed);
+    const int64_t segs = nodes * a.trees * active;
+    k_directions<<<(unsigned)((segs + 7) / 8), 256, 0, st>>>(a.X, a.dpad, ntot, l, a.trees, cur, a.dirs,
+                                                             a.segs, active);
     const int per_block = 8 * (32 / G);
-    int64_t blocks = (n + per_block - 1) / per_block;
+    int64_t blocks = (ntot + per_block - 1) / per_block;
     if (blocks > 148LL * 64) blocks = 148LL * 64;
     switch (G) {
-      case 1: k_project<1><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, a.inv, a.node, a.dirs, a.keys); break;
-      case 2: k_project<2><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, a.inv, a.node, a.dirs, a.keys); break;
-      case 4: k_project<4><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, a.inv, a.node, a.dirs, a.keys); break;
-      case 8: k_project<8><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, a.inv, a.node, a.dirs, a.keys); break;
-      case 16: k_project<16><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, a.inv, a.node, a.dirs, a.keys); break;
-      default: k_project<32><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, n, l, a.trees, a.inv, a.node, a.dirs, a.keys); break;
+      case 1: k_project<1><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, ntot, l, a.trees, a.inv, a.node, a.dirs, a.keys, a.segs, active); break;
+      case 2: k_project<2><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, ntot, l, a.trees, a.inv, a.node, a.dirs, a.keys, a.segs, active); break;
+      case 4: k_project<4><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, ntot, l, a.trees, a.inv, a.node, a.dirs, a.keys, a.segs, active); break;
+      case 8: k_project<8><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, ntot, l, a.trees, a.inv, a.node, a.dirs, a.keys, a.segs, active); break;
+      case 16: k_project<16><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, ntot, l, a.trees, a.inv, a.node, a.dirs, a.keys, a.segs, active); break;
+      default: k_project<32><<<(unsigned)blocks, 256, 0, st>>>(a.X, a.dpad, ntot, l, a.trees, a.inv, a.node, a.dirs, a.keys, a.segs, active); break;
     }
-    const int64_t maxcnt = (n + nodes - 1) / nodes;
+    // the largest active segment is the first
+    const int64_t maxcnt = (a.hsegs[0].n + nodes - 1) / nodes;
     int threads = (int)((maxcnt + 3) / 4);
     threads = ((threads + 31) / 32) * 32;
     if (threads < 64) threads = 64;
     if (threads > 1024) threads = 1024;
+    const unsigned grid = (unsigned)(segs + (int64_t)(a.nseg - active) * a.trees);
     if (maxcnt <= kSplitSmemKeys) {
-      k_split<true><<<(unsigned)segs, threads, (size_t)maxcnt * sizeof(uint64_t), st>>>(n, l, a.keys, cur, alt, a.inv, a.node);
+      k_split<true><<<grid, threads, (size_t)maxcnt * sizeof(uint64_t), st>>>(ntot, l, a.trees, a.segs, active, a.keys, cur, alt, a.inv, a.node);
     } else {
-      k_split<false><<<(unsigned)segs, threads, 0, st>>>(n, l, a.keys, cur, alt, a.inv, a.node);
+      k_split<false><<<grid, threads, 0, st>>>(ntot, l, a.trees, a.segs, active, a.keys, cur, alt, a.inv, a.node);
     }
     log.add(3);
     int32_t* tmp = cur;
@@ -301,7 +343,7 @@ int tree_build(const TreeArgs& a, LaunchLog& log) {
     alt = tmp;
   }
   if (cur != a.perm) {
-    cudaMemcpyAsync(a.perm, cur, sizeof(int32_t) * (size_t)a.trees * n, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(a.perm, cur, sizeof(int32_t) * (size_t)a.trees * ntot, cudaMemcpyDeviceToDevice, st);
   }
   return cudaPeekAtLastError() == cudaSuccess ? KNN_OK : KNN_ERR_CUDA;
 }

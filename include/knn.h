@@ -146,6 +146,32 @@ int knn_build_ex(knn_context* ctx, const void* points, int64_t n, int32_t d, int
                  int32_t* out_idx, float* out_dist, const knn_options* opt, knn_stats* stats);
 
 /*
+ * knn_build_batch -- many independent point sets in one call (no counterpart
+ * in the reference, which builds one set per process).  Sets of equal d are
+ * concatenated and every stage runs once for all of them; each set's trees,
+ * leaf blocks and propagation stay within the set, and its result equals a
+ * knn_build_ex of that set alone with the same seed (bit for bit in plain
+ * FP32).  The device work of a group of equal-d sets is captured as a CUDA
+ * graph the second time the same shapes are seen and replayed after that.
+ *   sets[i].points  [n][d] rows, host or device and element type per options
+ *                   (options.ld must be 0);  out_idx int32 [n][k] (ids local to
+ *                   the set) and out_dist float32 [n][k], host or device.
+ * Learned splits are not available here (KNN_ERR_UNSUPPORTED).
+ */
+typedef struct knn_dataset {
+  const void* points;
+  int64_t n;
+  int32_t d;
+  int32_t reserved;
+  uint64_t seed;
+  int32_t* out_idx;
+  float* out_dist;
+} knn_dataset;
+
+int knn_build_batch(knn_context* ctx, const knn_dataset* sets, int32_t count, int32_t k, int32_t trees,
+                    int32_t leaf, int32_t props, int32_t metric, const knn_options* opt, knn_stats* stats);
+
+/*
  * Stage entry points (host memory in and out), for stage-by-stage checks.
  *   knn_build_trees   leaf order of every tree: out_perm int32 [trees][n]
  *                     (replaces buildUpTheTrees, euclideandistancematrixgpu.cu:2407-2686)

@@ -44,24 +44,31 @@ def test_python_binding_covers_header():
 
 
 def test_struct_layout_matches_c(tmp_path):
+    """Every field offset and every struct size of the ctypes mirror equals
+    the C compiler's for the header's structs."""
+    acknn = load_package()
+    structs = {"knn_options": acknn.KnnOptions, "knn_stats": acknn.KnnStats,
+               "knn_dataset": acknn.KnnDataset}
+    lines, want = [], []
+    for cname, py in structs.items():
+        lines.append(f'printf("%zu\\n", sizeof({cname}));')
+        want.append(ctypes.sizeof(py))
+        for fname, _ in py._fields_:
+            lines.append(f'printf("%zu\\n", offsetof({cname}, {fname}));')
+            want.append(getattr(py, fname).offset)
     src = tmp_path / "probe.c"
+    body = "\n          ".join(lines)
     src.write_text(textwrap.dedent(f"""
         #include <stdio.h>
         #include <stddef.h>
         #include "{ROOT / 'include' / 'knn.h'}"
         int main(void) {{
-          printf("%zu %zu %zu %zu %zu\\n", sizeof(knn_options), sizeof(knn_stats),
-                 offsetof(knn_options, stream), offsetof(knn_stats, prop_candidates),
-                 offsetof(knn_stats, ms_prop_iter));
+          {body}
           return 0;
         }}"""))
     exe = tmp_path / "probe"
     subprocess.run(["/usr/bin/gcc", str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
-    acknn = load_package()
-    want = [ctypes.sizeof(acknn.KnnOptions), ctypes.sizeof(acknn.KnnStats),
-            acknn.KnnOptions.stream.offset, acknn.KnnStats.prop_candidates.offset,
-            acknn.KnnStats.ms_prop_iter.offset]
     assert [int(v) for v in out] == want
 
 
@@ -108,3 +115,22 @@ def test_missing_library_fails_loudly(tmp_path):
     acknn = load_package()
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         acknn.load_library(tmp_path / "libacknn.so")
+
+
+def test_batch_argument_errors_before_device():
+    """knn_build_batch rejects bad batches before touching a device."""
+    acknn = load_package()
+    x = np.zeros((10, 4), dtype=np.float32)
+    small = np.zeros((3, 4), dtype=np.float32)
+    with pytest.raises(acknn.KnnError) as e:
+        acknn.knn_build_batch([x, small], 5, 2, 8, 1, 0)
+    assert e.value.status == -2  # a set with n <= k
+    with pytest.raises(acknn.KnnError) as e:
+        acknn.knn_build_batch([x], 5, 0, 8, 1, 0)
+    assert e.value.status == -1
+    with pytest.raises(acknn.KnnError) as e:
+        acknn.knn_build_batch([x], 5, 2, 8, 1, 7)
+    assert e.value.status == -1
+    with pytest.raises(acknn.KnnError) as e:
+        acknn.knn_build_batch([], 5, 2, 8, 1, 0)
+    assert e.value.status == -1
