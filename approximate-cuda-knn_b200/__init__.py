@@ -66,7 +66,10 @@ class KnnOptions(ctypes.Structure):
         ("stream", ctypes.c_void_p),
         ("mlp_sample", ctypes.c_int32),
         ("mlp_steps", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 6),
+        ("autotune", ctypes.c_int32),
+        ("leaf_tile", ctypes.c_int32),
+        ("prop_warps", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
     ]
 
 
@@ -86,8 +89,10 @@ class KnnStats(ctypes.Structure):
         ("prop_candidates", ctypes.c_int64 * MAX_PROPS),
         ("ms_prop_iter", ctypes.c_float * MAX_PROPS),
         ("ms_learn", ctypes.c_float),
+        ("leaf_tile", ctypes.c_int32),
+        ("prop_warps", ctypes.c_int32),
         ("reserved_pad", ctypes.c_int32),
-        ("reserved", ctypes.c_int64 * 7),
+        ("reserved", ctypes.c_int64 * 6),
     ]
 
     def as_dict(self) -> dict:
@@ -97,6 +102,7 @@ class KnnStats(ctypes.Structure):
             "ms_learn": self.ms_learn, "ms_trees": self.ms_trees, "ms_leaf": self.ms_leaf,
             "ms_propagate": self.ms_propagate, "ms_download": self.ms_download,
             "launches": self.launches, "leaf_pairs": self.leaf_pairs,
+            "leaf_tile": self.leaf_tile, "prop_warps": self.prop_warps,
             "prop_candidates": [self.prop_candidates[i] for i in range(n)],
         }
 
@@ -193,7 +199,8 @@ def default_options(**kw) -> KnnOptions:
 
 def knn_build(points, k: int, trees: int, leaf: int, props: int, metric: int = 0,
               seed: int = 0, precision: int = PREC_FP32, learned: bool = False,
-              stats: bool = False, context=None, mlp_sample: int = 0, mlp_steps: int = 0):
+              stats: bool = False, context=None, mlp_sample: int = 0, mlp_steps: int = 0,
+              autotune: bool = False, leaf_tile: int = 0, prop_warps: int = 0):
     """k-NN graph of ``points`` ([n, d] float32/float16, host memory).
 
     ``learned`` builds the trees on the learned split network's embedding
@@ -207,7 +214,8 @@ def knn_build(points, k: int, trees: int, leaf: int, props: int, metric: int = 0
     dist = np.empty((n, k), dtype=np.float32)
     opt = default_options(dtype=F16 if x.dtype == np.float16 else F32, precision=precision,
                           learned_splits=int(bool(learned)), mlp_sample=mlp_sample,
-                          mlp_steps=mlp_steps)
+                          mlp_steps=mlp_steps, autotune=int(bool(autotune)), leaf_tile=leaf_tile,
+                          prop_warps=prop_warps)
     st = KnnStats()
     st.struct_size = ctypes.sizeof(KnnStats)
     rc = lib.knn_build_ex(context, _ptr(x), n, d, k, trees, leaf, props, metric, seed,
@@ -218,7 +226,8 @@ def knn_build(points, k: int, trees: int, leaf: int, props: int, metric: int = 0
 
 
 def knn_build_batch(datasets, k: int, trees: int, leaf: int, props: int, metric: int = 0,
-                    seeds=None, precision: int = PREC_FP32, stats: bool = False, context=None):
+                    seeds=None, precision: int = PREC_FP32, stats: bool = False, context=None,
+                    autotune: bool = False, leaf_tile: int = 0, prop_warps: int = 0):
     """k-NN graphs of many independent point sets in one call.
 
     ``datasets``: sequence of [n_i, d_i] arrays (all float32 or all float16);
@@ -242,7 +251,8 @@ def knn_build_batch(datasets, k: int, trees: int, leaf: int, props: int, metric:
         arr[i].out_idx = _ptr(idx)
         arr[i].out_dist = _ptr(dist)
     f16 = bool(xs) and xs[0].dtype == np.float16
-    opt = default_options(dtype=F16 if f16 else F32, precision=precision)
+    opt = default_options(dtype=F16 if f16 else F32, precision=precision,
+                          autotune=int(bool(autotune)), leaf_tile=leaf_tile, prop_warps=prop_warps)
     st = KnnStats()
     st.struct_size = ctypes.sizeof(KnnStats)
     _check(load_library().knn_build_batch(context, arr, len(xs), k, trees, leaf, props, metric,

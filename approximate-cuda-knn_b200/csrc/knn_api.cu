@@ -73,6 +73,9 @@ struct knn_context {
   };
   std::vector<Captured> graphs;
   std::vector<std::string> seen;
+  // Autotuned launch shapes by workload key: (FP32 leaf tile, propagation warps).
+  std::map<std::string, std::pair<int, int>> tuned;
+  cudaEvent_t tev[2] = {};
 
   // Device buffer `name` of at least `bytes`; grows by reallocation.
   int get(const char* name, size_t bytes, void** out) {
@@ -116,6 +119,8 @@ struct knn_context {
       if (kv.second.p) cudaFree(kv.second.p);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
+    for (auto& e : tev)
+      if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
     if (cur != device) cudaSetDevice(cur);
   }
@@ -137,6 +142,7 @@ int make_context(int device, knn_context** out) {
   c->device = device;
   KNN_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   for (auto& ev : c->ev) KNN_CK(cudaEventCreate(&ev));
+  for (auto& ev : c->tev) KNN_CK(cudaEventCreate(&ev));
   *out = c.release();
   return KNN_OK;
 }
@@ -303,7 +309,7 @@ Layout single_layout(int64_t n, int depth) {
 
 int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, int trees,
              const Layout& lay, int metric, const int32_t* perm, const float* norms, Lists* L,
-             unsigned long long* counter, cudaStream_t st, knn::LaunchLog& log) {
+             unsigned long long* counter, cudaStream_t st, knn::LaunchLog& log, int tile = 0) {
   const int kw = (k + 31) / 32;
   knn::launch_init_lists(L->key[L->cur], L->id[L->cur], L->flags[L->cur], n, k, kw, st);
   log.add(2);
@@ -322,6 +328,7 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
   a.rkey = L->key[L->cur];
   a.rid = L->id[L->cur];
   a.pair_counter = counter;
+  a.tile = tile;
   a.stream = st;
   int rc = knn::leaf_stage(a, log);
   if (rc) return fail_cuda(cudaGetLastError(), "leaf stage launch");
@@ -372,7 +379,7 @@ int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, in
 
 int run_prop(const float* X, int64_t n, int d, int dpad, int k, int metric, const float* norms,
              const int32_t* order, Lists* L, bool with_flags, unsigned long long* counter,
-             cudaStream_t st, knn::LaunchLog& log) {
+             cudaStream_t st, knn::LaunchLog& log, int warps = 0) {
   knn::PropArgs a{};
   a.X = X;
   a.n = n;
@@ -389,11 +396,118 @@ int run_prop(const float* X, int64_t n, int d, int dpad, int k, int metric, cons
   a.id_out = L->id[1 - L->cur];
   a.flags_out = L->flags[1 - L->cur];
   a.cand_counter = counter;
+  a.warps = warps;
   a.stream = st;
   int rc = knn::propagate_step(a, log);
   if (rc == KNN_ERR_UNSUPPORTED) return fail(rc, "propagation scratch exceeds shared memory (k or d too large)");
   if (rc) return fail_cuda(cudaGetLastError(), "propagation launch");
   L->cur = 1 - L->cur;
+  return KNN_OK;
+}
+
+// ---------------------------------------------------------------- tuning --
+// Launch shapes that do not change any result -- the FP32 leaf kernel's
+// query x candidate tile and the propagation kernel's warps per block -- are
+// picked by timing.  Each candidate runs twice on the call's own trees and
+// lists (into the spare list buffers; the second run is timed with events) and
+// the fastest is cached in the context per (metric, d, k, largest leaf).
+// Tuning happens only in eagerly launched calls; captured graphs use the cache.
+std::string tune_key(int metric, int d, int k, int64_t maxleaf) {
+  return "m" + std::to_string(metric) + ":d" + std::to_string(d) + ":k" + std::to_string(k) + ":L" +
+         std::to_string(maxleaf);
+}
+
+int time_since(knn_context* C, cudaStream_t st, float* ms) {
+  KNN_CK(cudaEventRecord(C->tev[1], st));
+  KNN_CK(cudaEventSynchronize(C->tev[1]));
+  KNN_CK(cudaEventElapsedTime(ms, C->tev[0], C->tev[1]));
+  return KNN_OK;
+}
+
+int tune_leaf_tile(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, const Layout& lay,
+                   int metric, const int32_t* perm, const float* norms, const Lists& L, cudaStream_t st,
+                   int* best) {
+  Lists S = L;
+  S.cur = 1 - L.cur;  // scratch lists
+  float best_ms = 3.4e38f;
+  *best = 64;
+  for (int tile : {64, 32}) {
+    float ms = 0;
+    for (int rep = 0; rep < 2; ++rep) {
+      knn::LaunchLog tl;
+      KNN_CK(cudaEventRecord(C->tev[0], st));
+      int rc = run_leaf(C, X, n, d, dpad, k, 1, lay, metric, perm, norms, &S, nullptr, st, tl, tile);
+      if (!rc) rc = time_since(C, st, &ms);
+      if (rc) return rc;
+    }
+    if (ms < best_ms) {
+      best_ms = ms;
+      *best = tile;
+    }
+  }
+  return KNN_OK;
+}
+
+int tune_prop_warps(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, int metric,
+                    const float* norms, const int32_t* order, Lists* L, cudaStream_t st, int* best) {
+  const int cur = L->cur;
+  float best_ms = 3.4e38f;
+  *best = 0;
+  for (int w : {8, 4, 2}) {
+    float ms = 0;
+    for (int rep = 0; rep < 2; ++rep) {
+      knn::LaunchLog tl;
+      KNN_CK(cudaEventRecord(C->tev[0], st));
+      int rc = run_prop(X, n, d, dpad, k, metric, norms, order, L, true, nullptr, st, tl, w);
+      L->cur = cur;  // the timing run's output is scratch
+      if (!rc) rc = time_since(C, st, &ms);
+      if (rc) return rc;
+    }
+    if (ms < best_ms) {
+      best_ms = ms;
+      *best = w;
+    }
+  }
+  return KNN_OK;
+}
+
+// Leaf tile and propagation warps for this call: forced by the options,
+// cached, or tuned now (when allowed).
+struct Shapes {
+  int leaf_tile = 0, prop_warps = 0;
+};
+
+int pick_shapes(knn_context* C, const knn_options& o, bool may_tune, bool fp32_leaf, int props, const float* X,
+                int64_t n, int d, int dpad, int k, const Layout& lay, int metric, const int32_t* perm,
+                const float* norms, Lists* L, cudaStream_t st, Shapes* sh, bool* tune_prop_after) {
+  sh->leaf_tile = o.leaf_tile;
+  sh->prop_warps = o.prop_warps;
+  *tune_prop_after = false;
+  if (!o.autotune) return KNN_OK;
+  const std::string key = tune_key(metric, d, k, lay.maxleaf);
+  auto it = C->tuned.find(key);
+  if (it != C->tuned.end()) {
+    if (!sh->leaf_tile) sh->leaf_tile = it->second.first;
+    if (!sh->prop_warps) sh->prop_warps = it->second.second;
+    if (!(fp32_leaf && sh->leaf_tile == 0) && !(props > 0 && sh->prop_warps == 0)) return KNN_OK;
+  }
+  if (!may_tune) return KNN_OK;
+  if (fp32_leaf && !sh->leaf_tile) {
+    int rc = tune_leaf_tile(C, X, n, d, dpad, k, lay, metric, perm, norms, *L, st, &sh->leaf_tile);
+    if (rc) return rc;
+    C->tuned[key].first = sh->leaf_tile;
+  }
+  *tune_prop_after = props > 0 && !sh->prop_warps;
+  return KNN_OK;
+}
+
+int finish_prop_tuning(knn_context* C, const knn_options& o, const float* X, int64_t n, int d, int dpad, int k,
+                       int metric, const float* norms, const int32_t* order, Lists* L, int64_t maxleaf,
+                       cudaStream_t st, Shapes* sh) {
+  int rc = tune_prop_warps(C, X, n, d, dpad, k, metric, norms, order, L, st, &sh->prop_warps);
+  if (rc) return rc;
+  C->tuned[tune_key(metric, d, k, maxleaf)].second = sh->prop_warps;
+  (void)o;
   return KNN_OK;
 }
 
@@ -514,6 +628,10 @@ int resolve_options(const knn_options* opt, knn_options* o) {
   if (o->precision < 0 || o->precision > 1) return fail(KNN_ERR_ARGS, "unknown precision mode");
   if (o->learned_splits < 0 || o->learned_splits > 1) return fail(KNN_ERR_ARGS, "learned_splits must be 0 or 1");
   if (o->mlp_sample < 0 || o->mlp_steps < 0) return fail(KNN_ERR_ARGS, "negative learned-split setting");
+  if (o->autotune < 0 || o->autotune > 1) return fail(KNN_ERR_ARGS, "autotune must be 0 or 1");
+  if (o->leaf_tile != 0 && o->leaf_tile != 32 && o->leaf_tile != 64)
+    return fail(KNN_ERR_ARGS, "leaf_tile must be 0, 32 or 64");
+  if (o->prop_warps < 0 || o->prop_warps > 8) return fail(KNN_ERR_ARGS, "prop_warps must be in 0..8");
   return KNN_OK;
 }
 
@@ -578,19 +696,30 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
   KNN_CK(cudaMemsetAsync(err_flag, 0, sizeof(int), st));
   const bool tensor_leaf = o.precision == KNN_PREC_BF16_RERANK && metric != KNN_METRIC_TAXICAB &&
                            d <= 256 && k <= 32;
+  const Layout lay = single_layout(n, T.depth);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  KNN_CK(cudaStreamIsCapturing(st, &cs));
+  Shapes sh;
+  bool tune_prop = false;
+  rc = pick_shapes(C, o, cs == cudaStreamCaptureStatusNone, !tensor_leaf, props, P.X, n, d, P.dpad, k, lay,
+                   metric, T.perm, norms, &L, st, &sh, &tune_prop);
+  if (rc) return rc;
   if (tensor_leaf) {
-    rc = run_leaf_umma(C, P.X, n, d, P.dpad, k, trees, single_layout(n, T.depth), metric, T.perm, norms, &L,
-                       err_flag, st, log);
+    rc = run_leaf_umma(C, P.X, n, d, P.dpad, k, trees, lay, metric, T.perm, norms, &L, err_flag, st, log);
   } else {
-    rc = run_leaf(C, P.X, n, d, P.dpad, k, trees, single_layout(n, T.depth), metric, T.perm, norms, &L,
-                  stats ? counters : nullptr, st, log);
+    rc = run_leaf(C, P.X, n, d, P.dpad, k, trees, lay, metric, T.perm, norms, &L, stats ? counters : nullptr, st,
+                  log, sh.leaf_tile);
   }
   if (rc) return rc;
+  if (tune_prop) {
+    rc = finish_prop_tuning(C, o, P.X, n, d, P.dpad, k, metric, norms, T.perm, &L, lay.maxleaf, st, &sh);
+    if (rc) return rc;
+  }
   if (timed) KNN_CK(cudaEventRecord(C->ev[3], st));
 
   for (int p = 0; p < props; ++p) {
     rc = run_prop(P.X, n, d, P.dpad, k, metric, norms, T.perm, &L, true,
-                  stats ? counters + 2 + p : nullptr, st, log);
+                  stats ? counters + 2 + p : nullptr, st, log, sh.prop_warps);
     if (rc) return rc;
   }
   if (timed) KNN_CK(cudaEventRecord(C->ev[4], st));
@@ -646,6 +775,8 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
     stats->ms_download = ms;
     stats->launches = log.count;
     stats->props_run = props;
+    stats->leaf_tile = tensor_leaf ? 128 : (sh.leaf_tile ? sh.leaf_tile : 64);
+    stats->prop_warps = sh.prop_warps;
     unsigned long long host[2 + KNN_MAX_PROPS];
     KNN_CK(cudaMemcpy(host, counters, sizeof(host), cudaMemcpyDeviceToHost));
     stats->leaf_pairs = (int64_t)host[0];
@@ -715,9 +846,12 @@ BatchGroup make_group(const knn_dataset* sets, std::vector<int> idx, int d, int 
 // The device part of a group's build, from the uploaded rows and table to the
 // finalised [ntot][k] lists with local ids.  Stream-ordered launches only
 // (no allocation once the buffers exist), so it can be captured.
-int group_compute(knn_context* C, const BatchGroup& g, int k, int trees, int props, int metric, int precision,
-                  const float* X, const knn::SegEntry* dsegs, int32_t* seg_of, float* norms, int* err_flag,
-                  float* out_dist, int32_t* out_idx, cudaStream_t st, knn::LaunchLog& log) {
+int group_compute(knn_context* C, const BatchGroup& g, int k, int trees, int props, int metric,
+                  const knn_options& o, bool may_tune, const float* X, const knn::SegEntry* dsegs, int32_t* seg_of,
+                  float* norms, int* err_flag, float* out_dist, int32_t* out_idx, cudaStream_t st,
+                  knn::LaunchLog& log, bool stage_events = false) {
+  const int precision = o.precision;
+  if (stage_events) KNN_CK(cudaEventRecord(C->ev[1], st));
   const int nseg = (int)g.hsegs.size();
   knn::launch_fill_seg_of(dsegs, nseg, seg_of, st);
   log.add();
@@ -735,6 +869,7 @@ int group_compute(knn_context* C, const BatchGroup& g, int k, int trees, int pro
   Trees T;
   int rc = run_trees_segs(C, X, g.ntot, g.d, g.dpad, trees, view, g.hsegs.data(), nseg, st, &T, log);
   if (rc) return rc;
+  if (stage_events) KNN_CK(cudaEventRecord(C->ev[2], st));
   Lists L;
   rc = get_lists(C, g.ntot, k, &L);
   if (rc) return rc;
@@ -744,15 +879,27 @@ int group_compute(knn_context* C, const BatchGroup& g, int k, int trees, int pro
   lay.maxleaf = g.maxleaf;
   const bool tensor_leaf = precision == KNN_PREC_BF16_RERANK && metric != KNN_METRIC_TAXICAB && g.d <= 256 &&
                            k <= 32;
+  Shapes sh;
+  bool tune_prop = false;
+  rc = pick_shapes(C, o, may_tune, !tensor_leaf, props, X, g.ntot, g.d, g.dpad, k, lay, metric, T.perm, norms, &L,
+                   st, &sh, &tune_prop);
+  if (rc) return rc;
   if (tensor_leaf)
     rc = run_leaf_umma(C, X, g.ntot, g.d, g.dpad, k, trees, lay, metric, T.perm, norms, &L, err_flag, st, log);
   else
-    rc = run_leaf(C, X, g.ntot, g.d, g.dpad, k, trees, lay, metric, T.perm, norms, &L, nullptr, st, log);
+    rc = run_leaf(C, X, g.ntot, g.d, g.dpad, k, trees, lay, metric, T.perm, norms, &L, nullptr, st, log,
+                  sh.leaf_tile);
   if (rc) return rc;
-  for (int p = 0; p < props; ++p) {
-    rc = run_prop(X, g.ntot, g.d, g.dpad, k, metric, norms, T.perm, &L, true, nullptr, st, log);
+  if (tune_prop) {
+    rc = finish_prop_tuning(C, o, X, g.ntot, g.d, g.dpad, k, metric, norms, T.perm, &L, lay.maxleaf, st, &sh);
     if (rc) return rc;
   }
+  if (stage_events) KNN_CK(cudaEventRecord(C->ev[3], st));
+  for (int p = 0; p < props; ++p) {
+    rc = run_prop(X, g.ntot, g.d, g.dpad, k, metric, norms, T.perm, &L, true, nullptr, st, log, sh.prop_warps);
+    if (rc) return rc;
+  }
+  if (stage_events) KNN_CK(cudaEventRecord(C->ev[4], st));
   knn::launch_finalize_local(L.key[L.cur], L.id[L.cur], g.ntot, k, metric, seg_of, dsegs, out_dist, out_idx, st);
   log.add();
   KNN_CK(cudaPeekAtLastError());
@@ -784,6 +931,7 @@ int batch_impl(knn_context* C, const knn_dataset* sets, int count, int32_t k, in
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   KNN_CK(cudaStreamIsCapturing(st, &cs));
   if (cs != cudaStreamCaptureStatusNone || timed) use_graphs = false;
+  float stage_ms[3] = {0, 0, 0};
 
   for (auto& kv : by_d) {
     const BatchGroup g = make_group(sets, kv.second, kv.first, leaf);
@@ -802,12 +950,24 @@ int batch_impl(knn_context* C, const knn_dataset* sets, int count, int32_t k, in
     if (!rc) rc = C->get("b_out_dist", (size_t)g.ntot * k, &od);
     if (!rc) rc = C->get("b_out_idx", (size_t)g.ntot * k, &oi);
     if (rc) return rc;
-    // inputs
-    for (size_t a = 0; a < g.order.size(); ++a) {
-      const knn_dataset& ds = sets[g.order[a]];
-      rc = upload_rows(C, ds.points, ds.n, g.d, o.dtype, o.points_on_device != 0,
-                       X + (size_t)g.hsegs[a].off * g.dpad, g.dpad, st, log);
+    // inputs: device sets in one gather launch, host sets by one copy each
+    if (o.points_on_device) {
+      std::vector<knn::RowSource> src(g.order.size());
+      for (size_t a = 0; a < g.order.size(); ++a)
+        src[a] = {sets[g.order[a]].points, g.hsegs[a].n, g.hsegs[a].off};
+      knn::RowSource* dsrc = nullptr;
+      rc = C->get("b_src", src.size(), &dsrc);
       if (rc) return rc;
+      KNN_CK(cudaMemcpyAsync(dsrc, src.data(), sizeof(knn::RowSource) * src.size(), cudaMemcpyHostToDevice, st));
+      knn::launch_gather_sets(dsrc, (int)src.size(), o.dtype, g.d, X, g.dpad, st);
+      log.add();
+    } else {
+      for (size_t a = 0; a < g.order.size(); ++a) {
+        const knn_dataset& ds = sets[g.order[a]];
+        rc = upload_rows(C, ds.points, ds.n, g.d, o.dtype, false, X + (size_t)g.hsegs[a].off * g.dpad, g.dpad, st,
+                         log);
+        if (rc) return rc;
+      }
     }
     KNN_CK(cudaMemcpyAsync(dsegs, g.hsegs.data(), sizeof(knn::SegEntry) * nseg, cudaMemcpyHostToDevice, st));
     // compute: replay a captured graph of this shape, capture it on its second
@@ -828,7 +988,7 @@ int batch_impl(knn_context* C, const knn_dataset* sets, int count, int32_t k, in
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         KNN_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        const int crc = group_compute(C, g, k, trees, props, metric, o.precision, X, dsegs, seg_of, norms,
+        const int crc = group_compute(C, g, k, trees, props, metric, o, false, X, dsegs, seg_of, norms,
                                       err_flag, od, oi, st, glog);
         cudaError_t e = cudaStreamEndCapture(st, &graph);
         if (crc == KNN_OK && e == cudaSuccess && C->generation == gen0) e = cudaGraphInstantiate(&exec, graph, 0);
@@ -855,9 +1015,19 @@ int batch_impl(knn_context* C, const knn_dataset* sets, int count, int32_t k, in
       }
     }
     if (!done) {
-      rc = group_compute(C, g, k, trees, props, metric, o.precision, X, dsegs, seg_of, norms, err_flag, od, oi, st,
-                         log);
+      rc = group_compute(C, g, k, trees, props, metric, o, cs == cudaStreamCaptureStatusNone, X, dsegs, seg_of,
+                         norms, err_flag, od, oi, st, log, timed);
       if (rc) return rc;
+      if (timed) {  // stage times summed over the groups
+        float a = 0, b = 0, c = 0;
+        KNN_CK(cudaEventSynchronize(C->ev[4]));
+        KNN_CK(cudaEventElapsedTime(&a, C->ev[1], C->ev[2]));
+        KNN_CK(cudaEventElapsedTime(&b, C->ev[2], C->ev[3]));
+        KNN_CK(cudaEventElapsedTime(&c, C->ev[3], C->ev[4]));
+        stage_ms[0] += a;
+        stage_ms[1] += b;
+        stage_ms[2] += c;
+      }
     }
     // outputs
     const cudaMemcpyKind kind = o.outputs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
@@ -884,6 +1054,9 @@ int batch_impl(knn_context* C, const knn_dataset* sets, int count, int32_t k, in
     float ms = 0;
     KNN_CK(cudaEventElapsedTime(&ms, C->ev[0], C->ev[5]));
     stats->ms_total = ms;
+    stats->ms_trees = stage_ms[0];
+    stats->ms_leaf = stage_ms[1];
+    stats->ms_propagate = stage_ms[2];
     stats->launches = log.count;
     stats->props_run = props;
   }

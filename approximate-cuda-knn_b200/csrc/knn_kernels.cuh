@@ -57,6 +57,8 @@ struct LeafArgs {
   float* rkey;           // [n][k] in/out, sorted
   uint32_t* rid;         // [n][k] in/out
   unsigned long long* pair_counter;  // optional
+  int tile;              // 32 or 64 (0: 64): query x candidate tile, results identical
+  int first_tree;        // trees [first_tree, first_tree + trees) of perm
   cudaStream_t stream;
 };
 int leaf_stage(const LeafArgs& a, LaunchLog& log);
@@ -94,6 +96,7 @@ struct PropArgs {
   uint32_t* id_out;
   uint32_t* flags_out;       // [n][kw]
   unsigned long long* cand_counter;  // optional
+  int warps;                 // warps per block (0: as many as shared memory allows, at most 8)
   cudaStream_t stream;
 };
 int propagate_step(const PropArgs& a, LaunchLog& log);
@@ -150,5 +153,13 @@ void launch_finalize_local(const float* key, const uint32_t* id, int64_t ntot, i
                            const int32_t* seg_of, const SegEntry* segs, float* out_dist, int32_t* out_idx,
                            cudaStream_t st);
 void launch_fill_seg_of(const SegEntry* segs, int count, int32_t* seg_of, cudaStream_t st);
+// Device rows of several sets ([n][d], element type dtype) gathered into one
+// padded array at row offsets `off`, in one launch.
+struct RowSource {
+  const void* src;
+  int64_t n, off;
+};
+void launch_gather_sets(const RowSource* sets, int count, int dtype, int d, float* dst, int dpad,
+                        cudaStream_t st);
 
 }  // namespace knn

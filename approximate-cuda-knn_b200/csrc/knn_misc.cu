@@ -53,6 +53,18 @@ __global__ void k_pad_rows(const T* __restrict__ src, int64_t n, int d, int64_t 
   dst[g] = c < d ? to_f32<T>(src[i * ld + c]) : 0.0f;
 }
 
+// Rows of many device point sets into one padded float32 array: block (x, y)
+// copies rows y, y + gridDim.y, ... of set x.
+template <typename T>
+__global__ void k_gather_sets(const RowSource* __restrict__ sets, int d, float* __restrict__ dst, int dpad) {
+  const RowSource s = sets[blockIdx.x];
+  const T* src = static_cast<const T*>(s.src);
+  for (int64_t i = blockIdx.y; i < s.n; i += gridDim.y) {
+    float* out = dst + (size_t)(s.off + i) * dpad;
+    for (int c = threadIdx.x; c < dpad; c += blockDim.x) out[c] = c < d ? to_f32<T>(src[i * d + c]) : 0.0f;
+  }
+}
+
 __global__ void k_finalize(const float* __restrict__ key, const uint32_t* __restrict__ id,
                            int64_t count, int metric, float* __restrict__ dist,
                            int32_t* __restrict__ idx) {
@@ -127,6 +139,14 @@ void launch_finalize_local(const float* key, const uint32_t* id, int64_t ntot, i
                            cudaStream_t st) {
   k_finalize_local<<<blocks_for(ntot * k, 256), 256, 0, st>>>(key, id, ntot, k, metric, seg_of, segs, out_dist,
                                                                out_idx);
+}
+void launch_gather_sets(const RowSource* sets, int count, int dtype, int d, float* dst, int dpad,
+                        cudaStream_t st) {
+  dim3 grid((unsigned)count, 128);
+  const int threads = dpad >= 128 ? 128 : 64;
+  if (dtype == KNN_F16) k_gather_sets<__half><<<grid, threads, 0, st>>>(sets, d, dst, dpad);
+  else if (dtype == KNN_BF16) k_gather_sets<__nv_bfloat16><<<grid, threads, 0, st>>>(sets, d, dst, dpad);
+  else k_gather_sets<float><<<grid, threads, 0, st>>>(sets, d, dst, dpad);
 }
 void launch_fill_seg_of(const SegEntry* segs, int count, int32_t* seg_of, cudaStream_t st) {
   k_fill_seg_of<<<(unsigned)count, 256, 0, st>>>(segs, seg_of);

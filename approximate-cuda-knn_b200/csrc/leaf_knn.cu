@@ -19,18 +19,36 @@
 namespace knn {
 
 namespace {
-constexpr int kTile = 64;   // queries x candidates per tile
 constexpr int kDC = 32;     // dims staged per chunk
-constexpr int kSP = kTile + 4;
 }  // namespace
 
-template <int METRIC, int KPL>
+// Register tile of R consecutive floats from shared memory (R = 2 or 4).
+template <int R>
+__device__ __forceinline__ void load_r(const float* p, float (&v)[R]) {
+  if constexpr (R == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  } else {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    v[0] = t.x; v[1] = t.y;
+  }
+}
+
+// TILE x TILE (query x candidate) tiles, 16 x 16 threads each holding an
+// R x R register tile, R = TILE / 16.  Every key is summed over dims in the
+// same order whatever the tile, and each row's list is the k best of the
+// union under (key, id), so all TILE variants give identical lists.
+template <int METRIC, int KPL, int TILE>
 __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d, int dpad,
                                               SegView segs, int k,
                                               const int32_t* __restrict__ perm,
                                               const float* __restrict__ norms,
                                               float* __restrict__ rkey, uint32_t* __restrict__ rid,
                                               unsigned long long* __restrict__ pair_counter) {
+  constexpr int kTile = TILE;
+  constexpr int kSP = TILE + 4;
+  constexpr int R = TILE / 16;
+  static_assert(R == 2 || R == 4, "tile of 32 or 64");
   __shared__ __align__(16) float Qs[kDC][kSP];
   __shared__ __align__(16) float Cs[kDC][kSP];
   __shared__ float Ks[kTile][kTile + 1];
@@ -66,18 +84,18 @@ __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d
       }
       __syncthreads();
 
-      float part[4][4], total[4][4];
+      float part[R][R], total[R][R];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < R; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
+        for (int b = 0; b < R; ++b) {
           part[a][b] = 0.f;
           total[a][b] = 0.f;
         }
       for (int ch = 0; ch < nchunks; ++ch) {
         const int cd = ch * kDC;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < kTile / 32; ++h) {
           const int f = tid + h * 256;
           const int r = f >> 3, c4 = f & 7;
           const int dim = cd + 4 * c4;
@@ -96,20 +114,19 @@ __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d
         __syncthreads();
 #pragma unroll 8
         for (int dd = 0; dd < kDC; ++dd) {
-          const float4 a4 = *reinterpret_cast<const float4*>(&Qs[dd][ty * 4]);
-          const float4 b4 = *reinterpret_cast<const float4*>(&Cs[dd][tx * 4]);
-          const float qa[4] = {a4.x, a4.y, a4.z, a4.w};
-          const float cb[4] = {b4.x, b4.y, b4.z, b4.w};
+          float qa[R], cb[R];
+          load_r<R>(&Qs[dd][ty * R], qa);
+          load_r<R>(&Cs[dd][tx * R], cb);
 #pragma unroll
-          for (int a = 0; a < 4; ++a)
+          for (int a = 0; a < R; ++a)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) part[a][b] = acc_step<METRIC>(qa[a], cb[b], part[a][b]);
+            for (int b = 0; b < R; ++b) part[a][b] = acc_step<METRIC>(qa[a], cb[b], part[a][b]);
         }
         if (((cd + kDC) & 255) == 0 || ch == nchunks - 1) {
 #pragma unroll
-          for (int a = 0; a < 4; ++a)
+          for (int a = 0; a < R; ++a)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) {
+            for (int b = 0; b < R; ++b) {
               total[a][b] = __fadd_rn(total[a][b], part[a][b]);
               part[a][b] = 0.f;
             }
@@ -117,10 +134,10 @@ __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d
         __syncthreads();
       }
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < R; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const int qq = ty * 4 + a, cc = tx * 4 + b;
+        for (int b = 0; b < R; ++b) {
+          const int qq = ty * R + a, cc = tx * R + b;
           float key = total[a][b];
           if (METRIC == KNN_METRIC_COSINE) key = cosine_key(key, qnorm[qq], cnorm[cc]);
           Ks[qq][cc] = (qq < mq && cc < mc) ? key : kInf;
@@ -171,23 +188,29 @@ __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d
   }
 }
 
+template <int METRIC, int TILE>
+static void launch_leaf_tile(const LeafArgs& a, const int32_t* perm, int kpl) {
+  dim3 grid((unsigned)a.leaves);
+  if (kpl == 1)
+    k_leaf<METRIC, 1, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+  else if (kpl == 2)
+    k_leaf<METRIC, 2, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+  else
+    k_leaf<METRIC, 4, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+}
+
 template <int METRIC>
 static void launch_leaf_metric(const LeafArgs& a, int t, int kpl) {
   const int32_t* perm = a.perm + (size_t)t * a.n;
-  dim3 grid((unsigned)a.leaves);
-  if (kpl == 1)
-    k_leaf<METRIC, 1><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
-  else if (kpl == 2)
-    k_leaf<METRIC, 2><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
-  else
-    k_leaf<METRIC, 4><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+  if (a.tile == 32) launch_leaf_tile<METRIC, 32>(a, perm, kpl);
+  else launch_leaf_tile<METRIC, 64>(a, perm, kpl);
 }
 
 // One launch per tree: a point sits in one leaf per tree, so the leaves of a
 // tree update disjoint lists, and stream order serialises the trees.
 int leaf_stage(const LeafArgs& a, LaunchLog& log) {
   const int kpl = kpl_for(a.k);
-  for (int t = 0; t < a.trees; ++t) {
+  for (int t = a.first_tree; t < a.first_tree + a.trees; ++t) {
     if (a.metric == KNN_METRIC_EUCLIDEAN) launch_leaf_metric<KNN_METRIC_EUCLIDEAN>(a, t, kpl);
     else if (a.metric == KNN_METRIC_TAXICAB) launch_leaf_metric<KNN_METRIC_TAXICAB>(a, t, kpl);
     else launch_leaf_metric<KNN_METRIC_COSINE>(a, t, kpl);

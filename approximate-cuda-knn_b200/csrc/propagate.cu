@@ -243,6 +243,7 @@ int propagate_step(const PropArgs& a, LaunchLog& log) {
   int wpb = (int)(kPropSmemBudget / wb);
   if (wpb > kPropMaxWarps) wpb = kPropMaxWarps;
   if (wpb < 1) return KNN_ERR_UNSUPPORTED;
+  if (a.warps > 0 && a.warps < wpb) wpb = a.warps;  // a tuned block size (results identical)
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

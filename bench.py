@@ -401,6 +401,185 @@ def run_ours(args, w):
     return 0
 
 
+# ------------------------------------------------------- single-build case --
+def run_single(args, w):
+    """One configuration, W warm-up builds then K timed builds on device-resident
+    points; prints per-stage times.  The case the ncu summaries in profiles/
+    are taken on (a fixed, committed command line)."""
+    import torch
+
+    torch.cuda.set_device(0)
+    acknn = load_package()
+    lib = acknn.load_library()
+    n, d, k, metric = w["n"], w["d"], w["k"], w["metric"]
+    p = dict(TARGET_PARAMS)
+    for key in ("trees", "leaf", "props"):
+        if getattr(args, key) is not None:
+            p[key] = getattr(args, key)
+    prec = acknn.PREC_BF16_RERANK if args.single == "mixed" else acknn.PREC_FP32
+    x = torch.from_numpy(make_points(acknn, n, seed=args.seed)).cuda()
+    idx = torch.empty((n, k), dtype=torch.int32, device="cuda")
+    dist = torch.empty((n, k), dtype=torch.float32, device="cuda")
+    ctx = acknn.Context(0)
+    stream = torch.cuda.current_stream()
+
+    def build(stats=None):
+        opt = acknn.default_options(points_on_device=1, outputs_on_device=1, stream=stream.cuda_stream,
+                                    precision=prec)
+        rc = lib.knn_build_ex(ctx.handle, x.data_ptr(), n, d, k, p["trees"], p["leaf"], p["props"], metric,
+                              args.seed, idx.data_ptr(), dist.data_ptr(), ctypes.byref(opt),
+                              ctypes.byref(stats) if stats is not None else None)
+        if rc:
+            raise acknn.KnnError(rc, lib.knn_last_error().decode())
+
+    for _ in range(args.warmup):
+        build()
+    st = acknn.KnnStats()
+    st.struct_size = ctypes.sizeof(acknn.KnnStats)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        build()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    build(stats=st)
+    torch.cuda.synchronize()
+    sd = st.as_dict()
+    print(json.dumps({"case": args.single, "workload": workload_desc(w, p), "ms_per_build": ms,
+                      "points_per_s": n / (ms / 1e3),
+                      "stages_ms": {kk: sd[kk] for kk in ("ms_trees", "ms_leaf", "ms_propagate", "ms_total")},
+                      "launches": sd["launches"], "depth": sd["depth"]}), flush=True)
+    ctx.close()
+    return 0
+
+
+# ---------------------------------------------------------- dataset batch --
+def run_batch(args):
+    """The 256-dataset batch: N log-uniform in [1e3, 2e5], d uniform over
+    {32, 64, 128, 256}, 16-cluster Gaussian mixtures, seeds 0..255; k=15, 8
+    trees, leaf 48, 3 propagations, EUCLIDEAN.  Times (device-resident sets) a
+    loop of single plain-FP32 builds, the batched plain-FP32 build and the
+    batched mixed-precision build (autotuned shapes, captured graphs replayed),
+    plus the batched mixed build end to end from pinned host buffers; recall
+    per set against the FP64 exact graph on up to 500 queries per set."""
+    import torch
+
+    torch.cuda.set_device(0)
+    acknn = load_package()
+    lib = acknn.load_library()
+    cfg = acknn.workloads.CONFIGS["dataset_batch"]
+    count = args.count or cfg["count"]
+    k, T, L, P, metric = cfg["k"], cfg["trees"], cfg["leaf"], cfg["props"], cfg["metric"]
+    xs = [acknn.workloads.batch_dataset(s) for s in range(count)]
+    ntot = sum(x.shape[0] for x in xs)
+    xh = [torch.from_numpy(x).pin_memory() for x in xs]
+    xd = [t.cuda() for t in xh]
+    oi = [torch.empty((x.shape[0], k), dtype=torch.int32, device="cuda") for x in xs]
+    od = [torch.empty((x.shape[0], k), dtype=torch.float32, device="cuda") for x in xs]
+    hi = [torch.empty((x.shape[0], k), dtype=torch.int32).pin_memory() for x in xs]
+    hd = [torch.empty((x.shape[0], k), dtype=torch.float32).pin_memory() for x in xs]
+    ctx = acknn.Context(0)
+    stream = torch.cuda.current_stream()
+
+    def table(host):
+        arr = (acknn.KnnDataset * count)()
+        for i, x in enumerate(xs):
+            arr[i].points = (xh if host else xd)[i].data_ptr()
+            arr[i].n, arr[i].d, arr[i].seed = x.shape[0], x.shape[1], i
+            arr[i].out_idx = (hi if host else oi)[i].data_ptr()
+            arr[i].out_dist = (hd if host else od)[i].data_ptr()
+        return arr
+
+    dev_tab, host_tab = table(False), table(True)
+
+    def batch(prec, host=False):
+        opt = acknn.default_options(points_on_device=0 if host else 1, outputs_on_device=0 if host else 1,
+                                    stream=stream.cuda_stream, precision=prec, autotune=1)
+        rc = lib.knn_build_batch(ctx.handle, host_tab if host else dev_tab, count, k, T, L, P, metric,
+                                 ctypes.byref(opt), None)
+        if rc:
+            raise acknn.KnnError(rc, lib.knn_last_error().decode())
+
+    def loop(prec):
+        for i, x in enumerate(xs):
+            opt = acknn.default_options(points_on_device=1, outputs_on_device=1, stream=stream.cuda_stream,
+                                        precision=prec)
+            rc = lib.knn_build_ex(ctx.handle, xd[i].data_ptr(), x.shape[0], x.shape[1], k, T, L, P, metric, i,
+                                  oi[i].data_ptr(), od[i].data_ptr(), ctypes.byref(opt), None)
+            if rc:
+                raise acknn.KnnError(rc, lib.knn_last_error().decode())
+
+    def timed(fn, steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    res = {}
+    for name, fn in (("loop_plain_fp32", lambda: loop(acknn.PREC_FP32)),
+                     ("batch_plain_fp32", lambda: batch(acknn.PREC_FP32)),
+                     ("batch_mixed", lambda: batch(acknn.PREC_BF16_RERANK))):
+        for _ in range(args.warmup):
+            fn()
+        clocks = ClockSampler(0)
+        clocks.start()
+        ms = timed(fn, args.steps)
+        res[name] = {"ms_per_step": ms, "points_per_s": ntot / (ms / 1e3), "clocks": clocks.stop()}
+    # per-stage device times of one batched build of each precision (stats mode: eager launches)
+    for name, prec in (("batch_plain_fp32", acknn.PREC_FP32), ("batch_mixed", acknn.PREC_BF16_RERANK)):
+        st = acknn.KnnStats()
+        st.struct_size = ctypes.sizeof(acknn.KnnStats)
+        opt = acknn.default_options(points_on_device=1, outputs_on_device=1, stream=stream.cuda_stream,
+                                    precision=prec, autotune=1)
+        rc = lib.knn_build_batch(ctx.handle, dev_tab, count, k, T, L, P, metric, ctypes.byref(opt),
+                                 ctypes.byref(st))
+        if rc:
+            raise acknn.KnnError(rc, lib.knn_last_error().decode())
+        res[name]["stages_ms"] = {"trees": st.ms_trees, "leaf": st.ms_leaf, "propagate": st.ms_propagate,
+                                  "total": st.ms_total}
+    # batched mixed graphs stay in the device outputs: per-set recall
+    rec = []
+    rng = np.random.Generator(np.random.PCG64(7))
+    for i, x in enumerate(xs):
+        q = np.sort(rng.choice(x.shape[0], size=min(500, x.shape[0]), replace=False)).astype(np.int64)
+        ei, _ = acknn.exact_fp64(x, k, q, metric)
+        ai = oi[i].cpu().numpy()[q]
+        rec.append(sum(len(np.intersect1d(a, b)) for a, b in zip(ai, ei)) / (k * len(q)))
+    for _ in range(args.warmup):
+        batch(acknn.PREC_BF16_RERANK, host=True)
+    ms_e2e = timed(lambda: batch(acknn.PREC_BF16_RERANK, host=True), args.steps)
+    same = all(torch.equal(oi[i].cpu(), hi[i]) for i in range(count))
+    value = res["batch_mixed"]["points_per_s"]
+    line = {
+        "metric": "k-NN graph points/s over a batch of independent datasets (aggregate)",
+        "value": value, "unit": "points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["batch_mixed"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16+f32", "data": "synthetic (seeded Gaussian mixtures)",
+        "config": {"workload": f"{count} datasets, N log-uniform in [1e3, 2e5] (total {ntot:,}), d in "
+                               f"{{32,64,128,256}}, 16 clusters each, seeds 0..{count - 1}; k={k}, {T} trees, "
+                               f"leaf {L}, {P} propagations, EUCLIDEAN",
+                   "path": "knn_build_batch, BF16 tcgen05 leaf tiles + FP32 re-rank, autotuned shapes, "
+                           "captured graphs replayed"},
+        "paths": res,
+        "batch_vs_loop_plain": res["batch_plain_fp32"]["points_per_s"] / res["loop_plain_fp32"]["points_per_s"],
+        "mixed_vs_loop_plain": value / res["loop_plain_fp32"]["points_per_s"],
+        "recall_per_set": {"min": min(rec), "mean": sum(rec) / len(rec),
+                           "sets_below_0.95": int(sum(r < 0.95 for r in rec))},
+        "e2e": {"value": ntot / (ms_e2e / 1e3), "unit": "points/s", "ms_per_step": ms_e2e,
+                "h2d_bytes_per_step": int(sum(x.nbytes for x in xs)), "d2h_bytes_per_step": int(ntot * k * 8),
+                "matches_device_run": same},
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -411,6 +590,13 @@ def main():
     ap.add_argument("--n", type=int, default=None, help="override N (smaller runs)")
     ap.add_argument("--cpu-sample", type=int, default=20_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["integer_mixture", "dataset_batch"], default="integer_mixture")
+    ap.add_argument("--count", type=int, default=None, help="datasets in the batch workload")
+    ap.add_argument("--single", choices=["mixed", "plain"], default=None,
+                    help="time one configuration only (the profiling case)")
+    ap.add_argument("--trees", type=int, default=None)
+    ap.add_argument("--leaf", type=int, default=None)
+    ap.add_argument("--props", type=int, default=None)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -419,6 +605,10 @@ def main():
         w["n"] = args.n
     if args.impl == "reference":
         return run_reference(args, w)
+    if args.workload == "dataset_batch":
+        return run_batch(args)
+    if args.single:
+        return run_single(args, w)
     return run_ours(args, w)
 
 

@@ -74,7 +74,12 @@ typedef struct knn_options {
   void* stream;              /* cudaStream_t; NULL: the context's own stream          */
   int32_t mlp_sample;        /* learned splits: points in the training sample (0: 65536) */
   int32_t mlp_steps;         /* learned splits: Adam steps (0: 300)                      */
-  int32_t reserved[6];
+  int32_t autotune;          /* 1: time the result-invariant launch shapes (FP32 leaf
+                                tile, propagation warps) on the first eager call of a
+                                workload and reuse the fastest from then on           */
+  int32_t leaf_tile;         /* FP32 leaf tile 32 or 64 (0: tuned, else 64)              */
+  int32_t prop_warps;        /* propagation warps per block 1..8 (0: tuned, else max)   */
+  int32_t reserved[3];
 } knn_options;
 
 typedef struct knn_stats {
@@ -92,8 +97,10 @@ typedef struct knn_stats {
   int64_t prop_candidates[KNN_MAX_PROPS]; /* keys evaluated per propagation iteration  */
   float ms_prop_iter[KNN_MAX_PROPS];      /* device time per propagation iteration     */
   float ms_learn;            /* learned splits: sample graph, training and embedding    */
+  int32_t leaf_tile;         /* leaf tile used: 32/64 FP32, 128 tensor-core             */
+  int32_t prop_warps;        /* propagation warps per block used (0: the default)       */
   int32_t reserved_pad;
-  int64_t reserved[7];
+  int64_t reserved[6];
 } knn_stats;
 
 typedef struct knn_context knn_context;
