@@ -165,7 +165,7 @@ __device__ __forceinline__ bool cand_less(float ka, uint32_t ia, float kb, uint3
 __host__ __device__ __forceinline__ int proj_group(int d) {
   int nc = (d + 3) / 4;
   int g = 1;
-  while (g < nc && g < 32) g <<= 1;
+  while (g < nc && g < 4) g <<= 1;
   return g;
 }
 

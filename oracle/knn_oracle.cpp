@@ -108,13 +108,13 @@ inline bool cand_less(const Cand& a, const Cand& b) {
 }
 
 // ------------------------------------------------------------ projection --
-// Projection x . v in the GPU's grouped order: G lanes (power of two, <= 32,
+// Projection x . v in the GPU's grouped order: G lanes (power of two, <= 4,
 // covering ceil(d/4) float4 chunks), lane l accumulates chunks l, l+G, ...
 // with fmaf, then an xor butterfly over the G lanes.
 inline int proj_group(int d) {
   int nc = (d + 3) / 4;
   int g = 1;
-  while (g < nc && g < 32) g <<= 1;
+  while (g < nc && g < 4) g <<= 1;
   return g;
 }
 float project(const float* x, const float* v, int d) {
