@@ -186,7 +186,8 @@ __global__ void __launch_bounds__(kUThreads, 2)
   float* qn = reinterpret_cast<float*>(cid + kBN);
   float* cn = qn + kBM;
   int* cnt = reinterpret_cast<int*>(cn + kBN);  // survivors of each row in the current round
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(cnt + kBM);
+  uint8_t* sq = reinterpret_cast<uint8_t*>(cnt + kBM);  // [128][kRound] their columns in the round
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sq + kBM * kRound);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
   int* status = reinterpret_cast<int*>(tmem_slot + 1);
 
@@ -279,47 +280,59 @@ __global__ void __launch_bounds__(kUThreads, 2)
         uint32_t v[32];
         tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)col0, v);
         const bool rv = r < mq;
-        const int32_t myid = qid[r];
         const float myn = qn[r];
+        // a superset of the keys that can still enter the row's list (the
+        // exact (key, id) rule, the self pair and listed ids are settled by
+        // the merge): one compare per column, survivors as a bit mask
         const float tk = Lk[r * kLS + kq - 1];
-        const uint32_t ti = Li[r * kLS + kq - 1];
-        int survivors = 0;
+        uint32_t mask = 0;
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
           const int c = col0 + j;
           const float dot = __uint_as_float(v[j]);
           const float key = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[c]))
                                                            : __fsub_rn(1.f, dot);
-          // only keys that can still enter the row's list survive
-          const bool s = rv && c < mc && cid[c] != myid && cand_less(key, (uint32_t)cid[c], tk, ti);
-          Ks[ks_at(r, half * 32 + j)] = s ? key : kInf;
-          survivors += s ? 1 : 0;
+          Ks[ks_at(r, half * 32 + j)] = key;
+          mask |= (rv && c < mc && key <= tk) ? (1u << j) : 0u;
         }
-        if (survivors) atomicAdd(&cnt[r], survivors);
+        if (mask) {
+          int slot = atomicAdd(&cnt[r], __popc(mask));
+          while (mask) {
+            const int j = __ffs(mask) - 1;
+            mask &= mask - 1;
+            sq[r * kRound + slot++] = (uint8_t)(half * 32 + j);
+          }
+        }
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       __syncthreads();
-      // one warp per query row with survivors: list one entry per lane; each
-      // survivor is checked against the list ids by one ballot and placed by
-      // warp_insert1
+      // one warp per query row with survivors, read from the row's queue: list
+      // one entry per lane; each survivor other than the row's own point is
+      // checked against the list ids by one ballot and placed by warp_insert1
+      // (which drops a candidate behind all 32 entries)
       for (int qq = warp; qq < mq; qq += kUThreads / 32) {
-        if (cnt[qq] == 0) continue;
+        const int ns = cnt[qq];
+        if (ns == 0) continue;
+        const uint32_t self = (uint32_t)qid[qq];
         float lk = Lk[qq * kLS + lane];
         uint32_t li = Li[qq * kLS + lane];
-        for (int cb = 0; cb < kRound; cb += 32) {
-          const float ck = Ks[ks_at(qq, cb + lane)];
-          const int c = rb + cb + lane;
-          const uint32_t ci = c < mc ? (uint32_t)cid[c] : kNoId;
-          uint32_t bal = __ballot_sync(0xFFFFFFFFu, ck < kInf);
+        for (int b0 = 0; b0 < ns; b0 += 32) {
+          const int e = b0 + lane;
+          float ck = kInf;
+          uint32_t ci = kNoId;
+          if (e < ns) {
+            const int col = sq[qq * kRound + e];
+            ck = Ks[ks_at(qq, col)];
+            ci = (uint32_t)cid[rb + col];
+          }
+          uint32_t bal = __ballot_sync(0xFFFFFFFFu, e < ns && ci != self);
           while (bal) {
             const int src = __ffs(bal) - 1;
             bal &= bal - 1;
             const float k1 = __shfl_sync(0xFFFFFFFFu, ck, src);
             const uint32_t i1 = __shfl_sync(0xFFFFFFFFu, ci, src);
-            const float tk = __shfl_sync(0xFFFFFFFFu, lk, kq - 1);
-            const uint32_t ti = __shfl_sync(0xFFFFFFFFu, li, kq - 1);
             const bool dup = __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
-            if (!dup && cand_less(k1, i1, tk, ti)) warp_insert1(lk, li, k1, i1);
+            if (!dup) warp_insert1(lk, li, k1, i1);
           }
         }
         Lk[qq * kLS + lane] = lk;
@@ -439,10 +452,11 @@ __global__ void __launch_bounds__(256) k_rerank(const float* __restrict__ X, int
 }
 
 size_t umma_smem_bytes(int Kp) {
-  // alignment slack + A + B (also the round keys) + lists + (qid, cid, qn, cn) + cnt + barrier words
+  // alignment slack + A + B (also the round keys) + lists + (qid, cid, qn, cn) + cnt + survivor
+  // queues + barrier words
   const size_t bbytes = std::max((size_t)(Kp / kKC) * kChunkBytes, (size_t)kKsBytes);
   return 1024 + (size_t)(Kp / kKC) * kChunkBytes + bbytes + (size_t)kBM * kLS * 8 +
-         (size_t)(kBM + kBN) * 8 + (size_t)kBM * 4 + 64;
+         (size_t)(kBM + kBN) * 8 + (size_t)kBM * 4 + (size_t)kBM * kRound + 64;
 }
 
 int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
