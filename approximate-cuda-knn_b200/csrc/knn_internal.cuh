@@ -293,6 +293,19 @@ __device__ __forceinline__ void warp_merge_pair(K& ak, uint32_t& ai, K& bk, uint
   warp_bitonic_merge32(bk, bi);
 }
 
+// a <- the 32 smallest of two ascending 32-lists a and b (b is left as is).
+template <typename K>
+__device__ __forceinline__ void warp_merge_lower(K& ak, uint32_t& ai, K bk, uint32_t bi) {
+  const int lane = threadIdx.x & 31;
+  const K rk = __shfl_sync(0xFFFFFFFFu, bk, 31 - lane);
+  const uint32_t ri = __shfl_sync(0xFFFFFFFFu, bi, 31 - lane);
+  if (cand_less(rk, ri, ak, ai)) {  // min(a, reversed b) is bitonic
+    ak = rk;
+    ai = ri;
+  }
+  warp_bitonic_merge32(ak, ai);
+}
+
 // Insert 32 candidates (one per lane, unsorted, +inf for none) into the list,
 // keeping its 32*KPL smallest.  The 32*KPL smallest of list u candidates are
 // the first KPL-1 registers plus the 32 smallest of (last register u

@@ -42,6 +42,7 @@ constexpr int kChunkBytes = kBM * 128; // one 128 x 64 bf16 operand chunk
 constexpr uint32_t kTmemCols = 128;
 constexpr int kUThreads = 256;
 constexpr int kRound = 64;          // tile columns per epilogue round
+constexpr int kBulkMerge = 12;      // first tree: survivors in a chunk from which sort + merge pays
 // Round keys live in the B-operand region once the tile's MMA has completed:
 // 128 rows x 64 floats (32 KB), column index xor-swizzled by the row at 32-float
 // granularity so that row-parallel writes and column-parallel reads hit distinct banks.
@@ -167,7 +168,10 @@ __device__ __forceinline__ void stage_operand(unsigned char* op, const __nv_bflo
 // then a per-row merge of the survivors.  Prologue, MMA issue, bounded wait
 // and the tensor-memory loads follow the single-tile sequence that was checked
 // on its own against a CPU product.
-template <int METRIC>
+// FIRST: the launch of the first tree, whose lists start empty; a point then
+// meets every candidate once, so no survivor can already be listed, and a
+// chunk with many survivors is sorted and merged into the list in one go.
+template <int METRIC, bool FIRST>
 __global__ void __launch_bounds__(kUThreads, 2)
     k_leaf_tc(const __nv_bfloat16* __restrict__ Xb, int Kp, SegView segs, int k, int kq,
               int qtiles, const int32_t* __restrict__ perm, const float* __restrict__ norms2,
@@ -282,8 +286,8 @@ __global__ void __launch_bounds__(kUThreads, 2)
         const bool rv = r < mq;
         const float myn = qn[r];
         // a superset of the keys that can still enter the row's list (the
-        // exact (key, id) rule, the self pair and listed ids are settled by
-        // the merge): one compare per column, survivors as a bit mask
+        // exact (key, id) rule and listed ids are settled by the merge): one
+        // compare per column, survivors as a bit mask
         const float tk = Lk[r * kLS + kq - 1];
         uint32_t mask = 0;
 #pragma unroll
@@ -295,6 +299,9 @@ __global__ void __launch_bounds__(kUThreads, 2)
           Ks[ks_at(r, half * 32 + j)] = key;
           mask |= (rv && c < mc && key <= tk) ? (1u << j) : 0u;
         }
+        // the row's own point (its leaf lies inside the block) never survives
+        const int64_t selfbit = (lo + q0 + r) - blo - c0 - col0;
+        if (selfbit >= 0 && selfbit < 32) mask &= ~(1u << (int)selfbit);
         if (mask) {
           int slot = atomicAdd(&cnt[r], __popc(mask));
           while (mask) {
@@ -307,13 +314,12 @@ __global__ void __launch_bounds__(kUThreads, 2)
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       __syncthreads();
       // one warp per query row with survivors, read from the row's queue: list
-      // one entry per lane; each survivor other than the row's own point is
-      // checked against the list ids by one ballot and placed by warp_insert1
-      // (which drops a candidate behind all 32 entries)
+      // one entry per lane; each survivor is checked against the list ids by
+      // one ballot and placed by warp_insert1 (which drops a candidate behind
+      // all 32 entries)
       for (int qq = warp; qq < mq; qq += kUThreads / 32) {
         const int ns = cnt[qq];
         if (ns == 0) continue;
-        const uint32_t self = (uint32_t)qid[qq];
         float lk = Lk[qq * kLS + lane];
         uint32_t li = Li[qq * kLS + lane];
         for (int b0 = 0; b0 < ns; b0 += 32) {
@@ -325,13 +331,18 @@ __global__ void __launch_bounds__(kUThreads, 2)
             ck = Ks[ks_at(qq, col)];
             ci = (uint32_t)cid[rb + col];
           }
-          uint32_t bal = __ballot_sync(0xFFFFFFFFu, e < ns && ci != self);
+          if (FIRST && ns - b0 >= kBulkMerge) {
+            warp_bitonic_sort32(ck, ci);
+            warp_merge_lower(lk, li, ck, ci);
+            continue;
+          }
+          uint32_t bal = __ballot_sync(0xFFFFFFFFu, e < ns);
           while (bal) {
             const int src = __ffs(bal) - 1;
             bal &= bal - 1;
             const float k1 = __shfl_sync(0xFFFFFFFFu, ck, src);
             const uint32_t i1 = __shfl_sync(0xFFFFFFFFu, ci, src);
-            const bool dup = __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
+            const bool dup = !FIRST && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
             if (!dup) warp_insert1(lk, li, k1, i1);
           }
         }
@@ -473,15 +484,21 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
   const int qtiles = (int)((a.maxleaf + kBM - 1) / kBM);
   for (int t = 0; t < a.trees; ++t) {
     const int32_t* perm = a.perm + (size_t)t * a.n;
+    const unsigned grid = (unsigned)(leaves * qtiles);
+#define KNN_TC_LAUNCH(M, F)                                                                               \
+  do {                                                                                                    \
+    cudaFuncSetAttribute(k_leaf_tc<M, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);       \
+    k_leaf_tc<M, F><<<grid, kUThreads, smem, st>>>(Xb, Kp, a.segs, a.k, a.kq, qtiles, perm, a.norms2, a.akey, \
+                                                   a.aid, a.err);                                        \
+  } while (0)
     if (a.metric == KNN_METRIC_EUCLIDEAN) {
-      cudaFuncSetAttribute(k_leaf_tc<KNN_METRIC_EUCLIDEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_leaf_tc<KNN_METRIC_EUCLIDEAN><<<(unsigned)(leaves * qtiles), kUThreads, smem, st>>>(
-          Xb, Kp, a.segs, a.k, a.kq, qtiles, perm, a.norms2, a.akey, a.aid, a.err);
+      if (t == 0) KNN_TC_LAUNCH(KNN_METRIC_EUCLIDEAN, true);
+      else KNN_TC_LAUNCH(KNN_METRIC_EUCLIDEAN, false);
     } else {
-      cudaFuncSetAttribute(k_leaf_tc<KNN_METRIC_COSINE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_leaf_tc<KNN_METRIC_COSINE><<<(unsigned)(leaves * qtiles), kUThreads, smem, st>>>(
-          Xb, Kp, a.segs, a.k, a.kq, qtiles, perm, a.norms2, a.akey, a.aid, a.err);
+      if (t == 0) KNN_TC_LAUNCH(KNN_METRIC_COSINE, true);
+      else KNN_TC_LAUNCH(KNN_METRIC_COSINE, false);
     }
+#undef KNN_TC_LAUNCH
     log.add();
   }
   const size_t rsm = (size_t)8 * (a.dpad + 32 * 64 + 32) * sizeof(float);
