@@ -252,6 +252,7 @@ int run_trees_segs(knn_context* C, const float* X, int64_t ntot, int d, int dpad
   if (!rc) rc = C->get("perm_node", (size_t)trees * ntot, &a.node);
   if (!rc) rc = C->get("keys", (size_t)trees * ntot, &a.keys);
   if (!rc) rc = C->get("dirs", knn::tree_dir_nodes(hsegs, nseg, trees) * dpad, &a.dirs);
+  if (!rc) rc = C->get("msplit", knn::msplit_scratch_bytes(hsegs[0].n), &a.msplit);
   if (rc) return rc;
   a.stream = st;
   rc = knn::tree_build(a, log);

@@ -11,6 +11,11 @@ namespace knn {
 // Keys of a node staged in shared memory by k_split when it has at most this
 // many points (96 KB).
 constexpr int kSplitSmemKeys = 12288;
+// Multi-block splits (levels with at most kMSplitMaxNodes split nodes and more
+// than 2 * kMChunk points in the largest): keys per block, and the scratch.
+constexpr int kMChunk = 8192;
+constexpr int kMSplitMaxNodes = 296;
+size_t msplit_scratch_bytes(int64_t max_node_points);
 
 // Counts kernel launches of one call.
 struct LaunchLog {
@@ -38,6 +43,7 @@ struct TreeArgs {
   int32_t* node;      // [trees][n] scratch: node of each point at the current level
   uint64_t* keys;     // [trees][n] scratch
   float* dirs;        // [tree_dir_nodes(...)][dpad] scratch
+  void* msplit;       // msplit_scratch_bytes(largest segment) scratch, or null (single-block splits)
   cudaStream_t stream;
 };
 int tree_build(const TreeArgs& a, LaunchLog& log);

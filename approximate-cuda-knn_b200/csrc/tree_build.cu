@@ -274,7 +274,230 @@ __global__ void __launch_bounds__(1024) k_split(int64_t ntot, int level, int tre
   }
 }
 
+// ------------------------------------------------------ multi-block split --
+// The top levels hold few nodes with many points each (level 0: one node of
+// all n points per tree), too few blocks for the GPU.  There every node is
+// spread over blocks of kMChunk keys: an MSB radix select over global
+// 256-bin histograms (one histogram pass and one select step per 8-bit
+// digit; a node stops once its target bucket holds a single key), then a
+// count pass and a stable scatter pass.  The pivot is the same order
+// statistic and the partition the same stable one as k_split's, so the trees
+// are identical.
+struct MSplitNode {
+  uint64_t prefix;  // known high digits of the pivot
+  int64_t rank;     // rank of the pivot among keys sharing those digits
+  int32_t shift;    // digits at and above `shift` are known
+  int32_t state;    // 0 selecting, 1 pivot known, 2 node not split (copy)
+};
+
+__device__ __forceinline__ void msplit_node(const SegView& segs, int level, int trees, int64_t s,
+                                            int64_t* lo, int64_t* hi, int64_t* mid, int* t, int64_t* j) {
+  const int64_t nodes = int64_t(1) << level;
+  const int a = (int)(s / (nodes * trees));
+  const int64_t r = s - (int64_t)a * nodes * trees;
+  *t = (int)(r / nodes);
+  *j = r - (int64_t)(*t) * nodes;
+  const SegEntry e = segs.get(a);
+  *lo = e.off + node_lo(e.n, level, *j);
+  *hi = e.off + node_lo(e.n, level, *j + 1);
+  *mid = e.off + node_lo(e.n, level + 1, 2 * (*j) + 1);
+}
+
+__global__ void k_msplit_init(SegView segs, int level, int trees, MSplitNode* st, uint32_t* hist) {
+  const int64_t s = blockIdx.x;
+  int64_t lo, hi, mid, j;
+  int t;
+  msplit_node(segs, level, trees, s, &lo, &hi, &mid, &t, &j);
+  const int64_t cnt = hi - lo, nl = mid - lo;
+  if (threadIdx.x == 0) {
+    st[s].prefix = 0;
+    st[s].rank = nl;
+    st[s].shift = 64;
+    st[s].state = (cnt < 2 || nl <= 0 || nl >= cnt) ? 2 : 0;
+  }
+  for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[s * 256 + b] = 0;
+}
+
+// One digit: block (b, s) histograms chunk b of node s.
+__global__ void __launch_bounds__(256) k_msplit_hist(SegView segs, int level, int trees, int64_t ntot, int pass,
+                                                     const uint64_t* __restrict__ keys,
+                                                     const MSplitNode* __restrict__ st, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t h[256];
+  const int64_t s = blockIdx.y;
+  const MSplitNode nd = st[s];
+  if (nd.state != 0) return;
+  int64_t lo, hi, mid, j;
+  int t;
+  msplit_node(segs, level, trees, s, &lo, &hi, &mid, &t, &j);
+  const int64_t c0 = lo + (int64_t)blockIdx.x * kMChunk;
+  if (c0 >= hi) return;
+  const int64_t c1 = min(hi, c0 + kMChunk);
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const int shift = 56 - 8 * pass;
+  const uint64_t* K = keys + (size_t)t * ntot;
+  for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+    const uint64_t key = K[i];
+    if (pass == 0 || (key >> (shift + 8)) == (nd.prefix >> (shift + 8))) atomicAdd(&h[(key >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  const uint32_t v = h[threadIdx.x];
+  if (v) atomicAdd(&hist[s * 256 + threadIdx.x], v);
+}
+
+// One digit: the bucket holding the target rank; histogram cleared for the next digit.
+__global__ void __launch_bounds__(256) k_msplit_select(int pass, MSplitNode* __restrict__ st, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t sum[8];
+  const int64_t s = blockIdx.x;
+  const MSplitNode nd = st[s];
+  if (nd.state != 0) return;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const uint32_t v = hist[s * 256 + tid];
+  uint32_t incl = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+    if (lane >= off) incl += o;
+  }
+  if (lane == 31) sum[w] = incl;
+  __syncthreads();
+  uint32_t before = 0;
+  for (int q = 0; q < w; ++q) before += sum[q];
+  const int64_t excl = (int64_t)before + incl - v;
+  const int shift = 56 - 8 * pass;
+  if (v > 0 && excl <= nd.rank && nd.rank < excl + (int64_t)v) {
+    MSplitNode out = nd;
+    out.prefix = nd.prefix | ((uint64_t)tid << shift);
+    out.rank = nd.rank - excl;
+    out.shift = shift;
+    out.state = (v == 1 || pass == 7) ? 1 : 0;
+    st[s] = out;
+  }
+  hist[s * 256 + tid] = 0;
+}
+
+__device__ __forceinline__ bool msplit_less(uint64_t key, const MSplitNode& nd) {
+  return (key >> nd.shift) < (nd.prefix >> nd.shift);
+}
+
+// Keys below the pivot in chunk b of node s.
+__global__ void __launch_bounds__(256) k_msplit_count(SegView segs, int level, int trees, int64_t ntot,
+                                                      const uint64_t* __restrict__ keys,
+                                                      const MSplitNode* __restrict__ st, int32_t* __restrict__ lcount,
+                                                      int nchunks) {
+  __shared__ int32_t red[8];
+  const int64_t s = blockIdx.y;
+  const MSplitNode nd = st[s];
+  int64_t lo, hi, mid, j;
+  int t;
+  msplit_node(segs, level, trees, s, &lo, &hi, &mid, &t, &j);
+  const int64_t c0 = lo + (int64_t)blockIdx.x * kMChunk;
+  const int64_t c1 = min(hi, c0 + kMChunk);
+  const uint64_t* K = keys + (size_t)t * ntot;
+  int32_t c = 0;
+  if (nd.state == 1)
+    for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) c += msplit_less(K[i], nd) ? 1 : 0;
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int32_t tot = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) tot += red[q];
+    lcount[s * nchunks + blockIdx.x] = tot;
+  }
+}
+
+// Stable scatter of chunk b of node s: left keys after the left keys of the
+// chunks before it, right keys after nl and the right keys before them.
+__global__ void __launch_bounds__(256) k_msplit_scatter(SegView segs, int level, int trees, int64_t ntot,
+                                                        const uint64_t* __restrict__ keys,
+                                                        const MSplitNode* __restrict__ st,
+                                                        const int32_t* __restrict__ lcount, int nchunks,
+                                                        const int32_t* __restrict__ perm,
+                                                        int32_t* __restrict__ perm_out, int32_t* __restrict__ inv,
+                                                        int32_t* __restrict__ node) {
+  __shared__ int64_t warp_sums[33];
+  __shared__ int64_t base_sh;
+  const int64_t s = blockIdx.y;
+  const MSplitNode nd = st[s];
+  int64_t lo, hi, mid, j;
+  int t;
+  msplit_node(segs, level, trees, s, &lo, &hi, &mid, &t, &j);
+  const int64_t c0 = lo + (int64_t)blockIdx.x * kMChunk;
+  if (c0 >= hi) return;
+  const int64_t c1 = min(hi, c0 + kMChunk);
+  const int32_t* Pin = perm + (size_t)t * ntot;
+  int32_t* Pout = perm_out + (size_t)t * ntot;
+  int32_t* Node = node + (size_t)t * ntot;
+  int32_t* Inv = inv + (size_t)t * ntot;
+  if (nd.state == 2) {  // not split: copy, children by position
+    for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+      const int32_t id = Pin[i];
+      Pout[i] = id;
+      Node[id] = (int32_t)(i < mid ? 2 * j : 2 * j + 1);
+    }
+    return;
+  }
+  if (threadIdx.x == 0) {
+    int64_t b = 0;
+    for (int q = 0; q < (int)blockIdx.x; ++q) b += lcount[s * nchunks + q];
+    base_sh = b;
+  }
+  __syncthreads();
+  const int64_t nl = mid - lo;
+  const uint64_t* K = keys + (size_t)t * ntot;
+  constexpr int ITEMS = 4;
+  const int64_t tile = (int64_t)blockDim.x * ITEMS;
+  int64_t left_base = base_sh;  // left keys before this tile, over the whole node
+  for (int64_t t0 = c0; t0 < c1; t0 += tile) {
+    const int64_t p0 = t0 + (int64_t)threadIdx.x * ITEMS;
+    bool f[ITEMS];
+    int c = 0;
+#pragma unroll
+    for (int q = 0; q < ITEMS; ++q) {
+      const int64_t p = p0 + q;
+      f[q] = p < c1 && msplit_less(K[p], nd);
+      c += f[q];
+    }
+    int64_t total;
+    int64_t before = block_excl_scan(c, warp_sums, &total) + left_base;
+#pragma unroll
+    for (int q = 0; q < ITEMS; ++q) {
+      const int64_t p = p0 + q;
+      if (p < c1) {
+        const int64_t rel = p - lo;
+        const int64_t dst = f[q] ? before : nl + (rel - before);
+        if (dst >= 0 && dst < hi - lo) {
+          const int32_t id = Pin[p];
+          Pout[lo + dst] = id;
+          Inv[id] = (int32_t)(lo + dst);
+          Node[id] = (int32_t)(f[q] ? 2 * j : 2 * j + 1);
+        }
+        before += f[q];
+      }
+    }
+    left_base += total;
+  }
+}
+
+// Ranges of the (segment, tree) pairs that no longer split, copied as they are.
+__global__ void k_copy_finished(SegView segs, int active, int trees, int64_t ntot, const int32_t* __restrict__ perm,
+                                int32_t* __restrict__ perm_out) {
+  const int a = active + (int)(blockIdx.x / trees);
+  const int t = (int)(blockIdx.x % trees);
+  const SegEntry e = segs.get(a);
+  for (int64_t i = threadIdx.x; i < e.n; i += blockDim.x)
+    perm_out[(size_t)t * ntot + e.off + i] = perm[(size_t)t * ntot + e.off + i];
+}
+
 // ------------------------------------------------------------------ host --
+size_t msplit_scratch_bytes(int64_t max_node_points) {
+  const int64_t chunks = (max_node_points + kMChunk - 1) / kMChunk;
+  return sizeof(MSplitNode) * kMSplitMaxNodes + sizeof(uint32_t) * 256 * kMSplitMaxNodes +
+         sizeof(int32_t) * (size_t)kMSplitMaxNodes * (size_t)(chunks > 0 ? chunks : 1);
+}
+
 size_t tree_dir_nodes(const SegEntry* hsegs, int nseg, int trees) {
   size_t best = 1;
   const int maxdepth = hsegs[0].depth;
@@ -332,12 +555,32 @@ int tree_build(const TreeArgs& a, LaunchLog& log) {
     if (threads < 64) threads = 64;
     if (threads > 1024) threads = 1024;
     const unsigned grid = (unsigned)(segs + (int64_t)(a.nseg - active) * a.trees);
-    if (maxcnt <= kSplitSmemKeys) {
+    if (a.msplit && segs <= kMSplitMaxNodes && maxcnt > 2 * kMChunk) {
+      const int nchunks = (int)((maxcnt + kMChunk - 1) / kMChunk);
+      MSplitNode* mst = static_cast<MSplitNode*>(a.msplit);
+      uint32_t* hist = reinterpret_cast<uint32_t*>(mst + kMSplitMaxNodes);
+      int32_t* lcount = reinterpret_cast<int32_t*>(hist + (size_t)kMSplitMaxNodes * 256);
+      const dim3 g2((unsigned)nchunks, (unsigned)segs);
+      k_msplit_init<<<(unsigned)segs, 256, 0, st>>>(a.segs, l, a.trees, mst, hist);
+      for (int pass = 0; pass < 8; ++pass) {
+        k_msplit_hist<<<g2, 256, 0, st>>>(a.segs, l, a.trees, ntot, pass, a.keys, mst, hist);
+        k_msplit_select<<<(unsigned)segs, 256, 0, st>>>(pass, mst, hist);
+      }
+      k_msplit_count<<<g2, 256, 0, st>>>(a.segs, l, a.trees, ntot, a.keys, mst, lcount, nchunks);
+      k_msplit_scatter<<<g2, 256, 0, st>>>(a.segs, l, a.trees, ntot, a.keys, mst, lcount, nchunks, cur, alt, a.inv,
+                                           a.node);
+      if (a.nseg > active)
+        k_copy_finished<<<(unsigned)((a.nseg - active) * a.trees), 256, 0, st>>>(a.segs, active, a.trees, ntot, cur,
+                                                                               alt);
+      log.add(19 + (a.nseg > active ? 1 : 0));
+    } else if (maxcnt <= kSplitSmemKeys) {
       k_split<true><<<grid, threads, (size_t)maxcnt * sizeof(uint64_t), st>>>(ntot, l, a.trees, a.segs, active, a.keys, cur, alt, a.inv, a.node);
+      log.add(1);
     } else {
       k_split<false><<<grid, threads, 0, st>>>(ntot, l, a.trees, a.segs, active, a.keys, cur, alt, a.inv, a.node);
+      log.add(1);
     }
-    log.add(3);
+    log.add(2);
     int32_t* tmp = cur;
     cur = alt;
     alt = tmp;

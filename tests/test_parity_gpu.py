@@ -93,6 +93,15 @@ def test_tree_large_node_path(lib, oracle):
                                   oracle.build_trees(x, 2, 50, seed=1))
 
 
+def test_tree_multiblock_split_ties(lib, oracle):
+    """Top levels with few, large nodes are split by several blocks per node
+    (global digit histograms, then a stable scatter); integer data gives many
+    tied projections, ordered by id."""
+    x = _rand(150000, 4, 5, "int")
+    np.testing.assert_array_equal(lib.build_trees(x, 3, 100, seed=3),
+                                  oracle.build_trees(x, 3, 100, seed=3))
+
+
 @pytest.mark.parametrize("metric", [0, 1, 2])
 def test_leaf_stage_identical(lib, oracle, metric):
     x = _rand(5000, 20, 9)
