@@ -23,6 +23,7 @@ import numpy as np
 
 from . import formats  # noqa: F401  (CSV / binary result formats)
 from . import workloads  # noqa: F401  (seeded synthetic point sets)
+from . import sharded  # noqa: F401  (multi-GPU builds over torch.distributed)
 
 PKG_DIR = Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR / "libacknn.so"
@@ -69,7 +70,10 @@ class KnnOptions(ctypes.Structure):
         ("autotune", ctypes.c_int32),
         ("leaf_tile", ctypes.c_int32),
         ("prop_warps", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 3),
+        ("tree_offset", ctypes.c_int32),
+        ("tree_stride", ctypes.c_int32),
+        ("raw_keys", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 4),
     ]
 
 
@@ -142,6 +146,9 @@ EXPORTS = {
     "knn_normalize_reference": (ctypes.c_int, [_P, _I64, _I32]),
     "knn_exact_fp64_noalloc": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _P, _I64, _P, _P, _P]),
     "knn_build_batch": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _I32, _I32, _I32, _P, _P]),
+    "knn_merge_lists": (ctypes.c_int, [_P, _P, _P, _I32, _I64, _I32, _I32, _I32, _P, _P, _P]),
+    "knn_propagate_range": (ctypes.c_int, [_P, _P, _I64, _I32, _I32, _I32, _I64, _I64, _P, _P, _P, _P, _P,
+                                           _P, _P]),
     "knn_mlp_param_count": (_I64, [_I32]),
     "knn_mlp_loss_grad": (ctypes.c_int, [_P, _I32, _P, _I32, ctypes.c_float, _P, _P]),
     "knn_mlp_train": (ctypes.c_int, [_P, _P, _I64, _I32, _I32, _I32, _U64, _P, _P, _P, _P, _P]),

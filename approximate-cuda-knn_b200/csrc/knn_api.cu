@@ -236,8 +236,10 @@ struct Trees {
 // Trees of a batch of segments (global positions), or of one point set.
 int run_trees_segs(knn_context* C, const float* X, int64_t ntot, int d, int dpad, int trees,
                    const knn::SegView& segs, const knn::SegEntry* hsegs, int nseg, cudaStream_t st,
-                   Trees* T, knn::LaunchLog& log) {
+                   Trees* T, knn::LaunchLog& log, int tree_offset = 0, int tree_stride = 1) {
   knn::TreeArgs a{};
+  a.tree_offset = tree_offset;
+  a.tree_stride = tree_stride > 0 ? tree_stride : 1;
   a.X = X;
   a.n = ntot;
   a.d = d;
@@ -263,7 +265,8 @@ int run_trees_segs(knn_context* C, const float* X, int64_t ntot, int d, int dpad
 }
 
 int run_trees(knn_context* C, const float* X, int64_t n, int d, int dpad, int trees, int leaf,
-              uint64_t seed, cudaStream_t st, Trees* T, knn::LaunchLog& log) {
+              uint64_t seed, cudaStream_t st, Trees* T, knn::LaunchLog& log, int tree_offset = 0,
+              int tree_stride = 1) {
   const int depth = knn::tree_depth(n, leaf);
   if (depth > 30) return fail(KNN_ERR_ARGS, "tree too deep (n / leaf too large)");
   knn::SegEntry e{};
@@ -272,7 +275,8 @@ int run_trees(knn_context* C, const float* X, int64_t n, int d, int dpad, int tr
   e.seed = seed;
   e.leaf_base = 0;
   e.depth = depth;
-  return run_trees_segs(C, X, n, d, dpad, trees, knn::single_segment(n, seed, depth), &e, 1, st, T, log);
+  return run_trees_segs(C, X, n, d, dpad, trees, knn::single_segment(n, seed, depth), &e, 1, st, T, log,
+                        tree_offset, tree_stride);
 }
 
 struct Lists {
@@ -633,6 +637,8 @@ int resolve_options(const knn_options* opt, knn_options* o) {
   if (o->leaf_tile != 0 && o->leaf_tile != 32 && o->leaf_tile != 64)
     return fail(KNN_ERR_ARGS, "leaf_tile must be 0, 32 or 64");
   if (o->prop_warps < 0 || o->prop_warps > 8) return fail(KNN_ERR_ARGS, "prop_warps must be in 0..8");
+  if (o->tree_offset < 0 || o->tree_stride < 0) return fail(KNN_ERR_ARGS, "negative tree offset or stride");
+  if (o->raw_keys < 0 || o->raw_keys > 1) return fail(KNN_ERR_ARGS, "raw_keys must be 0 or 1");
   return KNN_OK;
 }
 
@@ -683,7 +689,7 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
     if (timed) KNN_CK(cudaEventRecord(C->ev[6], st));
     rc = run_trees(C, Z, n, knn::kMlpEmbed, knn::kMlpEmbed, trees, leaf, seed, st, &T, log);
   } else {
-    rc = run_trees(C, P.X, n, d, P.dpad, trees, leaf, seed, st, &T, log);
+    rc = run_trees(C, P.X, n, d, P.dpad, trees, leaf, seed, st, &T, log, o.tree_offset, o.tree_stride);
   }
   if (rc) return rc;
   if (timed) KNN_CK(cudaEventRecord(C->ev[2], st));
@@ -733,7 +739,8 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
     if (!rc) rc = C->get("out_idx", (size_t)n * k, &di);
     if (rc) return rc;
   }
-  knn::launch_finalize(L.key[L.cur], L.id[L.cur], n, k, metric, dd, di, st);
+  // raw keys: no sqrt (the TAXICAB transform is the identity)
+  knn::launch_finalize(L.key[L.cur], L.id[L.cur], n, k, o.raw_keys ? KNN_METRIC_TAXICAB : metric, dd, di, st);
   log.add();
   if (!o.outputs_on_device) {
     KNN_CK(cudaMemcpyAsync(out_dist, dd, sizeof(float) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
@@ -1352,6 +1359,102 @@ int knn_normalize_reference(float* points, int64_t n, int32_t d) {
   knn::launch_normalize_reference(X, n, d, st);
   KNN_CK(cudaPeekAtLastError());
   KNN_CK(cudaMemcpyAsync(points, X, sizeof(float) * (size_t)n * d, cudaMemcpyDeviceToHost, st));
+  KNN_CK(cudaStreamSynchronize(st));
+  return KNN_OK;
+}
+
+int knn_merge_lists(knn_context* ctx, const int32_t* idx, const float* key, int32_t lists, int64_t n, int32_t k,
+                    int32_t metric, int32_t as_distance, int32_t* idx_out, float* key_out,
+                    const knn_options* opt) {
+  knn_options o;
+  int rc = resolve_options(opt, &o);
+  if (rc) return rc;
+  if (!idx || !key || !idx_out || !key_out) return fail(KNN_ERR_ARGS, "NULL pointer");
+  if (lists < 1 || n < 1 || n >= (int64_t)INT32_MAX || k < 1 || k > KNN_MAX_K)
+    return fail(KNN_ERR_ARGS, "size out of range");
+  if (metric < 0 || metric > 2 || as_distance < 0 || as_distance > 1) return fail(KNN_ERR_ARGS, "bad metric or mode");
+  rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  cudaStream_t st = o.stream ? static_cast<cudaStream_t>(o.stream) : ctx->stream;
+  const size_t in = (size_t)lists * n * k, out = (size_t)n * k;
+  const int32_t* di = idx;
+  const float* dk = key;
+  int32_t* oi = idx_out;
+  float* ok = key_out;
+  if (!o.points_on_device) {
+    int32_t* ti = nullptr;
+    float* tk = nullptr;
+    rc = ctx->get("ml_in_idx", in, &ti);
+    if (!rc) rc = ctx->get("ml_in_key", in, &tk);
+    if (!rc) rc = ctx->get("ml_out_idx", out, &oi);
+    if (!rc) rc = ctx->get("ml_out_key", out, &ok);
+    if (rc) return rc;
+    KNN_CK(cudaMemcpyAsync(ti, idx, sizeof(int32_t) * in, cudaMemcpyHostToDevice, st));
+    KNN_CK(cudaMemcpyAsync(tk, key, sizeof(float) * in, cudaMemcpyHostToDevice, st));
+    di = ti;
+    dk = tk;
+  }
+  knn::launch_merge_lists(di, dk, lists, n, k, oi, ok, st);
+  if (as_distance) {  // keys -> distances (ids without flag bits already)
+    knn::launch_finalize(ok, reinterpret_cast<const uint32_t*>(oi), n, k, metric, ok, oi, st);
+  }
+  KNN_CK(cudaPeekAtLastError());
+  if (!o.points_on_device) {
+    KNN_CK(cudaMemcpyAsync(idx_out, oi, sizeof(int32_t) * out, cudaMemcpyDeviceToHost, st));
+    KNN_CK(cudaMemcpyAsync(key_out, ok, sizeof(float) * out, cudaMemcpyDeviceToHost, st));
+  }
+  KNN_CK(cudaStreamSynchronize(st));
+  return KNN_OK;
+}
+
+int knn_propagate_range(knn_context* ctx, const void* points, int64_t n, int32_t d, int32_t k, int32_t metric,
+                        int64_t r0, int64_t r1, const int32_t* idx_in, const float* key_in,
+                        const uint32_t* flags_in, int32_t* idx_out, float* key_out, uint32_t* flags_out,
+                        const knn_options* opt) {
+  knn_options o;
+  int rc = resolve_options(opt, &o);
+  if (rc) return rc;
+  rc = check_common(points, n, d, k, metric);
+  if (rc) return rc;
+  if (!idx_in || !key_in || !idx_out || !key_out || !flags_out) return fail(KNN_ERR_ARGS, "NULL pointer");
+  if (r0 < 0 || r1 > n || r0 > r1) return fail(KNN_ERR_ARGS, "point range out of bounds");
+  rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  cudaStream_t st = o.stream ? static_cast<cudaStream_t>(o.stream) : ctx->stream;
+  knn::LaunchLog log;
+  Prepared P;
+  rc = prepare_points(ctx, points, n, d, o, st, &P, log);
+  if (rc) return rc;
+  float* norms = nullptr;
+  if (metric == KNN_METRIC_COSINE) {
+    rc = ctx->get("norms", (size_t)n, &norms);
+    if (rc) return rc;
+    knn::launch_norms(P.X, n, d, P.dpad, norms, st);
+  }
+  if (r1 > r0) {
+    knn::PropArgs a{};
+    a.X = P.X;
+    a.n = n;
+    a.d = d;
+    a.dpad = P.dpad;
+    a.k = k;
+    a.metric = metric;
+    a.norms = norms;
+    a.order = nullptr;
+    a.key_in = key_in;
+    a.id_in = reinterpret_cast<const uint32_t*>(idx_in);
+    a.flags_in = flags_in;
+    a.key_out = key_out;
+    a.id_out = reinterpret_cast<uint32_t*>(idx_out);
+    a.flags_out = flags_out;
+    a.r0 = r0;
+    a.r1 = r1;
+    a.warps = o.prop_warps;
+    a.stream = st;
+    rc = knn::propagate_step(a, log);
+    if (rc == KNN_ERR_UNSUPPORTED) return fail(rc, "propagation scratch exceeds shared memory (k or d too large)");
+    if (rc) return fail_cuda(cudaGetLastError(), "propagation launch");
+  }
   KNN_CK(cudaStreamSynchronize(st));
   return KNN_OK;
 }

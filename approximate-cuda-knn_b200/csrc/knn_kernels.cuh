@@ -34,6 +34,7 @@ struct TreeArgs {
   int64_t n;
   int d, dpad;
   int trees;
+  int tree_offset, tree_stride;  // local tree t is global tree tree_offset + t * tree_stride
   SegView segs;
   const SegEntry* hsegs;
   int nseg;
@@ -103,6 +104,7 @@ struct PropArgs {
   uint32_t* flags_out;       // [n][kw]
   unsigned long long* cand_counter;  // optional
   int warps;                 // warps per block (0: as many as shared memory allows, at most 8)
+  int64_t r0, r1;            // process points (order positions) [r0, r1); r1 = 0: all n
   cudaStream_t stream;
 };
 int propagate_step(const PropArgs& a, LaunchLog& log);
@@ -159,6 +161,10 @@ void launch_finalize_local(const float* key, const uint32_t* id, int64_t ntot, i
                            const int32_t* seg_of, const SegEntry* segs, float* out_dist, int32_t* out_idx,
                            cudaStream_t st);
 void launch_fill_seg_of(const SegEntry* segs, int count, int32_t* seg_of, cudaStream_t st);
+// out[i] = the k best distinct ids by (key, id) of `lists` candidate lists
+// [lists][n][k] of each point (ids < 0 or keys +inf are empty entries).
+void launch_merge_lists(const int32_t* idx, const float* key, int lists, int64_t n, int k, int32_t* idx_out,
+                        float* key_out, cudaStream_t st);
 // Device rows of several sets ([n][d], element type dtype) gathered into one
 // padded array at row offsets `off`, in one launch.
 struct RowSource {

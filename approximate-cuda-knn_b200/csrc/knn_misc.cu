@@ -90,6 +90,53 @@ __global__ void k_finalize_local(const float* __restrict__ key, const uint32_t* 
   }
 }
 
+// Warp per point: the k best distinct ids by (key, id) over `lists` sorted
+// candidate lists [lists][n][k] (id < 0: empty).  A list holds an id once, so
+// an id met again comes from another list and is dropped.
+template <int KPL>
+__global__ void k_merge_lists(const int32_t* __restrict__ idx, const float* __restrict__ key, int lists, int64_t n,
+                              int k, int32_t* __restrict__ idx_out, float* __restrict__ key_out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const float kInf = __int_as_float(0x7F800000);
+  for (int64_t i = w0; i < n; i += nw) {
+    WarpList<KPL> L;
+#pragma unroll
+    for (int r = 0; r < KPL; ++r) {
+      L.key[r] = kInf;
+      L.id[r] = kNoId;
+    }
+    for (int l = 0; l < lists; ++l) {
+      const size_t row = ((size_t)l * n + i) * k;
+      for (int c0 = 0; c0 < k; c0 += 32) {
+        const int e = c0 + lane;
+        const int32_t id = e < k ? idx[row + e] : -1;
+        const float ck = id >= 0 ? key[row + e] : kInf;
+        const uint32_t ci = id >= 0 ? (uint32_t)id : kNoId;
+        float tk;
+        uint32_t ti;
+        warp_list_get(L, k - 1, tk, ti);
+        bool pass = id >= 0 && cand_less(ck, ci, tk, ti);
+        if (!__any_sync(0xFFFFFFFFu, pass)) continue;
+        // every lane takes part in the id check's shuffles
+        const bool dup = warp_list_contains(L, ci, k);
+        pass = pass && !dup;
+        if (!__any_sync(0xFFFFFFFFu, pass)) continue;
+        warp_list_insert(L, pass ? ck : kInf, pass ? ci : kNoId);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < KPL; ++r) {
+      const int e = r * 32 + lane;
+      if (e < k) {
+        idx_out[(size_t)i * k + e] = L.id[r] == kNoId ? -1 : (int32_t)(L.id[r] & kIdMask);
+        key_out[(size_t)i * k + e] = L.key[r];
+      }
+    }
+  }
+}
+
 // seg_of[i] = segment of global position i; block per segment.
 __global__ void k_fill_seg_of(const SegEntry* __restrict__ segs, int32_t* __restrict__ seg_of) {
   const SegEntry e = segs[blockIdx.x];
@@ -147,6 +194,14 @@ void launch_gather_sets(const RowSource* sets, int count, int dtype, int d, floa
   if (dtype == KNN_F16) k_gather_sets<__half><<<grid, threads, 0, st>>>(sets, d, dst, dpad);
   else if (dtype == KNN_BF16) k_gather_sets<__nv_bfloat16><<<grid, threads, 0, st>>>(sets, d, dst, dpad);
   else k_gather_sets<float><<<grid, threads, 0, st>>>(sets, d, dst, dpad);
+}
+void launch_merge_lists(const int32_t* idx, const float* key, int lists, int64_t n, int k, int32_t* idx_out,
+                        float* key_out, cudaStream_t st) {
+  const unsigned grid = blocks_for(n * 32, 256);
+  const int kpl = kpl_for(k);
+  if (kpl == 1) k_merge_lists<1><<<grid, 256, 0, st>>>(idx, key, lists, n, k, idx_out, key_out);
+  else if (kpl == 2) k_merge_lists<2><<<grid, 256, 0, st>>>(idx, key, lists, n, k, idx_out, key_out);
+  else k_merge_lists<4><<<grid, 256, 0, st>>>(idx, key, lists, n, k, idx_out, key_out);
 }
 void launch_fill_seg_of(const SegEntry* segs, int count, int32_t* seg_of, cudaStream_t st) {
   k_fill_seg_of<<<(unsigned)count, 256, 0, st>>>(segs, seg_of);

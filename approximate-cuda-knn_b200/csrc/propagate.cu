@@ -66,7 +66,7 @@ size_t prop_warp_bytes(int k, int dpad) {
 
 template <int METRIC, int KPL>
 __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
-    const float* __restrict__ X, int64_t n, int d, int dpad, int k, int kw, int hbits,
+    const float* __restrict__ X, int64_t n, int64_t r0, int64_t cnt, int d, int dpad, int k, int kw, int hbits,
     size_t warp_bytes, const float* __restrict__ norms, const int32_t* __restrict__ order,
     const float* __restrict__ key_in, const uint32_t* __restrict__ id_in,
     const uint32_t* __restrict__ flags_in, float* __restrict__ key_out,
@@ -86,8 +86,9 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
 
   const int wpb = blockDim.x >> 5;
   const int64_t nwarps = (int64_t)gridDim.x * wpb;
-  for (int64_t w = (int64_t)blockIdx.x * wpb + warp; w < n; w += nwarps) {
-    const int32_t i = order ? order[w] : (int32_t)w;
+  // points (or order positions) r0 .. r0 + cnt - 1
+  for (int64_t w = (int64_t)blockIdx.x * wpb + warp; w < cnt; w += nwarps) {
+    const int32_t i = order ? order[r0 + w] : (int32_t)(r0 + w);
     WarpList<KPL> L;
     uint32_t oid[KPL];
     bool oflag[KPL];
@@ -96,9 +97,13 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
       const int e = r * 32 + lane;
       if (e < k) {
         L.key[r] = key_in[(size_t)i * k + e];
+        // an id outside [0, n) is an empty entry: kept out of the list and
+        // never followed
         const uint32_t u = id_in[(size_t)i * k + e] & kIdMask;
-        L.id[r] = u;
-        oid[r] = u;
+        const bool ok = u < (uint64_t)n;
+        L.key[r] = ok ? L.key[r] : kInf;
+        L.id[r] = ok ? u : kNoId;
+        oid[r] = ok ? u : kNoId;
         oflag[r] = flags_in ? ((flags_in[(size_t)i * kw + r] >> lane) & 1u) : true;
       } else {
         L.key[r] = kInf;
@@ -114,7 +119,7 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
     if (lane == 0) hash_insert(H, hbits, i);
 #pragma unroll
     for (int r = 0; r < KPL; ++r)
-      if (r * 32 + lane < k) hash_insert(H, hbits, (int32_t)oid[r]);
+      if (r * 32 + lane < k && oid[r] != kNoId) hash_insert(H, hbits, (int32_t)oid[r]);
     __syncwarp();
     const float ni = (METRIC == KNN_METRIC_COSINE) ? norms[i] : 0.f;
 
@@ -177,6 +182,7 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
         }
       const uint32_t a = __shfl_sync(0xFFFFFFFFu, av, src);
       const bool af = __shfl_sync(0xFFFFFFFFu, fv, src) != 0;
+      if (a == kNoId) continue;  // warp-uniform
       for (int r0 = 0; r0 < k; r0 += 32) {
         const int e = r0 + lane;
         bool cand = false;
@@ -184,7 +190,7 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
         if (e < k) {
           jj = (int32_t)(id_in[(size_t)a * k + e] & kIdMask);
           const bool jf = flags_in ? ((flags_in[(size_t)a * kw + (r0 >> 5)] >> lane) & 1u) : true;
-          cand = (af || jf) && hash_insert(H, hbits, jj);
+          cand = (af || jf) && (int64_t)jj < n && hash_insert(H, hbits, jj);
         }
         const uint32_t bal = __ballot_sync(0xFFFFFFFFu, cand);
         if (cand) Q[qn + __popc(bal & lt_mask)] = (uint32_t)jj;
@@ -221,13 +227,14 @@ template <int METRIC>
 static void launch_prop_metric(const PropArgs& a, int kpl, int hbits, size_t wb, int wpb,
                                unsigned grid) {
   const int kw = (a.k + 31) / 32;
+  const int64_t r0 = a.r0, cnt = (a.r1 > 0 ? a.r1 : a.n) - a.r0;
   const size_t smem = wb * wpb;
 #define KNN_PROP_LAUNCH(KP)                                                                       \
   do {                                                                                            \
     cudaFuncSetAttribute(k_propagate<METRIC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                          (int)kPropSmemBudget);                                                   \
     k_propagate<METRIC, KP><<<grid, wpb * 32, smem, a.stream>>>(                                  \
-        a.X, a.n, a.d, a.dpad, a.k, kw, hbits, wb, a.norms, a.order, a.key_in, a.id_in,           \
+        a.X, a.n, r0, cnt, a.d, a.dpad, a.k, kw, hbits, wb, a.norms, a.order, a.key_in, a.id_in,  \
         a.flags_in, a.key_out, a.id_out, a.flags_out, a.cand_counter);                            \
   } while (0)
   if (kpl == 1) KNN_PROP_LAUNCH(1);
@@ -249,7 +256,9 @@ int propagate_step(const PropArgs& a, LaunchLog& log) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int per_sm = (int)((220 * 1024) / (wb * wpb));
   if (per_sm < 1) per_sm = 1;
-  const int64_t want = (a.n + wpb - 1) / wpb;
+  const int64_t cnt = (a.r1 > 0 ? a.r1 : a.n) - a.r0;
+  if (cnt <= 0) return KNN_OK;
+  const int64_t want = (cnt + wpb - 1) / wpb;
   const int64_t cap = (int64_t)sms * per_sm;
   const unsigned grid = (unsigned)(want < cap ? want : cap);
   if (a.metric == KNN_METRIC_EUCLIDEAN) launch_prop_metric<KNN_METRIC_EUCLIDEAN>(a, kpl, hbits, wb, wpb, grid);

@@ -22,7 +22,7 @@ namespace knn {
 // x[b] - x[a] of two member points.  Global positions index the perm rows.
 __global__ void k_directions(const float* __restrict__ X, int dpad, int64_t ntot, int level,
                              int trees, const int32_t* __restrict__ perm, float* __restrict__ dirs,
-                             SegView segs, int active) {
+                             SegView segs, int active, int tree_offset, int tree_stride) {
   const int64_t nodes = int64_t(1) << level;
   const int64_t gw = (int64_t)(blockIdx.x * (blockDim.x >> 5)) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
@@ -41,7 +41,7 @@ __global__ void k_directions(const float* __restrict__ X, int dpad, int64_t ntot
     return;
   }
   int64_t p1, p2;
-  pivot_positions(e.seed, t, level, j, cnt, &p1, &p2);
+  pivot_positions(e.seed, tree_offset + t * tree_stride, level, j, cnt, &p1, &p2);
   const int32_t ia = perm[(size_t)t * ntot + lo + p1];
   const int32_t ib = perm[(size_t)t * ntot + lo + p2];
   const float4* xa = reinterpret_cast<const float4*>(X + (size_t)ia * dpad);
@@ -536,7 +536,8 @@ int tree_build(const TreeArgs& a, LaunchLog& log) {
     const int64_t nodes = int64_t(1) << l;
     const int64_t segs = nodes * a.trees * active;
     k_directions<<<(unsigned)((segs + 7) / 8), 256, 0, st>>>(a.X, a.dpad, ntot, l, a.trees, cur, a.dirs,
-                                                             a.segs, active);
+                                                             a.segs, active, a.tree_offset,
+                                                             a.tree_stride > 0 ? a.tree_stride : 1);
     const int per_block = 8 * (32 / G);
     int64_t blocks = (ntot + per_block - 1) / per_block;
     if (blocks > 148LL * 64) blocks = 148LL * 64;

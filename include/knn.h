@@ -79,7 +79,11 @@ typedef struct knn_options {
                                 workload and reuse the fastest from then on           */
   int32_t leaf_tile;         /* FP32 leaf tile 32 or 64 (0: tuned, else 64)              */
   int32_t prop_warps;        /* propagation warps per block 1..8 (0: tuned, else max)   */
-  int32_t reserved[3];
+  int32_t tree_offset;       /* sharded builds: local tree t is the global tree          */
+  int32_t tree_stride;       /*   tree_offset + t * tree_stride (stride 0 means 1)       */
+  int32_t raw_keys;          /* 1: out_dist receives the ranking keys (squared L2 for
+                                EUCLIDEAN) instead of distances                       */
+  int32_t reserved[4];
 } knn_options;
 
 typedef struct knn_stats {
@@ -177,6 +181,32 @@ typedef struct knn_dataset {
 
 int knn_build_batch(knn_context* ctx, const knn_dataset* sets, int32_t count, int32_t k, int32_t trees,
                     int32_t leaf, int32_t props, int32_t metric, const knn_options* opt, knn_stats* stats);
+
+/*
+ * Sharded builds (several GPUs, one process each; no counterpart in the
+ * reference).  Rank r of G builds the global trees r, r+G, ... with
+ * knn_build_ex (tree_offset = r, tree_stride = G, raw_keys = 1, props = 0);
+ * the G lists of every point are gathered and merged by knn_merge_lists (the
+ * k best distinct ids of the union: the lists of all trees at once); each
+ * propagation step then runs on a point range per rank (knn_propagate_range)
+ * and the ranges are gathered.  The graph equals the single-GPU build's.
+ *
+ * knn_merge_lists: idx/key [lists][n][k] sorted lists (id < 0: empty) ->
+ *   idx_out/key_out [n][k]; as_distance = 1 writes distances (sqrt of the key
+ *   for EUCLIDEAN) instead of keys.  Device memory when
+ *   options.points_on_device, else host.
+ * knn_propagate_range: one Jacobi propagation step for the points
+ *   [r0, r1); lists in device memory (idx/key [n][k] with keys, flags
+ *   [n][ceil(k/32)] NEW bits or NULL for all new); rows outside the range of
+ *   the outputs are left as they are.  Points per options.
+ */
+int knn_merge_lists(knn_context* ctx, const int32_t* idx, const float* key, int32_t lists, int64_t n, int32_t k,
+                    int32_t metric, int32_t as_distance, int32_t* idx_out, float* key_out,
+                    const knn_options* opt);
+int knn_propagate_range(knn_context* ctx, const void* points, int64_t n, int32_t d, int32_t k, int32_t metric,
+                        int64_t r0, int64_t r1, const int32_t* idx_in, const float* key_in,
+                        const uint32_t* flags_in, int32_t* idx_out, float* key_out, uint32_t* flags_out,
+                        const knn_options* opt);
 
 /*
  * Stage entry points (host memory in and out), for stage-by-stage checks.

@@ -283,6 +283,17 @@ int oracle_build_trees(const float* X, int64_t n, int32_t d, int32_t trees, int3
 }
 
 // Initial k-NN from given trees. out_key holds keys (squared L2 / L1 / 1-cos).
+// Trees with global indices tree_offset + t * tree_stride (a rank's share of a
+// sharded build); oracle_build_trees is offset 0, stride 1.
+int oracle_build_trees_ex(const float* X, int64_t n, int32_t d, int32_t trees, int32_t leaf, uint64_t seed,
+                          int32_t tree_offset, int32_t tree_stride, int32_t* perm, int32_t nthreads) {
+  if (!X || n < 1 || d < 1 || trees < 1 || leaf < 1 || !perm || tree_offset < 0 || tree_stride < 1) return -1;
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  Data D{X, n, d, kEuclidean, {}};
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int t = 0; t < trees; ++t) build_tree(D, tree_offset + t * tree_stride, leaf, seed, perm + (size_t)t * n);
+  return 0;
+}
 int oracle_leaf_stage(const float* X, int64_t n, int32_t d, int32_t k, int32_t trees,
                       int32_t leaf, int32_t metric, const int32_t* perm, int32_t* out_idx,
                       float* out_key, int32_t nthreads) {

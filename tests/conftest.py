@@ -44,6 +44,7 @@ class Oracle:
             "oracle_project": (ctypes.c_float, [P, P, I32]),
             "oracle_pair_key": (ctypes.c_float, [P, P, I32, I32]),
             "oracle_build_trees": (ctypes.c_int, [P, I64, I32, I32, I32, U64, P, I32]),
+            "oracle_build_trees_ex": (ctypes.c_int, [P, I64, I32, I32, I32, U64, I32, I32, P, I32]),
             "oracle_leaf_stage": (ctypes.c_int, [P, I64, I32, I32, I32, I32, I32, P, P, P, I32]),
             "oracle_propagate": (ctypes.c_int, [P, I64, I32, I32, I32, P, P, P, P, I32]),
             "oracle_finalize": (None, [I64, I32, P, P]),
@@ -69,6 +70,14 @@ class Oracle:
         perm = np.empty((trees, n), dtype=np.int32)
         assert self.lib.oracle_build_trees(x.ctypes.data, n, d, trees, leaf, seed,
                                            perm.ctypes.data, threads) == 0
+        return perm
+
+    def build_trees_ex(self, points, trees, leaf, seed, tree_offset, tree_stride, threads=0):
+        x = self._x(points)
+        n, d = x.shape
+        perm = np.empty((trees, n), dtype=np.int32)
+        assert self.lib.oracle_build_trees_ex(x.ctypes.data, n, d, trees, leaf, seed, tree_offset,
+                                              tree_stride, perm.ctypes.data, threads) == 0
         return perm
 
     def leaf_stage(self, points, k, perm, leaf, metric=0, threads=0):
@@ -134,6 +143,13 @@ class Oracle:
         x = self._x(x)
         v = self._x(v)
         return self.lib.oracle_project(x.ctypes.data, v.ctypes.data, x.shape[0])
+
+    def finalize(self, key, metric=0):
+        """Keys -> distances (sqrt for EUCLIDEAN), float32."""
+        k = np.ascontiguousarray(key, dtype=np.float32)
+        out = np.empty_like(k)
+        self.lib.oracle_finalize(k.size, metric, k.ctypes.data, out.ctypes.data)
+        return out
 
     def mlp_forward(self, params, rows):
         """FP64 f(rows) of the learned split network: [m, 64]."""
