@@ -371,8 +371,15 @@ def run_ours(args, w):
     dom = max(cand, key=lambda kname: cand[kname][0])
     dms, dbytes, dlaunch = cand[dom]
     achieved = dbytes / (dms / 1e3) / 1e9
+    # DRAM bytes (read + write) per k_leaf_tc launch measured by ncu on 500,000
+    # points of this workload and configuration (356 MB), scaled by n
+    traffic = None
+    if dom == "leaf_tc" and (d, k, T, head["leaf"]) == (128, 16, 8, 2048):
+        traffic = 356e6 * n / 500_000
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_leaf_tc "
+                                  "launch at 500,000 points, scaled by n" if traffic else None,
                 "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": dbytes / dlaunch,
                 "mean_launch_ms": dms / dlaunch}
