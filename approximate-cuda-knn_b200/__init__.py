@@ -73,7 +73,8 @@ class KnnOptions(ctypes.Structure):
         ("tree_offset", ctypes.c_int32),
         ("tree_stride", ctypes.c_int32),
         ("raw_keys", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("split_rule", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
     ]
 
 
@@ -207,7 +208,8 @@ def default_options(**kw) -> KnnOptions:
 def knn_build(points, k: int, trees: int, leaf: int, props: int, metric: int = 0,
               seed: int = 0, precision: int = PREC_FP32, learned: bool = False,
               stats: bool = False, context=None, mlp_sample: int = 0, mlp_steps: int = 0,
-              autotune: bool = False, leaf_tile: int = 0, prop_warps: int = 0):
+              autotune: bool = False, leaf_tile: int = 0, prop_warps: int = 0,
+              split_rule: int = 0):
     """k-NN graph of ``points`` ([n, d] float32/float16, host memory).
 
     ``learned`` builds the trees on the learned split network's embedding
@@ -222,7 +224,7 @@ def knn_build(points, k: int, trees: int, leaf: int, props: int, metric: int = 0
     opt = default_options(dtype=F16 if x.dtype == np.float16 else F32, precision=precision,
                           learned_splits=int(bool(learned)), mlp_sample=mlp_sample,
                           mlp_steps=mlp_steps, autotune=int(bool(autotune)), leaf_tile=leaf_tile,
-                          prop_warps=prop_warps)
+                          prop_warps=prop_warps, split_rule=split_rule)
     st = KnnStats()
     st.struct_size = ctypes.sizeof(KnnStats)
     rc = lib.knn_build_ex(context, _ptr(x), n, d, k, trees, leaf, props, metric, seed,

@@ -279,6 +279,40 @@ int run_trees(knn_context* C, const float* X, int64_t n, int d, int dpad, int tr
                         tree_offset, tree_stride);
 }
 
+// Reference-rule trees (tree_faithful.cu); T->depth = levels built.
+int run_faithful_trees(knn_context* C, const float* X, int64_t n, int d, int dpad, int trees, int leaf,
+                       uint64_t seed, int tree_offset, int tree_stride, cudaStream_t st, Trees* T,
+                       knn::FaithfulTrees* FT, knn::LaunchLog& log) {
+  knn::FaithfulArgs a{};
+  a.X = X;
+  a.n = n;
+  a.d = d;
+  a.dpad = dpad;
+  a.trees = trees;
+  a.leaf = leaf;
+  a.seed = seed;
+  a.tree_offset = tree_offset;
+  a.tree_stride = tree_stride;
+  // splitting nodes per level: at most trees * n / (leaf + 1); chunk counts
+  // sum to at most that plus trees * n / 1024
+  a.node_cap = (size_t)trees * (size_t)(n / (leaf + 1) + 1);
+  a.count_cap = a.node_cap + (size_t)trees * (size_t)(n / 1024 + 1);
+  int rc = C->get("perm", (size_t)trees * n, &a.perm);
+  if (!rc) rc = C->get("perm_alt", (size_t)trees * n, &a.perm_alt);
+  if (!rc) rc = C->get("f_side", (size_t)trees * n, &a.side);
+  if (!rc) rc = C->get("f_nodes", a.node_cap, &a.dnodes);
+  if (!rc) rc = C->get("f_lcount", a.count_cap, &a.lcount);
+  if (!rc) rc = C->get("f_nleft", a.node_cap, &a.nleft);
+  if (rc) return rc;
+  a.stream = st;
+  rc = knn::faithful_tree_build(a, FT, log);
+  if (rc == KNN_ERR_UNSUPPORTED) return fail(rc, "reference-rule tree deeper than the level limit");
+  if (rc) return fail_cuda(cudaGetLastError(), "reference-rule tree build");
+  T->perm = a.perm;
+  T->depth = FT->levels;
+  return KNN_OK;
+}
+
 struct Lists {
   float* key[2];
   uint32_t* id[2];
@@ -302,6 +336,10 @@ int get_lists(knn_context* C, int64_t n, int k, Lists* L) {
 struct Layout {
   knn::SegView segs;
   int64_t leaves = 1, maxleaf = 1;
+  // reference-rule trees: explicit leaf table (device) and per-tree offsets / counts (host)
+  const int64_t* ftable = nullptr;
+  const int64_t* foff = nullptr;
+  const int64_t* fcount = nullptr;
 };
 
 Layout single_layout(int64_t n, int depth) {
@@ -334,6 +372,9 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
   a.rid = L->id[L->cur];
   a.pair_counter = counter;
   a.tile = tile;
+  a.ftable = lay.ftable;
+  a.foff = lay.foff;
+  a.fcount = lay.fcount;
   a.stream = st;
   int rc = knn::leaf_stage(a, log);
   if (rc) return fail_cuda(cudaGetLastError(), "leaf stage launch");
@@ -360,6 +401,9 @@ int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, in
   a.segs = lay.segs;
   a.leaves = lay.leaves;
   a.maxleaf = lay.maxleaf;
+  a.ftable = lay.ftable;
+  a.foff = lay.foff;
+  a.fcount = lay.fcount;
   a.metric = metric;
   a.perm = perm;
   a.norms = norms;
@@ -639,6 +683,9 @@ int resolve_options(const knn_options* opt, knn_options* o) {
   if (o->prop_warps < 0 || o->prop_warps > 8) return fail(KNN_ERR_ARGS, "prop_warps must be in 0..8");
   if (o->tree_offset < 0 || o->tree_stride < 0) return fail(KNN_ERR_ARGS, "negative tree offset or stride");
   if (o->raw_keys < 0 || o->raw_keys > 1) return fail(KNN_ERR_ARGS, "raw_keys must be 0 or 1");
+  if (o->split_rule < 0 || o->split_rule > 1) return fail(KNN_ERR_ARGS, "unknown split rule");
+  if (o->split_rule == KNN_SPLIT_REFERENCE && o->learned_splits)
+    return fail(KNN_ERR_UNSUPPORTED, "reference-rule splits and learned splits do not combine");
   return KNN_OK;
 }
 
@@ -679,7 +726,20 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
   if (timed) KNN_CK(cudaEventRecord(C->ev[1], st));
 
   Trees T;
-  if (o.learned_splits) {
+  knn::FaithfulTrees FT;
+  std::vector<int64_t> ftab_h, foff_h, fcount_h;
+  const int64_t* ftab_d = nullptr;
+  if (o.split_rule == KNN_SPLIT_REFERENCE) {
+    rc = run_faithful_trees(C, P.X, n, d, P.dpad, trees, leaf, seed, o.tree_offset, o.tree_stride, st, &T, &FT,
+                            log);
+    if (rc) return rc;
+    knn::faithful_leaf_table(FT, trees, k, &ftab_h, &foff_h, &fcount_h);
+    int64_t* dt = nullptr;
+    rc = C->get("ftable", ftab_h.size(), &dt);
+    if (rc) return rc;
+    KNN_CK(cudaMemcpyAsync(dt, ftab_h.data(), sizeof(int64_t) * ftab_h.size(), cudaMemcpyHostToDevice, st));
+    ftab_d = dt;
+  } else if (o.learned_splits) {
     // Trees on the learned 64-dim embedding; leaf and propagation on X.
     Learned Lr;
     rc = learn_network(C, P.X, n, d, P.dpad, k, metric, seed, o, st, &Lr, log);
@@ -703,7 +763,13 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
   KNN_CK(cudaMemsetAsync(err_flag, 0, sizeof(int), st));
   const bool tensor_leaf = o.precision == KNN_PREC_BF16_RERANK && metric != KNN_METRIC_TAXICAB &&
                            d <= 256 && k <= 32;
-  const Layout lay = single_layout(n, T.depth);
+  Layout lay = single_layout(n, T.depth);
+  if (ftab_d) {
+    lay.ftable = ftab_d;
+    lay.foff = foff_h.data();
+    lay.fcount = fcount_h.data();
+    lay.maxleaf = leaf;
+  }
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   KNN_CK(cudaStreamIsCapturing(st, &cs));
   Shapes sh;
@@ -1166,6 +1232,7 @@ int knn_build_batch(knn_context* ctx, const knn_dataset* sets, int32_t count, in
   if (props < 0 || props > KNN_MAX_PROPS) return fail(KNN_ERR_ARGS, "props out of range");
   if (o.ld != 0) return fail(KNN_ERR_ARGS, "batches take contiguous rows (options.ld must be 0)");
   if (o.learned_splits) return fail(KNN_ERR_UNSUPPORTED, "learned splits are not available for batches");
+  if (o.split_rule != 0) return fail(KNN_ERR_UNSUPPORTED, "reference-rule splits are not available for batches");
   if (stats && stats->struct_size != (int32_t)sizeof(knn_stats))
     return fail(KNN_ERR_ARGS, "knn_stats.struct_size mismatch");
   std::map<int, int64_t> per_d;

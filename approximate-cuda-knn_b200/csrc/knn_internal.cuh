@@ -64,6 +64,37 @@ inline int tree_depth(int64_t n, int leaf) {
   return l;
 }
 
+// ------------------------------------------------------------------ scan --
+// Block-wide exclusive scan of one value per thread; returns the exclusive
+// prefix and writes the block total to *total.
+__device__ __forceinline__ int64_t block_excl_scan(int64_t v, int64_t* warp_sums, int64_t* total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int64_t incl = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    int64_t o = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+    if (lane >= off) incl += o;
+  }
+  if (lane == 31) warp_sums[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    int64_t s = lane < nw ? warp_sums[lane] : 0;
+    int64_t si = s;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      int64_t o = __shfl_up_sync(0xFFFFFFFFu, si, off);
+      if (lane >= off) si += o;
+    }
+    if (lane < nw) warp_sums[lane] = si - s;
+    if (lane == 31) warp_sums[32] = si;
+  }
+  __syncthreads();
+  const int64_t r = warp_sums[w] + incl - v;
+  *total = warp_sums[32];
+  __syncthreads();
+  return r;
+}
+
 // ------------------------------------------------------------- segments --
 // A batch of independent point sets concatenated in one array.  Segment a
 // holds the global positions / ids [off, off + n) and its trees have `depth`

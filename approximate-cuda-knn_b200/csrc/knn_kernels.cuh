@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "knn_internal.cuh"
 
 namespace knn {
@@ -52,7 +54,42 @@ int tree_build(const TreeArgs& a, LaunchLog& log);
 // (segments still splitting at l) * trees * 2^l.
 size_t tree_dir_nodes(const SegEntry* hsegs, int nseg, int trees);
 
+// Reference-rule trees (tree_faithful.cu): node records, split per level on
+// an explicit list of splitting nodes.
+constexpr int kFaithfulMaxLevels = 4096;
+struct FNode {
+  int64_t lo, hi, id, parent;
+  int32_t tree, p1, p2, cbase;  // cbase: the node's first slot in the chunk counts
+};
+struct FaithfulArgs {
+  const float* X;
+  int64_t n;
+  int d, dpad, trees, leaf;
+  uint64_t seed;
+  int tree_offset, tree_stride;  // local tree t is global tree tree_offset + t * tree_stride
+  int32_t* perm;       // [trees][n] out: leaf order
+  int32_t* perm_alt;   // [trees][n] scratch
+  uint8_t* side;       // [trees][n] scratch
+  FNode* dnodes;       // [node_cap] scratch
+  size_t node_cap;
+  int32_t* lcount;     // [count_cap] scratch
+  size_t count_cap;
+  int64_t* nleft;      // [node_cap] scratch
+  cudaStream_t stream;
+};
+struct FaithfulTrees {
+  std::vector<FNode> nodes;   // every node, roots first; id = index
+  std::vector<uint8_t> split; // 1: the node was split
+  int levels = 0;
+};
+int faithful_tree_build(const FaithfulArgs& a, FaithfulTrees* out, LaunchLog& log);
+// (lo, hi, blo, bhi) per leaf, per tree in position order; offset / count in leaves.
+void faithful_leaf_table(const FaithfulTrees& T, int trees, int k, std::vector<int64_t>* table,
+                         std::vector<int64_t>* offset, std::vector<int64_t>* count);
+
 // n = all points (a batch: of every segment); leaves = leaf blocks per tree.
+// With ftable the leaves of tree t are the fcount[t] entries (lo, hi, blo,
+// bhi) from entry foff[t] of ftable (device; foff and fcount on the host).
 struct LeafArgs {
   const float* X;
   int64_t n;
@@ -66,6 +103,9 @@ struct LeafArgs {
   unsigned long long* pair_counter;  // optional
   int tile;              // 32 or 64 (0: 64): query x candidate tile, results identical
   int first_tree;        // trees [first_tree, first_tree + trees) of perm
+  const int64_t* ftable;
+  const int64_t* foff;
+  const int64_t* fcount;
   cudaStream_t stream;
 };
 int leaf_stage(const LeafArgs& a, LaunchLog& log);
@@ -86,6 +126,9 @@ struct UmmaLeafArgs {
   float* rkey;           // [n][k] out: exact keys, sorted
   uint32_t* rid;
   int* err;              // set when a bounded wait expires
+  const int64_t* ftable; // as in LeafArgs
+  const int64_t* foff;
+  const int64_t* fcount;
   cudaStream_t stream;
 };
 int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log);

@@ -40,7 +40,7 @@ __device__ __forceinline__ void load_r(const float* p, float (&v)[R]) {
 // union under (key, id), so all TILE variants give identical lists.
 template <int METRIC, int KPL, int TILE>
 __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d, int dpad,
-                                              SegView segs, int k,
+                                              SegView segs, const int64_t* __restrict__ ftab, int k,
                                               const int32_t* __restrict__ perm,
                                               const float* __restrict__ norms,
                                               float* __restrict__ rkey, uint32_t* __restrict__ rid,
@@ -55,9 +55,18 @@ __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d
   __shared__ int32_t qid[kTile], cid[kTile];
   __shared__ float qnorm[kTile], cnorm[kTile];
 
-  int64_t j, lo, hi, blo, bhi;
-  const SegEntry seg = segs.leaf(blockIdx.x, &j);
-  leaf_block(seg, j, k, &lo, &hi, &blo, &bhi);
+  int64_t lo, hi, blo, bhi;
+  if (ftab) {  // explicit leaf table (reference-rule trees)
+    const int64_t* e = ftab + 4 * (int64_t)blockIdx.x;
+    lo = e[0];
+    hi = e[1];
+    blo = e[2];
+    bhi = e[3];
+  } else {
+    int64_t j;
+    const SegEntry seg = segs.leaf(blockIdx.x, &j);
+    leaf_block(seg, j, k, &lo, &hi, &blo, &bhi);
+  }
   const int nq = (int)(hi - lo);
   const int nb = (int)(bhi - blo);
 
@@ -189,21 +198,24 @@ __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d
 }
 
 template <int METRIC, int TILE>
-static void launch_leaf_tile(const LeafArgs& a, const int32_t* perm, int kpl) {
-  dim3 grid((unsigned)a.leaves);
+static void launch_leaf_tile(const LeafArgs& a, const int32_t* perm, const int64_t* ftab, int64_t leaves, int kpl) {
+  if (leaves <= 0) return;
+  dim3 grid((unsigned)leaves);
   if (kpl == 1)
-    k_leaf<METRIC, 1, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 1, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
   else if (kpl == 2)
-    k_leaf<METRIC, 2, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 2, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
   else
-    k_leaf<METRIC, 4, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 4, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
 }
 
 template <int METRIC>
 static void launch_leaf_metric(const LeafArgs& a, int t, int kpl) {
   const int32_t* perm = a.perm + (size_t)t * a.n;
-  if (a.tile == 32) launch_leaf_tile<METRIC, 32>(a, perm, kpl);
-  else launch_leaf_tile<METRIC, 64>(a, perm, kpl);
+  const int64_t* ftab = a.ftable ? a.ftable + 4 * a.foff[t] : nullptr;
+  const int64_t leaves = a.ftable ? a.fcount[t] : a.leaves;
+  if (a.tile == 32) launch_leaf_tile<METRIC, 32>(a, perm, ftab, leaves, kpl);
+  else launch_leaf_tile<METRIC, 64>(a, perm, ftab, leaves, kpl);
 }
 
 // One launch per tree: a point sits in one leaf per tree, so the leaves of a

@@ -173,7 +173,8 @@ __device__ __forceinline__ void stage_operand(unsigned char* op, const __nv_bflo
 // chunk with many survivors is sorted and merged into the list in one go.
 template <int METRIC, bool FIRST>
 __global__ void __launch_bounds__(kUThreads, 2)
-    k_leaf_tc(const __nv_bfloat16* __restrict__ Xb, int Kp, SegView segs, int k, int kq,
+    k_leaf_tc(const __nv_bfloat16* __restrict__ Xb, int Kp, SegView segs, const int64_t* __restrict__ ftab, int k,
+              int kq,
               int qtiles, const int32_t* __restrict__ perm, const float* __restrict__ norms2,
               float* __restrict__ akey, uint32_t* __restrict__ aid, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -198,9 +199,18 @@ __global__ void __launch_bounds__(kUThreads, 2)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t leaf = blockIdx.x / qtiles;
   const int qt = (int)(blockIdx.x - leaf * qtiles);
-  int64_t j, lo, hi, blo, bhi;
-  const SegEntry seg = segs.leaf(leaf, &j);
-  leaf_block(seg, j, k, &lo, &hi, &blo, &bhi);
+  int64_t lo, hi, blo, bhi;
+  if (ftab) {  // explicit leaf table (reference-rule trees)
+    const int64_t* e = ftab + 4 * leaf;
+    lo = e[0];
+    hi = e[1];
+    blo = e[2];
+    bhi = e[3];
+  } else {
+    int64_t j;
+    const SegEntry seg = segs.leaf(leaf, &j);
+    leaf_block(seg, j, k, &lo, &hi, &blo, &bhi);
+  }
   const int nq = (int)(hi - lo);
   const int q0 = qt * kBM;
   if (q0 >= nq) return;  // whole block, before any barrier or allocation
@@ -484,11 +494,14 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
   const int qtiles = (int)((a.maxleaf + kBM - 1) / kBM);
   for (int t = 0; t < a.trees; ++t) {
     const int32_t* perm = a.perm + (size_t)t * a.n;
-    const unsigned grid = (unsigned)(leaves * qtiles);
+    const int64_t* ftab = a.ftable ? a.ftable + 4 * a.foff[t] : nullptr;
+    const int64_t tleaves = a.ftable ? a.fcount[t] : leaves;
+    if (tleaves <= 0) continue;
+    const unsigned grid = (unsigned)(tleaves * qtiles);
 #define KNN_TC_LAUNCH(M, F)                                                                               \
   do {                                                                                                    \
     cudaFuncSetAttribute(k_leaf_tc<M, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);       \
-    k_leaf_tc<M, F><<<grid, kUThreads, smem, st>>>(Xb, Kp, a.segs, a.k, a.kq, qtiles, perm, a.norms2, a.akey, \
+    k_leaf_tc<M, F><<<grid, kUThreads, smem, st>>>(Xb, Kp, a.segs, ftab, a.k, a.kq, qtiles, perm, a.norms2, a.akey, \
                                                    a.aid, a.err);                                        \
   } while (0)
     if (a.metric == KNN_METRIC_EUCLIDEAN) {

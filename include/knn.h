@@ -58,6 +58,16 @@ extern "C" {
                                   |x|^2+|y|^2-2x.y form, each point's best 2k
                                   re-ranked with exact FP32 keys                 */
 
+/* Tree split rules.  MEDIAN: each node splits at the median of its points'
+ * projections (balanced trees of static shape).  REFERENCE: the split of
+ * buildUpTheTrees (euclideandistancematrixgpu.cu:2138-2181, :2291-2365): the
+ * sign of x . (x[p2] - x[p1]) through the origin, positions p1, p2 drawn once
+ * per level and shared by its nodes, p1 forced left and p2 right, nodes
+ * split until they hold at most `leaf` points -- for like-for-like recall
+ * comparisons with the reference (single builds only). */
+#define KNN_SPLIT_MEDIAN 0
+#define KNN_SPLIT_REFERENCE 1
+
 #define KNN_MAX_K 128
 #define KNN_MAX_PROPS 64
 
@@ -83,7 +93,8 @@ typedef struct knn_options {
   int32_t tree_stride;       /*   tree_offset + t * tree_stride (stride 0 means 1)       */
   int32_t raw_keys;          /* 1: out_dist receives the ranking keys (squared L2 for
                                 EUCLIDEAN) instead of distances                       */
-  int32_t reserved[4];
+  int32_t split_rule;        /* KNN_SPLIT_MEDIAN (default) or KNN_SPLIT_REFERENCE     */
+  int32_t reserved[3];
 } knn_options;
 
 typedef struct knn_stats {

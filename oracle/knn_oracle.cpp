@@ -256,6 +256,76 @@ void merge_topk(std::vector<Cand>& list, std::vector<Cand>& add, int k) {
   }
 }
 
+// ------------------------------------------------ reference-rule trees --
+// The split of buildUpTheTrees (euclideandistancematrixgpu.cu:2138-2181,
+// :2291-2365, :2478-2487) made deterministic: per level two draws shared by
+// every node (p1 = R1 % c, p2 = R2 % c, p2 = (p1+1) % c if equal), side by
+// the sign of the sequential fused sum x . (x[p2] - x[p1]) (left when < 0),
+// p1 forced left and p2 right, stable partition, nodes of at most `leaf`
+// points stop.
+struct FNodeO {
+  int64_t lo, hi, parent;
+  bool split;
+};
+
+uint32_t faithful_draw(uint64_t seed, int tree, int level, int which) {
+  const uint64_t h = splitmix64(seed ^ splitmix64(0xF417F01ull + (uint64_t)tree * 0x9E3779B97F4A7C15ull +
+                                                  (uint64_t)level * 0xD1B54A32D192ED03ull + (uint64_t)which));
+  return (uint32_t)(h & 0x7FFFFFFFu);
+}
+
+void build_tree_faithful(const Data& D, int tree, int leaf, uint64_t seed, int32_t* perm,
+                         std::vector<FNodeO>& nodes) {
+  const int64_t n = D.n;
+  const int d = D.d;
+  for (int64_t i = 0; i < n; ++i) perm[i] = (int32_t)i;
+  nodes.clear();
+  nodes.push_back({0, n, -1, false});
+  std::vector<int64_t> active;
+  if (n > leaf) active.push_back(0);
+  std::vector<int32_t> tmp;
+  std::vector<float> diff(d);
+  int level = 0;
+  while (!active.empty()) {
+    std::vector<int64_t> next;
+    for (int64_t a : active) {
+      const int64_t lo = nodes[a].lo, hi = nodes[a].hi, cnt = hi - lo;
+      int64_t p1 = 0, p2 = 0;
+      if (cnt > 1) {
+        p1 = faithful_draw(seed, tree, level, 1) % (uint64_t)cnt;
+        p2 = faithful_draw(seed, tree, level, 2) % (uint64_t)cnt;
+        if (p1 == p2) p2 = (p1 + 1) % cnt;
+      }
+      const float* xa = D.row(perm[lo + p1]);
+      const float* xb = D.row(perm[lo + p2]);
+      for (int c = 0; c < d; ++c) diff[c] = xb[c] - xa[c];
+      tmp.clear();
+      std::vector<int32_t> right;
+      for (int64_t p = lo; p < hi; ++p) {
+        const float* x = D.row(perm[p]);
+        float acc = 0.0f;
+        for (int c = 0; c < d; ++c) acc = std::fmaf(x[c], diff[c], acc);
+        bool left = acc < 0.0f;
+        if (p == lo + p1) left = true;
+        if (p == lo + p2) left = false;
+        if (left) tmp.push_back(perm[p]);
+        else right.push_back(perm[p]);
+      }
+      const int64_t nl = (int64_t)tmp.size();
+      for (int32_t v : right) tmp.push_back(v);
+      std::memcpy(perm + lo, tmp.data(), sizeof(int32_t) * (size_t)cnt);
+      nodes[a].split = true;
+      const int64_t L = (int64_t)nodes.size();
+      nodes.push_back({lo, lo + nl, a, false});
+      nodes.push_back({lo + nl, hi, a, false});
+      if (nl > leaf) next.push_back(L);
+      if (hi - lo - nl > leaf) next.push_back(L + 1);
+    }
+    active.swap(next);
+    ++level;
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -415,6 +485,65 @@ int oracle_knn_build(const float* X, int64_t n, int32_t d, int32_t k, int32_t tr
 
 // FP64 exact k-NN of the given query ids against all n points (self excluded),
 // ties by index.  dist: sqrt(sum sq) / sum |.| / 1 - cos, in double.
+// The whole build with reference-rule trees: leaves are the nodes that were
+// not split; a leaf's block is its smallest ancestor-or-self with at least
+// k+1 points.
+int oracle_knn_build_faithful(const float* X, int64_t n, int32_t d, int32_t k, int32_t trees, int32_t leaf,
+                              int32_t props, int32_t metric, uint64_t seed, int32_t* out_idx, float* out_dist,
+                              int32_t nthreads) {
+  if (!X || !out_idx || !out_dist || n < 1 || d < 1 || k < 1 || trees < 1 || leaf < 1 || props < 0) return -1;
+  if (metric < 0 || metric > 2) return -1;
+  if (n <= k) return -2;
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  Data D{X, n, d, metric, {}};
+  prepare(D);
+  std::vector<int32_t> perm((size_t)trees * n);
+  std::vector<std::vector<FNodeO>> nodes(trees);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int t = 0; t < trees; ++t) build_tree_faithful(D, t, leaf, seed, perm.data() + (size_t)t * n, nodes[t]);
+  std::vector<std::vector<Cand>> lists(n);
+  for (int t = 0; t < trees; ++t) {
+    const int32_t* pm = perm.data() + (size_t)t * n;
+    std::vector<int64_t> leaves;
+    for (int64_t j = 0; j < (int64_t)nodes[t].size(); ++j)
+      if (!nodes[t][j].split) leaves.push_back(j);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t li = 0; li < (int64_t)leaves.size(); ++li) {
+      const FNodeO& lf = nodes[t][leaves[li]];
+      int64_t b = leaves[li];
+      while (nodes[t][b].hi - nodes[t][b].lo < k + 1 && nodes[t][b].parent >= 0) b = nodes[t][b].parent;
+      const int64_t blo = nodes[t][b].lo, bhi = nodes[t][b].hi;
+      std::vector<Cand> add;
+      for (int64_t q = lf.lo; q < lf.hi; ++q) {
+        const int32_t i = pm[q];
+        add.clear();
+        for (int64_t c = blo; c < bhi; ++c) {
+          const int32_t jj = pm[c];
+          if (jj == i) continue;
+          add.push_back({D.key(i, jj), jj});
+        }
+        merge_topk(lists[i], add, k);
+      }
+    }
+  }
+  std::vector<int32_t> ia((size_t)n * k), ib((size_t)n * k);
+  std::vector<float> ka((size_t)n * k), kb((size_t)n * k);
+  for (int64_t i = 0; i < n; ++i)
+    for (int s = 0; s < k; ++s) {
+      ia[i * k + s] = lists[i][s].id;
+      ka[i * k + s] = lists[i][s].key;
+    }
+  for (int p = 0; p < props; ++p) {
+    int rc = oracle_propagate(X, n, d, k, metric, ia.data(), ka.data(), ib.data(), kb.data(), nthreads);
+    if (rc) return rc;
+    ia.swap(ib);
+    ka.swap(kb);
+  }
+  std::memcpy(out_idx, ia.data(), ia.size() * sizeof(int32_t));
+  oracle_finalize((int64_t)ka.size(), metric, ka.data(), out_dist);
+  return 0;
+}
+
 int oracle_exact_knn(const float* X, int64_t n, int32_t d, int32_t k, int32_t metric,
                      const int64_t* queries, int64_t nq, int32_t* out_idx, double* out_dist,
                      int32_t nthreads) {

@@ -45,6 +45,7 @@ class Oracle:
             "oracle_pair_key": (ctypes.c_float, [P, P, I32, I32]),
             "oracle_build_trees": (ctypes.c_int, [P, I64, I32, I32, I32, U64, P, I32]),
             "oracle_build_trees_ex": (ctypes.c_int, [P, I64, I32, I32, I32, U64, I32, I32, P, I32]),
+            "oracle_knn_build_faithful": (ctypes.c_int, [P, I64, I32, I32, I32, I32, I32, I32, U64, P, P, I32]),
             "oracle_leaf_stage": (ctypes.c_int, [P, I64, I32, I32, I32, I32, I32, P, P, P, I32]),
             "oracle_propagate": (ctypes.c_int, [P, I64, I32, I32, I32, P, P, P, P, I32]),
             "oracle_finalize": (None, [I64, I32, P, P]),
@@ -111,6 +112,18 @@ class Oracle:
                                        idx.ctypes.data, dist.ctypes.data, threads)
         if rc:
             raise ValueError(f"oracle_knn_build rc={rc}")
+        return idx, dist
+
+    def knn_build_faithful(self, points, k, trees, leaf, props, metric=0, seed=0, threads=0):
+        """The build with reference-rule trees (sign split through the origin)."""
+        x = self._x(points)
+        n, d = x.shape
+        idx = np.empty((n, k), dtype=np.int32)
+        dist = np.empty((n, k), dtype=np.float32)
+        rc = self.lib.oracle_knn_build_faithful(x.ctypes.data, n, d, k, trees, leaf, props, metric, seed,
+                                                idx.ctypes.data, dist.ctypes.data, threads)
+        if rc:
+            raise ValueError(f"oracle_knn_build_faithful rc={rc}")
         return idx, dist
 
     def exact(self, points, k, queries=None, metric=0, threads=0):

@@ -70,8 +70,15 @@ def test_reference_recall_small_gaussians(tmp_path, oracle, capsys):
     ex, _ = oracle.exact(x, 10)
     ref_ids, ref_ms = run_reference(tmp_path, x, 10, trees=10, leaf=32, props=3)
     ora_ids, _ = oracle.knn_build(x, 10, 10, 32, 3, 0)
+    # like for like: the reference normalises its input (normalizeDataStep1/2)
+    # and splits through the origin; the same rule here on the same data
+    xn = acknn.normalize_reference(x)
+    exn, _ = oracle.exact(xn, 10)
+    fai_ids, _ = acknn.knn_build(xn, 10, 10, 32, 3, 0, split_rule=1)
     r_ref, r_ora = recall_at_k(ref_ids, ex), recall_at_k(ora_ids, ex)
+    r_fai = recall_at_k(fai_ids, exn)
     with capsys.disabled():
         print(f"\nsmall_gaussians k=10 T=10 leaf=32 P=3: reference recall {r_ref:.4f} "
-              f"({ref_ms} ms on the GPU), restatement recall {r_ora:.4f}")
-    assert r_ref > 0.3 and r_ora > 0.9
+              f"({ref_ms} ms on the GPU), median-split restatement {r_ora:.4f}, "
+              f"reference-rule splits {r_fai:.4f}")
+    assert r_ref > 0.3 and r_ora > 0.9 and r_fai > 0.3
