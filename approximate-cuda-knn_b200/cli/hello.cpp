@@ -139,6 +139,43 @@ bool save_result(const std::string& out, const std::vector<int32_t>& idx, const 
   return true;
 }
 
+// Knobs the reference does not have come from the environment so that the
+// positional command line stays the reference's:
+//   ACKNN_PRECISION  fp32 (default) | bf16   leaf blocks in FP32 or BF16 tiles + FP32 re-rank
+//   ACKNN_SPLITS     median (default) | reference | learned
+//   ACKNN_SEED       unsigned integer, default 0
+// An unknown value is reported and fails the initialisation (exit code 8).
+bool env_knobs(knn_options& opt, uint64_t& seed) {
+  if (const char* v = std::getenv("ACKNN_PRECISION")) {
+    const std::string s = v;
+    if (s == "fp32") opt.precision = KNN_PREC_FP32;
+    else if (s == "bf16") opt.precision = KNN_PREC_BF16_RERANK;
+    else {
+      std::cout << "ACKNN_PRECISION must be fp32 or bf16\n";
+      return false;
+    }
+  }
+  if (const char* v = std::getenv("ACKNN_SPLITS")) {
+    const std::string s = v;
+    if (s == "median") opt.split_rule = KNN_SPLIT_MEDIAN;
+    else if (s == "reference") opt.split_rule = KNN_SPLIT_REFERENCE;
+    else if (s == "learned") opt.learned_splits = 1;
+    else {
+      std::cout << "ACKNN_SPLITS must be median, reference or learned\n";
+      return false;
+    }
+  }
+  if (const char* v = std::getenv("ACKNN_SEED")) {
+    char* end = nullptr;
+    seed = std::strtoull(v, &end, 10);
+    if (*v == '\0' || *v == '-' || *end != '\0') {
+      std::cout << "ACKNN_SEED must be an unsigned integer\n";
+      return false;
+    }
+  }
+  return true;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -216,12 +253,17 @@ int main(int argc, char** argv) {
   knn_options opt;
   knn_default_options(&opt);
   opt.device = devices[0];
+  uint64_t seed = 0;
+  if (!env_knobs(opt, seed)) {
+    std::cout << "Initialization failed.\n";
+    return 8;
+  }
   std::vector<int32_t> idx((size_t)n * (k > 0 ? k : 1));
   std::vector<float> dist((size_t)n * (k > 0 ? k : 1));
   const auto t0 = std::chrono::steady_clock::now();
   int rc = knn_normalize_reference(x.data(), n, d);
   if (rc == KNN_OK)
-    rc = knn_build_ex(nullptr, x.data(), n, d, k, trees, leaf, props, metric, 0, idx.data(),
+    rc = knn_build_ex(nullptr, x.data(), n, d, k, trees, leaf, props, metric, seed, idx.data(),
                       dist.data(), &opt, nullptr);
   const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (rc != KNN_OK) {

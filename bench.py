@@ -604,6 +604,73 @@ def run_batch(args):
     return 0
 
 
+# ------------------------------------------------------- other configurations --
+def run_config(args):
+    """One named configuration at its literal parameters (sparse prototypes,
+    d=784, TAXICAB; normalised mixture, 10M x 96 FP16, COSINE): time of each
+    applicable path with device-resident points (plain FP32; mixed BF16 +
+    re-rank; for COSINE also learned splits trained on a 1M-point sample), and
+    recall@k against the FP64 exact graph on 10,000 seeded queries."""
+    import torch
+
+    torch.cuda.set_device(0)
+    acknn = load_package()
+    lib = acknn.load_library()
+    cfg = acknn.workloads.CONFIGS[args.workload]
+    n = args.n or cfg["n"]
+    k, T, L, P, metric = cfg["k"], cfg["trees"], cfg["leaf"], cfg["props"], cfg["metric"]
+    x = cfg["gen"](0, n=n)
+    d = x.shape[1]
+    dtype = acknn.F16 if x.dtype == np.float16 else acknn.F32
+    xd = torch.from_numpy(x).cuda()
+    idx = torch.empty((n, k), dtype=torch.int32, device="cuda")
+    dist = torch.empty((n, k), dtype=torch.float32, device="cuda")
+    ctx = acknn.Context(0)
+    stream = torch.cuda.current_stream()
+    paths = {"plain_fp32": dict(precision=acknn.PREC_FP32)}
+    if metric != 1:
+        paths["mixed"] = dict(precision=acknn.PREC_BF16_RERANK)
+    if metric == 2:
+        paths["mixed_learned"] = dict(precision=acknn.PREC_BF16_RERANK, learned_splits=1,
+                                      mlp_sample=min(n, 1_000_000))
+    rng = np.random.Generator(np.random.PCG64(12345))
+    q = np.sort(rng.choice(n, size=min(10_000, n), replace=False)).astype(np.int64)
+    ei, _ = acknn.exact_fp64(x, k, q, metric)
+    res = {}
+    for name, kw in paths.items():
+        def build(stats=None, kw=kw):
+            opt = acknn.default_options(points_on_device=1, outputs_on_device=1, dtype=dtype,
+                                        stream=stream.cuda_stream, **kw)
+            rc = lib.knn_build_ex(ctx.handle, xd.data_ptr(), n, d, k, T, L, P, metric, 0, idx.data_ptr(),
+                                  dist.data_ptr(), ctypes.byref(opt), ctypes.byref(stats) if stats else None)
+            if rc:
+                raise acknn.KnnError(rc, lib.knn_last_error().decode())
+        for _ in range(args.warmup):
+            build()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            build()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        st = acknn.KnnStats()
+        st.struct_size = ctypes.sizeof(acknn.KnnStats)
+        build(stats=st)
+        torch.cuda.synchronize()
+        ai = idx.cpu().numpy()[q]
+        rec = sum(len(np.intersect1d(a, b)) for a, b in zip(ai, ei)) / (k * len(q))
+        sd = st.as_dict()
+        res[name] = {"ms_per_build": ms, "points_per_s": n / (ms / 1e3), "recall": rec,
+                     "stages_ms": {kk: sd[kk] for kk in ("ms_learn", "ms_trees", "ms_leaf", "ms_propagate")}}
+    print(json.dumps({"workload": args.workload, "n": n, "d": d, "k": k, "trees": T, "leaf": L, "props": P,
+                      "metric": METRIC_NAMES[metric], "dtype": str(x.dtype), "queries": int(len(q)),
+                      "steps": args.steps, "warmup": args.warmup, "paths": res}), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -614,7 +681,8 @@ def main():
     ap.add_argument("--n", type=int, default=None, help="override N (smaller runs)")
     ap.add_argument("--cpu-sample", type=int, default=20_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["integer_mixture", "dataset_batch"], default="integer_mixture")
+    ap.add_argument("--workload", choices=["integer_mixture", "dataset_batch", "sparse_prototypes",
+                                           "normalized_mixture"], default="integer_mixture")
     ap.add_argument("--count", type=int, default=None, help="datasets in the batch workload")
     ap.add_argument("--single", choices=["mixed", "plain"], default=None,
                     help="time one configuration only (the profiling case)")
@@ -631,6 +699,8 @@ def main():
         return run_reference(args, w)
     if args.workload == "dataset_batch":
         return run_batch(args)
+    if args.workload in ("sparse_prototypes", "normalized_mixture"):
+        return run_config(args)
     if args.single:
         return run_single(args, w)
     return run_ours(args, w)

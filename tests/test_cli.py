@@ -89,3 +89,45 @@ def test_cli_matches_library_and_mirror(hello, tmp_path, metric):
     assert edm.deinitialize() is False
     assert (tmp_path / "mirror.bin").read_bytes() == out.read_bytes()
     assert (tmp_path / "mirror.binDEBUG").read_text() == (tmp_path / "out.binDEBUG").read_text()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("env, kw", [
+    ({"ACKNN_PRECISION": "bf16", "ACKNN_SEED": "11"}, {"precision": 1, "seed": 11}),
+    ({"ACKNN_SPLITS": "reference", "ACKNN_SEED": "3"}, {"split_rule": 1, "seed": 3}),
+])
+def test_cli_environment_knobs(hello, tmp_path, env, kw):
+    """Precision, split rule and seed come from ACKNN_* variables; the
+    positional command line is unchanged and the graph is the library's with
+    the same options."""
+    import os
+
+    acknn = load_package()
+    f = acknn.formats
+    n, d, k = 4000, 12, 8
+    x = _points(n, d, 8)
+    csv = tmp_path / "in.csv"
+    f.write_csv(str(csv), x)
+    out = tmp_path / "out.bin"
+    r = subprocess.run([hello, str(csv), str(out), str(k), "4", "64", "1", "EUCLIDEAN", "0", "F"],
+                       capture_output=True, text=True, timeout=600, env={**os.environ, **env})
+    assert r.returncode == 0, r.stdout
+    _, _, ids, stored = f.read_result(str(out))
+    xn = acknn.normalize_reference(f.read_csv(str(csv), klaster=False)[0])
+    idx, dist = acknn.knn_build(xn, k, 4, 64, 1, 0, **kw)
+    np.testing.assert_array_equal(ids, idx)
+    np.testing.assert_array_equal(stored, f.stored_distance(dist, 0))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("env", [{"ACKNN_PRECISION": "fp8"}, {"ACKNN_SPLITS": "sideways"}, {"ACKNN_SEED": "-1"}])
+def test_cli_rejects_unknown_knob_values(hello, tmp_path, env):
+    import os
+
+    acknn = load_package()
+    csv = tmp_path / "in.csv"
+    acknn.formats.write_csv(str(csv), _points(100, 4, 1))
+    r = subprocess.run([hello, str(csv), str(tmp_path / "o"), "3", "2", "16", "1", "EUCLIDEAN", "0", "F"],
+                       capture_output=True, text=True, timeout=600, env={**os.environ, **env})
+    assert r.returncode == 8
+    assert "Initialization failed." in r.stdout
