@@ -21,10 +21,11 @@
 //   * completion: tcgen05.commit -> mbarrier, waited with an iteration limit
 //     (on expiry the block records an error, drains, frees TMEM and returns);
 //   * epilogue: per 64-column round, tcgen05.ld 32x32b.x32 by all 8 warps (warp
-//     w reads lane quarter w%4, 32 columns), keys filtered against each row's
-//     current last entry, then one warp per row inserts the row's few
-//     survivors into that query's sorted list (held in shared memory for the
-//     whole block) with one ballot and one lane shift each.
+//     w reads lane quarter w%4, 32 columns); three instructions per key filter
+//     it against a slightly widened bound of the row's current last entry into
+//     a survivor bit mask, then one warp per row computes its few survivors'
+//     keys and inserts them into that query's sorted list (held in shared
+//     memory for the whole block) with one ballot and one lane shift each.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -42,12 +43,11 @@ constexpr int kChunkBytes = kBM * 128; // one 128 x 64 bf16 operand chunk
 constexpr uint32_t kTmemCols = 128;
 constexpr int kUThreads = 256;
 constexpr int kRound = 64;          // tile columns per epilogue round
-constexpr int kBulkMerge = 12;      // first tree: survivors in a chunk from which sort + merge pays
-// Round keys live in the B-operand region once the tile's MMA has completed:
-// 128 rows x 64 floats (32 KB), column index xor-swizzled by the row at 32-float
-// granularity so that row-parallel writes and column-parallel reads hit distinct banks.
+constexpr int kBulkMerge = 12;      // first tree: survivors in a half round from which sort + merge pays
+constexpr float kSlack = 4.76837158203125e-07f;  // 2^-21: filter widening, eight units of FP32 rounding
+// Round products live in the B-operand region once the tile's MMA has completed:
+// 128 rows x 64 floats (32 KB).
 constexpr int kKsBytes = kBM * kRound * 4;
-__device__ __forceinline__ int ks_at(int r, int c) { return r * kRound + (c ^ (r & 31)); }
 constexpr int kLS = 33;              // list row stride (row owners hit distinct banks)
 // A 128x128x256 tile finishes in about a microsecond; 2^16 polls with 32 ns
 // sleeps (a few ms) is far beyond that, and keeps a failing launch short.
@@ -164,13 +164,14 @@ __device__ __forceinline__ void stage_operand(unsigned char* op, const __nv_bflo
 // One block per (leaf, 128-query tile).  The 128 queries' lists stay in shared
 // memory for the whole loop over candidate tiles (read once, written once);
 // each 128x128 tensor-core tile is emptied in two 64-column rounds: epilogue
-// (tcgen05.ld, approximate key, filter against the row's current last entry)
-// then a per-row merge of the survivors.  Prologue, MMA issue, bounded wait
-// and the tensor-memory loads follow the single-tile sequence that was checked
-// on its own against a CPU product.
+// (tcgen05.ld, a conservative per-row filter packed into survivor bit masks,
+// raw products parked in shared memory) then a per-row merge that computes the
+// survivors' keys and applies the exact rule.  Prologue, MMA issue, bounded
+// wait and the tensor-memory loads follow the single-tile sequence that was
+// checked on its own against a CPU product.
 // FIRST: the launch of the first tree, whose lists start empty; a point then
 // meets every candidate once, so no survivor can already be listed, and a
-// chunk with many survivors is sorted and merged into the list in one go.
+// half round with many survivors is sorted and merged into the list in one go.
 template <int METRIC, bool FIRST>
 __global__ void __launch_bounds__(kUThreads, 2)
     k_leaf_tc(const __nv_bfloat16* __restrict__ Xb, int Kp, SegView segs, const int64_t* __restrict__ ftab, int k,
@@ -183,16 +184,16 @@ __global__ void __launch_bounds__(kUThreads, 2)
   unsigned char* opA = smem;
   unsigned char* opB = opA + nchunks * kChunkBytes;
   const int bbytes = max(nchunks * kChunkBytes, kKsBytes);
-  float* Ks = reinterpret_cast<float*>(opB);                           // round keys (reuses B)
+  float* Ks = reinterpret_cast<float*>(opB);                           // round products (reuses B)
   float* Lk = reinterpret_cast<float*>(opB + bbytes);                  // [128][kLS] list keys
   uint32_t* Li = reinterpret_cast<uint32_t*>(Lk + kBM * kLS);         // [128][kLS] list ids
   int32_t* qid = reinterpret_cast<int32_t*>(Li + kBM * kLS);
   int32_t* cid = qid + kBM;
   float* qn = reinterpret_cast<float*>(cid + kBN);
-  float* cn = qn + kBM;
-  int* cnt = reinterpret_cast<int*>(cn + kBN);  // survivors of each row in the current round
-  uint8_t* sq = reinterpret_cast<uint8_t*>(cnt + kBM);  // [128][kRound] their columns in the round
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(sq + kBM * kRound);
+  float* cn = qn + kBM;  // candidate norms (EUCLIDEAN) or 0; +inf for padding columns
+  uint32_t* msk = reinterpret_cast<uint32_t*>(cn + kBN);  // [128][2] survivor bits of the round
+  float* cmax = reinterpret_cast<float*>(msk + kBM * 2);  // [4] largest candidate norm per warp
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(cmax + 4);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
   int* status = reinterpret_cast<int*>(tmem_slot + 1);
 
@@ -217,6 +218,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
   const int mq = min(kBM, nq - q0);
   const int nb = (int)(bhi - blo);
   const float kInf = __int_as_float(0x7F800000);
+  const float kMaxF = __int_as_float(0x7F7FFFFF);
   const uint32_t bar = smem_u32(mbar);
 
   if (warp == 0) {
@@ -248,11 +250,14 @@ __global__ void __launch_bounds__(kUThreads, 2)
   uint32_t phase = 0;
   for (int c0 = 0; c0 < nb; c0 += kBN) {
     const int mc = min(kBN, nb - c0);
-    if (tid < kBN) {
+    if (tid < kBN) {  // warps 0-3, whole warps
       const int32_t id = tid < mc ? perm[blo + c0 + tid] : -1;
       cid[tid] = id;
-      cn[tid] = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
-      cnt[tid] = 0;
+      const float nv = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
+      cn[tid] = id >= 0 ? nv : kInf;
+      // norms are >= 0, so their bit patterns order as unsigned integers
+      const uint32_t wm = __reduce_max_sync(0xFFFFFFFFu, __float_as_uint(nv));
+      if (lane == 0) cmax[warp] = __uint_as_float(wm);
     }
     __syncthreads();
     stage_operand(opB, Xb, Kp, cid);
@@ -285,6 +290,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
     phase ^= 1u;
     if (*status != 0) break;  // uniform: read after the barrier
 
+    const float cm = fmaxf(fmaxf(cmax[0], cmax[1]), fmaxf(cmax[2], cmax[3]));
     for (int rb = 0; rb < mc; rb += kRound) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
       {
@@ -293,60 +299,79 @@ __global__ void __launch_bounds__(kUThreads, 2)
         const int col0 = rb + half * 32;
         uint32_t v[32];
         tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)col0, v);
-        const bool rv = r < mq;
-        const float myn = qn[r];
-        // a superset of the keys that can still enter the row's list (the
-        // exact (key, id) rule and listed ids are settled by the merge): one
-        // compare per column, survivors as a bit mask
-        const float tk = Lk[r * kLS + kq - 1];
-        uint32_t mask = 0;
+        // raw products for the merge: 16-byte chunks xor-swizzled by the row,
+        // so that row-parallel writes and column-parallel reads hit distinct banks
+        float4* ks4 = reinterpret_cast<float4*>(Ks) + r * (kRound / 4);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int c = col0 + j;
-          const float dot = __uint_as_float(v[j]);
-          const float key = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[c]))
-                                                           : __fsub_rn(1.f, dot);
-          Ks[ks_at(r, half * 32 + j)] = key;
-          mask |= (rv && c < mc && key <= tk) ? (1u << j) : 0u;
+        for (int q = 0; q < 8; ++q)
+          ks4[(half * 8 + q) ^ (r & 7)] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                                                       __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+        // Row filter, a superset of what the exact rule (key <= the row's
+        // current last entry tk) can admit: key' = |y|^2 - 2 x.y (EUCLIDEAN)
+        // or -x.y (COSINE) against thr = tk - |x|^2 (or tk - 1) widened by
+        // 2^-21 (|tk| + |x|^2 + max|y|^2), which bounds the rounding of both
+        // the key and the threshold.  Padding columns have key' = +inf, a row
+        // outside the block thr = -inf, a list with free slots thr = FLT_MAX.
+        const float tk = Lk[r * kLS + kq - 1];
+        float thr;
+        if (r >= mq) thr = -kInf;
+        else if (tk == kInf) thr = kMaxF;
+        else if (METRIC == KNN_METRIC_EUCLIDEAN) {
+          const float myn = qn[r];
+          thr = fminf((tk - myn) + kSlack * (fabsf(tk) + myn + cm), kMaxF);
+        } else {
+          thr = fminf((tk - 1.f) + kSlack * (fabsf(tk) + 2.f), kMaxF);
         }
+        // bit j of neg = sign of thr - key'_j, shifted in from column 31 down
+        const float4* cn4 = reinterpret_cast<const float4*>(cn + col0);
+        uint32_t neg = 0;
+#pragma unroll
+        for (int q = 7; q >= 0; --q) {
+          const float4 c = cn4[q];
+          const float cc[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+          for (int e = 3; e >= 0; --e) {
+            const float dot = __uint_as_float(v[4 * q + e]);
+            const float kp = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, cc[e]) : __fsub_rn(cc[e], dot);
+            neg = __funnelshift_l(__float_as_uint(__fsub_rn(thr, kp)), neg, 1);
+          }
+        }
+        uint32_t mask = ~neg;
         // the row's own point (its leaf lies inside the block) never survives
         const int64_t selfbit = (lo + q0 + r) - blo - c0 - col0;
         if (selfbit >= 0 && selfbit < 32) mask &= ~(1u << (int)selfbit);
-        if (mask) {
-          int slot = atomicAdd(&cnt[r], __popc(mask));
-          while (mask) {
-            const int j = __ffs(mask) - 1;
-            mask &= mask - 1;
-            sq[r * kRound + slot++] = (uint8_t)(half * 32 + j);
-          }
-        }
+        msk[r * 2 + half] = mask;
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       __syncthreads();
-      // one warp per query row with survivors, read from the row's queue: list
-      // one entry per lane; each survivor is checked against the list ids by
-      // one ballot and placed by warp_insert1 (which drops a candidate behind
-      // all 32 entries)
+      // one warp per query row with survivors; lane l holds the round's
+      // columns l and 32 + l.  The survivor's exact key is computed here; each
+      // is checked against the list ids by one ballot and placed by
+      // warp_insert1 (which drops a candidate behind all 32 entries).
       for (int qq = warp; qq < mq; qq += kUThreads / 32) {
-        const int ns = cnt[qq];
-        if (ns == 0) continue;
+        const uint32_t m0 = msk[qq * 2], m1 = msk[qq * 2 + 1];
+        if ((m0 | m1) == 0) continue;
         float lk = Lk[qq * kLS + lane];
         uint32_t li = Li[qq * kLS + lane];
-        for (int b0 = 0; b0 < ns; b0 += 32) {
-          const int e = b0 + lane;
+        const float myn = qn[qq];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          uint32_t bal = h ? m1 : m0;
+          if (bal == 0) continue;
+          const int col = h * 32 + lane;
           float ck = kInf;
           uint32_t ci = kNoId;
-          if (e < ns) {
-            const int col = sq[qq * kRound + e];
-            ck = Ks[ks_at(qq, col)];
+          if ((bal >> lane) & 1u) {
+            const float dot = Ks[qq * kRound + ((((col >> 2) ^ (qq & 7)) << 2) | (col & 3))];
+            ck = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[rb + col]))
+                                                : __fsub_rn(1.f, dot);
             ci = (uint32_t)cid[rb + col];
           }
-          if (FIRST && ns - b0 >= kBulkMerge) {
+          if (FIRST && __popc(bal) >= kBulkMerge) {
             warp_bitonic_sort32(ck, ci);
             warp_merge_lower(lk, li, ck, ci);
             continue;
           }
-          uint32_t bal = __ballot_sync(0xFFFFFFFFu, e < ns);
           while (bal) {
             const int src = __ffs(bal) - 1;
             bal &= bal - 1;
@@ -358,8 +383,6 @@ __global__ void __launch_bounds__(kUThreads, 2)
         }
         Lk[qq * kLS + lane] = lk;
         Li[qq * kLS + lane] = li;
-        __syncwarp();
-        if (lane == 0) cnt[qq] = 0;
       }
       __syncthreads();
     }
@@ -473,11 +496,11 @@ __global__ void __launch_bounds__(256) k_rerank(const float* __restrict__ X, int
 }
 
 size_t umma_smem_bytes(int Kp) {
-  // alignment slack + A + B (also the round keys) + lists + (qid, cid, qn, cn) + cnt + survivor
-  // queues + barrier words
+  // alignment slack + A + B (also the round products) + lists + (qid, cid, qn, cn) + survivor
+  // masks + per-warp norm maxima + barrier words
   const size_t bbytes = std::max((size_t)(Kp / kKC) * kChunkBytes, (size_t)kKsBytes);
   return 1024 + (size_t)(Kp / kKC) * kChunkBytes + bbytes + (size_t)kBM * kLS * 8 +
-         (size_t)(kBM + kBN) * 8 + (size_t)kBM * 4 + (size_t)kBM * kRound + 64;
+         (size_t)(kBM + kBN) * 8 + (size_t)kBM * 2 * 4 + 16 + 64;
 }
 
 int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
