@@ -413,6 +413,7 @@ int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, in
   a.rid = L->id[L->cur];
   int rc = C->get("Xb", (size_t)n * Kp * 2, &a.Xb);
   if (!rc) rc = C->get("norms2", (size_t)n, &a.norms2);
+  if (!rc && trees > 1) rc = C->get("linv", (size_t)n, &a.inv);
   if (!rc) rc = C->get("akey", (size_t)n * kq, &a.akey);
   if (!rc) rc = C->get("aid", (size_t)n * kq, &a.aid);
   if (rc) return rc;

@@ -121,6 +121,7 @@ struct UmmaLeafArgs {
   const float* norms;    // [n] FP32 norms (COSINE) or null
   void* Xb;              // [n][Kp] bf16 scratch (Kp = d rounded up to 64)
   float* norms2;         // [n] scratch
+  int32_t* inv;          // [n] scratch: a tree's inverse order (null: duplicate checks in the merge)
   float* akey;           // [n][kq] approximate lists (in: empty)
   uint32_t* aid;
   float* rkey;           // [n][k] out: exact keys, sorted

@@ -45,6 +45,11 @@ constexpr int kUThreads = 256;
 constexpr int kRound = 64;          // tile columns per epilogue round
 constexpr int kBulkMerge = 12;      // first tree: survivors in a half round from which sort + merge pays
 constexpr float kSlack = 4.76837158203125e-07f;  // 2^-21: filter widening, eight units of FP32 rounding
+// Listed candidates inside the block, per row: sorted 16-bit column positions
+// ending in kXEnd (blocks of up to kXMaxBlock columns).
+constexpr int kXS = 34;
+constexpr uint32_t kXEnd = 0xFFFFu;
+constexpr int kXMaxBlock = 65000;
 // Round products live in the B-operand region once the tile's MMA has completed:
 // 128 rows x 64 floats (32 KB).
 constexpr int kKsBytes = kBM * kRound * 4;
@@ -161,6 +166,21 @@ __device__ __forceinline__ void stage_operand(unsigned char* op, const __nv_bflo
 
 }  // namespace
 
+// Ascending sort of one value per lane (bitonic network over the warp).
+__device__ __forceinline__ uint32_t warp_sort32_u32(uint32_t v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+    for (int m = size >> 1; m >= 1; m >>= 1) {
+      const uint32_t o = __shfl_xor_sync(0xFFFFFFFFu, v, m);
+      const bool keep_min = ((lane & size) == 0) == ((lane & m) == 0);
+      v = keep_min ? min(v, o) : max(v, o);
+    }
+  }
+  return v;
+}
+
 // One block per (leaf, 128-query tile).  The 128 queries' lists stay in shared
 // memory for the whole loop over candidate tiles (read once, written once);
 // each 128x128 tensor-core tile is emptied in two 64-column rounds: epilogue
@@ -172,12 +192,18 @@ __device__ __forceinline__ void stage_operand(unsigned char* op, const __nv_bflo
 // FIRST: the launch of the first tree, whose lists start empty; a point then
 // meets every candidate once, so no survivor can already be listed, and a
 // half round with many survivors is sorted and merged into the list in one go.
+// Later trees, with inv (the tree's inverse order): the block's columns that
+// hold an id already in the row's list are found up front (inv of each listed
+// id) and masked out of the survivors, so the merge needs no duplicate check;
+// a candidate meets a row once per tree, so ids inserted during the block
+// cannot come back.
 template <int METRIC, bool FIRST>
 __global__ void __launch_bounds__(kUThreads, 2)
     k_leaf_tc(const __nv_bfloat16* __restrict__ Xb, int Kp, SegView segs, const int64_t* __restrict__ ftab, int k,
               int kq,
-              int qtiles, const int32_t* __restrict__ perm, const float* __restrict__ norms2,
-              float* __restrict__ akey, uint32_t* __restrict__ aid, int* __restrict__ err) {
+              int qtiles, const int32_t* __restrict__ perm, const int32_t* __restrict__ inv,
+              const float* __restrict__ norms2, float* __restrict__ akey, uint32_t* __restrict__ aid,
+              int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int nchunks = Kp / kKC;
@@ -193,7 +219,8 @@ __global__ void __launch_bounds__(kUThreads, 2)
   float* cn = qn + kBM;  // candidate norms (EUCLIDEAN) or 0; +inf for padding columns
   uint32_t* msk = reinterpret_cast<uint32_t*>(cn + kBN);  // [128][2] survivor bits of the round
   float* cmax = reinterpret_cast<float*>(msk + kBM * 2);  // [4] largest candidate norm per warp
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(cmax + 4);
+  uint16_t* xp = reinterpret_cast<uint16_t*>(cmax + 4);   // [128][kXS] listed columns
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(xp + kBM * kXS);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
   int* status = reinterpret_cast<int*>(tmem_slot + 1);
 
@@ -217,6 +244,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
   if (q0 >= nq) return;  // whole block, before any barrier or allocation
   const int mq = min(kBM, nq - q0);
   const int nb = (int)(bhi - blo);
+  const bool xcl = !FIRST && inv != nullptr && nb <= kXMaxBlock;  // block-uniform
   const float kInf = __int_as_float(0x7F800000);
   const float kMaxF = __int_as_float(0x7F7FFFFF);
   const uint32_t bar = smem_u32(mbar);
@@ -246,6 +274,31 @@ __global__ void __launch_bounds__(kUThreads, 2)
     Li[r * kLS + s] = live ? aid[(size_t)id * kq + s] : kNoId;
   }
   stage_operand(opA, Xb, Kp, qid);
+  if (xcl) {
+    // warp w: rows w, w + 8, ...; lane s: the row's s-th listed id
+    uint32_t pos[kBM / 8];
+#pragma unroll
+    for (int i = 0; i < kBM / 8; ++i) {
+      const int32_t id = qid[warp + 8 * i];
+      pos[i] = (id >= 0 && lane < kq) ? aid[(size_t)id * kq + lane] : kNoId;
+    }
+#pragma unroll
+    for (int i = 0; i < kBM / 8; ++i) {
+      uint32_t p = kXEnd;
+      if (pos[i] != kNoId) {
+        const int64_t q = (int64_t)inv[pos[i]] - blo;
+        if (q >= 0 && q < nb) p = (uint32_t)q;
+      }
+      pos[i] = p;
+    }
+#pragma unroll
+    for (int i = 0; i < kBM / 8; ++i) {
+      const uint32_t v = warp_sort32_u32(pos[i]);
+      xp[(warp + 8 * i) * kXS + lane] = (uint16_t)v;
+      if (lane == 0) xp[(warp + 8 * i) * kXS + 32] = (uint16_t)kXEnd;
+    }
+  }
+  int xptr = 0;  // this thread's next entry of its row's listed columns
 
   uint32_t phase = 0;
   for (int c0 = 0; c0 < nb; c0 += kBN) {
@@ -340,49 +393,68 @@ __global__ void __launch_bounds__(kUThreads, 2)
         // the row's own point (its leaf lies inside the block) never survives
         const int64_t selfbit = (lo + q0 + r) - blo - c0 - col0;
         if (selfbit >= 0 && selfbit < 32) mask &= ~(1u << (int)selfbit);
+        if (xcl) {
+          // listed ids among these 32 columns: walk the row's sorted
+          // positions (each thread's columns only increase)
+          const int lo_c = c0 + col0;
+          uint32_t ex = 0;
+          int p = xp[r * kXS + xptr];
+          while (p < lo_c + 32) {
+            if (p >= lo_c) ex |= 1u << (p - lo_c);
+            p = xp[r * kXS + (++xptr)];
+          }
+          mask &= ~ex;
+        }
         msk[r * 2 + half] = mask;
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       __syncthreads();
-      // one warp per query row with survivors; lane l holds the round's
-      // columns l and 32 + l.  The survivor's exact key is computed here; each
-      // is checked against the list ids by one ballot and placed by
-      // warp_insert1 (which drops a candidate behind all 32 entries).
-      for (int qq = warp; qq < mq; qq += kUThreads / 32) {
-        const uint32_t m0 = msk[qq * 2], m1 = msk[qq * 2 + 1];
-        if ((m0 | m1) == 0) continue;
-        float lk = Lk[qq * kLS + lane];
-        uint32_t li = Li[qq * kLS + lane];
-        const float myn = qn[qq];
+      // one warp per query row with survivors (found by one ballot over the
+      // warp's 16 rows); lane l holds the round's columns l and 32 + l.  The
+      // survivor's exact key is computed here; few survivors are placed one
+      // by one by warp_insert1 (which drops a candidate behind all 32
+      // entries), many (first tree) by one sort and merge.
+      {
+        const int myrow = warp + (kUThreads / 32) * (lane & 15);
+        const bool has = lane < 16 && myrow < mq && (msk[myrow * 2] | msk[myrow * 2 + 1]) != 0;
+        uint32_t rows = __ballot_sync(0xFFFFFFFFu, has);
+        while (rows) {
+          const int qq = warp + (kUThreads / 32) * (__ffs(rows) - 1);
+          rows &= rows - 1;
+          const uint32_t m0 = msk[qq * 2], m1 = msk[qq * 2 + 1];
+          float lk = Lk[qq * kLS + lane];
+          uint32_t li = Li[qq * kLS + lane];
+          const float myn = qn[qq];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          uint32_t bal = h ? m1 : m0;
-          if (bal == 0) continue;
-          const int col = h * 32 + lane;
-          float ck = kInf;
-          uint32_t ci = kNoId;
-          if ((bal >> lane) & 1u) {
-            const float dot = Ks[qq * kRound + ((((col >> 2) ^ (qq & 7)) << 2) | (col & 3))];
-            ck = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[rb + col]))
-                                                : __fsub_rn(1.f, dot);
-            ci = (uint32_t)cid[rb + col];
+          for (int h = 0; h < 2; ++h) {
+            uint32_t bal = h ? m1 : m0;
+            if (bal == 0) continue;
+            const int col = h * 32 + lane;
+            float ck = kInf;
+            uint32_t ci = kNoId;
+            if ((bal >> lane) & 1u) {
+              const float dot = Ks[qq * kRound + ((((col >> 2) ^ (qq & 7)) << 2) | (col & 3))];
+              ck = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[rb + col]))
+                                                  : __fsub_rn(1.f, dot);
+              ci = (uint32_t)cid[rb + col];
+            }
+            if (FIRST && __popc(bal) >= kBulkMerge) {
+              warp_bitonic_sort32(ck, ci);
+              warp_merge_lower(lk, li, ck, ci);
+              continue;
+            }
+            while (bal) {
+              const int src = __ffs(bal) - 1;
+              bal &= bal - 1;
+              const float k1 = __shfl_sync(0xFFFFFFFFu, ck, src);
+              const uint32_t i1 = __shfl_sync(0xFFFFFFFFu, ci, src);
+              const bool dup = !FIRST && !xcl && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
+              if (!dup) warp_insert1(lk, li, k1, i1);
+            }
           }
-          if (FIRST && __popc(bal) >= kBulkMerge) {
-            warp_bitonic_sort32(ck, ci);
-            warp_merge_lower(lk, li, ck, ci);
-            continue;
-          }
-          while (bal) {
-            const int src = __ffs(bal) - 1;
-            bal &= bal - 1;
-            const float k1 = __shfl_sync(0xFFFFFFFFu, ck, src);
-            const uint32_t i1 = __shfl_sync(0xFFFFFFFFu, ci, src);
-            const bool dup = !FIRST && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
-            if (!dup) warp_insert1(lk, li, k1, i1);
-          }
+          Lk[qq * kLS + lane] = lk;
+          Li[qq * kLS + lane] = li;
         }
-        Lk[qq * kLS + lane] = lk;
-        Li[qq * kLS + lane] = li;
       }
       __syncthreads();
     }
@@ -403,6 +475,12 @@ __global__ void __launch_bounds__(kUThreads, 2)
     __syncwarp();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(*tmem_slot), "r"(kTmemCols));
   }
+}
+
+// inv[order[i]] = i: the position of each point in a tree's order.
+__global__ void k_inverse_order(const int32_t* __restrict__ order, int64_t n, int32_t* __restrict__ inv) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    inv[order[i]] = (int32_t)i;
 }
 
 // BF16 operand copy: rows of Kp bf16 (zero padded), COSINE rows divided by
@@ -497,10 +575,10 @@ __global__ void __launch_bounds__(256) k_rerank(const float* __restrict__ X, int
 
 size_t umma_smem_bytes(int Kp) {
   // alignment slack + A + B (also the round products) + lists + (qid, cid, qn, cn) + survivor
-  // masks + per-warp norm maxima + barrier words
+  // masks + per-warp norm maxima + listed columns + barrier words
   const size_t bbytes = std::max((size_t)(Kp / kKC) * kChunkBytes, (size_t)kKsBytes);
   return 1024 + (size_t)(Kp / kKC) * kChunkBytes + bbytes + (size_t)kBM * kLS * 8 +
-         (size_t)(kBM + kBN) * 8 + (size_t)kBM * 2 * 4 + 16 + 64;
+         (size_t)(kBM + kBN) * 8 + (size_t)kBM * 2 * 4 + 16 + (size_t)kBM * kXS * 2 + 64;
 }
 
 int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
@@ -521,11 +599,17 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
     const int64_t tleaves = a.ftable ? a.fcount[t] : leaves;
     if (tleaves <= 0) continue;
     const unsigned grid = (unsigned)(tleaves * qtiles);
+    const int32_t* inv = nullptr;
+    if (t > 0 && a.inv) {
+      k_inverse_order<<<(unsigned)std::min<int64_t>((a.n + 255) / 256, 148 * 16), 256, 0, st>>>(perm, a.n, a.inv);
+      log.add();
+      inv = a.inv;
+    }
 #define KNN_TC_LAUNCH(M, F)                                                                               \
   do {                                                                                                    \
     cudaFuncSetAttribute(k_leaf_tc<M, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);       \
-    k_leaf_tc<M, F><<<grid, kUThreads, smem, st>>>(Xb, Kp, a.segs, ftab, a.k, a.kq, qtiles, perm, a.norms2, a.akey, \
-                                                   a.aid, a.err);                                        \
+    k_leaf_tc<M, F><<<grid, kUThreads, smem, st>>>(Xb, Kp, a.segs, ftab, a.k, a.kq, qtiles, perm, inv, a.norms2, \
+                                                   a.akey, a.aid, a.err);                                \
   } while (0)
     if (a.metric == KNN_METRIC_EUCLIDEAN) {
       if (t == 0) KNN_TC_LAUNCH(KNN_METRIC_EUCLIDEAN, true);
