@@ -50,6 +50,11 @@ constexpr float kSlack = 4.76837158203125e-07f;  // 2^-21: filter widening, eigh
 constexpr int kXS = 34;
 constexpr uint32_t kXEnd = 0xFFFFu;
 constexpr int kXMaxBlock = 65000;
+// First tree: blocks of at least kPrepassMin columns get a bounding pass; its
+// group minima (64 per row, row stride kGS) use the list area.
+constexpr int kPrepassMin = 1024;
+constexpr int kGroups = 64;
+constexpr int kGS = kGroups + 1;
 // Round products live in the B-operand region once the tile's MMA has completed:
 // 128 rows x 64 floats (32 KB).
 constexpr int kKsBytes = kBM * kRound * 4;
@@ -220,7 +225,8 @@ __global__ void __launch_bounds__(kUThreads, 2)
   uint32_t* msk = reinterpret_cast<uint32_t*>(cn + kBN);  // [128][2] survivor bits of the round
   float* cmax = reinterpret_cast<float*>(msk + kBM * 2);  // [4] largest candidate norm per warp
   uint16_t* xp = reinterpret_cast<uint16_t*>(cmax + 4);   // [128][kXS] listed columns
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(xp + kBM * kXS);
+  float* tcap = reinterpret_cast<float*>(xp + kBM * kXS);  // [128] first tree: bound on the kq-th key
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tcap + kBM);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
   int* status = reinterpret_cast<int*>(tmem_slot + 1);
 
@@ -265,13 +271,26 @@ __global__ void __launch_bounds__(kUThreads, 2)
     qid[tid] = id;
     qn[tid] = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
   }
+  // First tree, blocks of kPrepassMin columns or more: pass 0 runs the tiles
+  // once to record each row's smallest exact key in each of kGroups groups of
+  // columns (32-column slices, wrapping).  The kq-th smallest group minimum is
+  // the key of kq distinct candidates, so it bounds the kq-th key of the
+  // final list; pass 1 filters against it from the first tile on, which
+  // leaves a few dozen survivors per row instead of ~kq ln(columns / kq).
+  const bool pre = FIRST && nb >= kPrepassMin;
+  float* gm = Lk;  // [128][kGS] group minima during pass 0 (spans Lk and Li)
+  if (tid < kBM) tcap[tid] = kInf;
   __syncthreads();
-  for (int e = tid; e < kBM * 32; e += kUThreads) {
-    const int r = e >> 5, s = e & 31;
-    const int32_t id = qid[r];
-    const bool live = id >= 0 && s < kq;
-    Lk[r * kLS + s] = live ? akey[(size_t)id * kq + s] : kInf;
-    Li[r * kLS + s] = live ? aid[(size_t)id * kq + s] : kNoId;
+  if (pre) {
+    for (int e = tid; e < kBM * kGS; e += kUThreads) gm[e] = kInf;
+  } else {
+    for (int e = tid; e < kBM * 32; e += kUThreads) {
+      const int r = e >> 5, s = e & 31;
+      const int32_t id = qid[r];
+      const bool live = id >= 0 && s < kq;
+      Lk[r * kLS + s] = live ? akey[(size_t)id * kq + s] : kInf;
+      Li[r * kLS + s] = live ? aid[(size_t)id * kq + s] : kNoId;
+    }
   }
   stage_operand(opA, Xb, Kp, qid);
   if (xcl) {
@@ -301,162 +320,208 @@ __global__ void __launch_bounds__(kUThreads, 2)
   int xptr = 0;  // this thread's next entry of its row's listed columns
 
   uint32_t phase = 0;
-  for (int c0 = 0; c0 < nb; c0 += kBN) {
-    const int mc = min(kBN, nb - c0);
-    if (tid < kBN) {  // warps 0-3, whole warps
-      const int32_t id = tid < mc ? perm[blo + c0 + tid] : -1;
-      cid[tid] = id;
-      const float nv = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
-      cn[tid] = id >= 0 ? nv : kInf;
-      // norms are >= 0, so their bit patterns order as unsigned integers
-      const uint32_t wm = __reduce_max_sync(0xFFFFFFFFu, __float_as_uint(nv));
-      if (lane == 0) cmax[warp] = __uint_as_float(wm);
-    }
-    __syncthreads();
-    stage_operand(opB, Xb, Kp, cid);
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    const uint32_t tmem = *tmem_slot;
-    if (tid == 0) {
-      if (*reinterpret_cast<volatile int*>(err) != 0) {
-        *status = 2;  // another block failed: issue nothing more
-      } else {
-        const uint32_t a0 = smem_u32(opA), b0 = smem_u32(opB);
-        for (int ch = 0; ch < nchunks; ++ch)
-#pragma unroll
-          for (int kk = 0; kk < kKC / 16; ++kk) {
-            const uint32_t off = ch * kChunkBytes + kk * 32;
-            umma_bf16(tmem, desc_sw128(a0 + off), desc_sw128(b0 + off), (ch | kk) != 0 ? 1u : 0u);
-          }
-        umma_commit(bar);
-        if (!mbar_wait_bounded(bar, phase)) {
-          *status = 1;
-          atomicExch(err, 1);
-          mbar_wait_bounded(bar, phase);  // let the MMAs drain before TMEM is freed
-        }
+  for (int pass = pre ? 0 : 1; pass < 2; ++pass) {
+    for (int c0 = 0; c0 < nb; c0 += kBN) {
+      const int mc = min(kBN, nb - c0);
+      if (tid < kBN) {  // warps 0-3, whole warps
+        const int32_t id = tid < mc ? perm[blo + c0 + tid] : -1;
+        cid[tid] = id;
+        const float nv = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
+        cn[tid] = id >= 0 ? nv : kInf;
+        // norms are >= 0, so their bit patterns order as unsigned integers
+        const uint32_t wm = __reduce_max_sync(0xFFFFFFFFu, __float_as_uint(nv));
+        if (lane == 0) cmax[warp] = __uint_as_float(wm);
       }
-    }
-    __syncthreads();
-    phase ^= 1u;
-    if (*status != 0) break;  // uniform: read after the barrier
-
-    const float cm = fmaxf(fmaxf(cmax[0], cmax[1]), fmaxf(cmax[2], cmax[3]));
-    for (int rb = 0; rb < mc; rb += kRound) {
-      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      {
-        const int quarter = warp & 3, half = warp >> 2;
-        const int r = quarter * 32 + lane;
-        const int col0 = rb + half * 32;
-        uint32_t v[32];
-        tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)col0, v);
-        // raw products for the merge: 16-byte chunks xor-swizzled by the row,
-        // so that row-parallel writes and column-parallel reads hit distinct banks
-        float4* ks4 = reinterpret_cast<float4*>(Ks) + r * (kRound / 4);
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-          ks4[(half * 8 + q) ^ (r & 7)] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
-                                                       __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
-        // Row filter, a superset of what the exact rule (key <= the row's
-        // current last entry tk) can admit: key' = |y|^2 - 2 x.y (EUCLIDEAN)
-        // or -x.y (COSINE) against thr = tk - |x|^2 (or tk - 1) widened by
-        // 2^-21 (|tk| + |x|^2 + max|y|^2), which bounds the rounding of both
-        // the key and the threshold.  Padding columns have key' = +inf, a row
-        // outside the block thr = -inf, a list with free slots thr = FLT_MAX.
-        const float tk = Lk[r * kLS + kq - 1];
-        float thr;
-        if (r >= mq) thr = -kInf;
-        else if (tk == kInf) thr = kMaxF;
-        else if (METRIC == KNN_METRIC_EUCLIDEAN) {
-          const float myn = qn[r];
-          thr = fminf((tk - myn) + kSlack * (fabsf(tk) + myn + cm), kMaxF);
-        } else {
-          thr = fminf((tk - 1.f) + kSlack * (fabsf(tk) + 2.f), kMaxF);
-        }
-        // bit j of neg = sign of thr - key'_j, shifted in from column 31 down
-        const float4* cn4 = reinterpret_cast<const float4*>(cn + col0);
-        uint32_t neg = 0;
-#pragma unroll
-        for (int q = 7; q >= 0; --q) {
-          const float4 c = cn4[q];
-          const float cc[4] = {c.x, c.y, c.z, c.w};
-#pragma unroll
-          for (int e = 3; e >= 0; --e) {
-            const float dot = __uint_as_float(v[4 * q + e]);
-            const float kp = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, cc[e]) : __fsub_rn(cc[e], dot);
-            neg = __funnelshift_l(__float_as_uint(__fsub_rn(thr, kp)), neg, 1);
-          }
-        }
-        uint32_t mask = ~neg;
-        // the row's own point (its leaf lies inside the block) never survives
-        const int64_t selfbit = (lo + q0 + r) - blo - c0 - col0;
-        if (selfbit >= 0 && selfbit < 32) mask &= ~(1u << (int)selfbit);
-        if (xcl) {
-          // listed ids among these 32 columns: walk the row's sorted
-          // positions (each thread's columns only increase)
-          const int lo_c = c0 + col0;
-          uint32_t ex = 0;
-          int p = xp[r * kXS + xptr];
-          while (p < lo_c + 32) {
-            if (p >= lo_c) ex |= 1u << (p - lo_c);
-            p = xp[r * kXS + (++xptr)];
-          }
-          mask &= ~ex;
-        }
-        msk[r * 2 + half] = mask;
-      }
+      __syncthreads();
+      stage_operand(opB, Xb, Kp, cid);
+      asm volatile("cp.async.wait_all;\n" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       __syncthreads();
-      // one warp per query row with survivors (found by one ballot over the
-      // warp's 16 rows); lane l holds the round's columns l and 32 + l.  The
-      // survivor's exact key is computed here; few survivors are placed one
-      // by one by warp_insert1 (which drops a candidate behind all 32
-      // entries), many (first tree) by one sort and merge.
-      {
-        const int myrow = warp + (kUThreads / 32) * (lane & 15);
-        const bool has = lane < 16 && myrow < mq && (msk[myrow * 2] | msk[myrow * 2 + 1]) != 0;
-        uint32_t rows = __ballot_sync(0xFFFFFFFFu, has);
-        while (rows) {
-          const int qq = warp + (kUThreads / 32) * (__ffs(rows) - 1);
-          rows &= rows - 1;
-          const uint32_t m0 = msk[qq * 2], m1 = msk[qq * 2 + 1];
-          float lk = Lk[qq * kLS + lane];
-          uint32_t li = Li[qq * kLS + lane];
-          const float myn = qn[qq];
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t tmem = *tmem_slot;
+      if (tid == 0) {
+        if (*reinterpret_cast<volatile int*>(err) != 0) {
+          *status = 2;  // another block failed: issue nothing more
+        } else {
+          const uint32_t a0 = smem_u32(opA), b0 = smem_u32(opB);
+          for (int ch = 0; ch < nchunks; ++ch)
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            uint32_t bal = h ? m1 : m0;
-            if (bal == 0) continue;
-            const int col = h * 32 + lane;
-            float ck = kInf;
-            uint32_t ci = kNoId;
-            if ((bal >> lane) & 1u) {
-              const float dot = Ks[qq * kRound + ((((col >> 2) ^ (qq & 7)) << 2) | (col & 3))];
-              ck = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[rb + col]))
-                                                  : __fsub_rn(1.f, dot);
-              ci = (uint32_t)cid[rb + col];
+            for (int kk = 0; kk < kKC / 16; ++kk) {
+              const uint32_t off = ch * kChunkBytes + kk * 32;
+              umma_bf16(tmem, desc_sw128(a0 + off), desc_sw128(b0 + off), (ch | kk) != 0 ? 1u : 0u);
             }
-            if (FIRST && __popc(bal) >= kBulkMerge) {
-              warp_bitonic_sort32(ck, ci);
-              warp_merge_lower(lk, li, ck, ci);
-              continue;
-            }
-            while (bal) {
-              const int src = __ffs(bal) - 1;
-              bal &= bal - 1;
-              const float k1 = __shfl_sync(0xFFFFFFFFu, ck, src);
-              const uint32_t i1 = __shfl_sync(0xFFFFFFFFu, ci, src);
-              const bool dup = !FIRST && !xcl && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
-              if (!dup) warp_insert1(lk, li, k1, i1);
-            }
+          umma_commit(bar);
+          if (!mbar_wait_bounded(bar, phase)) {
+            *status = 1;
+            atomicExch(err, 1);
+            mbar_wait_bounded(bar, phase);  // let the MMAs drain before TMEM is freed
           }
-          Lk[qq * kLS + lane] = lk;
-          Li[qq * kLS + lane] = li;
         }
       }
       __syncthreads();
+      phase ^= 1u;
+      if (*status != 0) break;  // uniform: read after the barrier
+
+      const float cm = fmaxf(fmaxf(cmax[0], cmax[1]), fmaxf(cmax[2], cmax[3]));
+      for (int rb = 0; rb < mc; rb += kRound) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        {
+          const int quarter = warp & 3, half = warp >> 2;
+          const int r = quarter * 32 + lane;
+          const int col0 = rb + half * 32;
+          uint32_t v[32];
+          tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)col0, v);
+          if (FIRST && pass == 0) {
+            // smallest exact key of these 32 columns (the row's own column
+            // left out) into the slice's group
+            const float4* cn4 = reinterpret_cast<const float4*>(cn + col0);
+            const float myn = qn[r];
+            const int64_t sb = (lo + q0 + r) - blo - c0 - col0;
+            float m = kInf;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const float4 c = cn4[q];
+              const float cc[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                const float dot = __uint_as_float(v[4 * q + e]);
+                const float key = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cc[e]))
+                                                                 : __fsub_rn(1.f + cc[e], dot);
+                m = (sb == 4 * q + e) ? m : fminf(m, key);
+              }
+            }
+            const int g = ((c0 / kBN) * 4 + (rb / kRound) * 2 + half) & (kGroups - 1);
+            gm[r * kGS + g] = fminf(gm[r * kGS + g], m);
+          } else {
+            // raw products for the merge: 16-byte chunks xor-swizzled by the row,
+            // so that row-parallel writes and column-parallel reads hit distinct banks
+            float4* ks4 = reinterpret_cast<float4*>(Ks) + r * (kRound / 4);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+              ks4[(half * 8 + q) ^ (r & 7)] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                                                           __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+            // Row filter, a superset of what the exact rule (key <= the row's
+            // current last entry tk) can admit: key' = |y|^2 - 2 x.y (EUCLIDEAN)
+            // or -x.y (COSINE) against thr = tk - |x|^2 (or tk - 1) widened by
+            // 2^-21 (|tk| + |x|^2 + max|y|^2), which bounds the rounding of both
+            // the key and the threshold.  Padding columns have key' = +inf, a row
+            // outside the block thr = -inf, a list with free slots thr = FLT_MAX.
+            const float tk = FIRST ? fminf(Lk[r * kLS + kq - 1], tcap[r]) : Lk[r * kLS + kq - 1];
+            float thr;
+            if (r >= mq) thr = -kInf;
+            else if (tk == kInf) thr = kMaxF;
+            else if (METRIC == KNN_METRIC_EUCLIDEAN) {
+              const float myn = qn[r];
+              thr = fminf((tk - myn) + kSlack * (fabsf(tk) + myn + cm), kMaxF);
+            } else {
+              thr = fminf((tk - 1.f) + kSlack * (fabsf(tk) + 2.f), kMaxF);
+            }
+            // bit j of neg = sign of thr - key'_j, shifted in from column 31 down
+            const float4* cn4 = reinterpret_cast<const float4*>(cn + col0);
+            uint32_t neg = 0;
+#pragma unroll
+            for (int q = 7; q >= 0; --q) {
+              const float4 c = cn4[q];
+              const float cc[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+              for (int e = 3; e >= 0; --e) {
+                const float dot = __uint_as_float(v[4 * q + e]);
+                const float kp = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, cc[e]) : __fsub_rn(cc[e], dot);
+                neg = __funnelshift_l(__float_as_uint(__fsub_rn(thr, kp)), neg, 1);
+              }
+            }
+            uint32_t mask = ~neg;
+            // the row's own point (its leaf lies inside the block) never survives
+            const int64_t selfbit = (lo + q0 + r) - blo - c0 - col0;
+            if (selfbit >= 0 && selfbit < 32) mask &= ~(1u << (int)selfbit);
+            if (xcl) {
+              // listed ids among these 32 columns: walk the row's sorted
+              // positions (each thread's columns only increase)
+              const int lo_c = c0 + col0;
+              uint32_t ex = 0;
+              int p = xp[r * kXS + xptr];
+              while (p < lo_c + 32) {
+                if (p >= lo_c) ex |= 1u << (p - lo_c);
+                p = xp[r * kXS + (++xptr)];
+              }
+              mask &= ~ex;
+            }
+            msk[r * 2 + half] = mask;
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncthreads();
+        if (pass == 1) {
+          // one warp per query row with survivors (found by one ballot over the
+          // warp's 16 rows); lane l holds the round's columns l and 32 + l.  The
+          // survivor's exact key is computed here; few survivors are placed one
+          // by one by warp_insert1 (which drops a candidate behind all 32
+          // entries), many (first tree) by one sort and merge.
+          {
+            const int myrow = warp + (kUThreads / 32) * (lane & 15);
+            const bool has = lane < 16 && myrow < mq && (msk[myrow * 2] | msk[myrow * 2 + 1]) != 0;
+            uint32_t rows = __ballot_sync(0xFFFFFFFFu, has);
+            while (rows) {
+              const int qq = warp + (kUThreads / 32) * (__ffs(rows) - 1);
+              rows &= rows - 1;
+              const uint32_t m0 = msk[qq * 2], m1 = msk[qq * 2 + 1];
+              float lk = Lk[qq * kLS + lane];
+              uint32_t li = Li[qq * kLS + lane];
+              const float myn = qn[qq];
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                uint32_t bal = h ? m1 : m0;
+                if (bal == 0) continue;
+                const int col = h * 32 + lane;
+                float ck = kInf;
+                uint32_t ci = kNoId;
+                if ((bal >> lane) & 1u) {
+                  const float dot = Ks[qq * kRound + ((((col >> 2) ^ (qq & 7)) << 2) | (col & 3))];
+                  ck = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[rb + col]))
+                                                      : __fsub_rn(1.f, dot);
+                  ci = (uint32_t)cid[rb + col];
+                }
+                if (FIRST && __popc(bal) >= kBulkMerge) {
+                  warp_bitonic_sort32(ck, ci);
+                  warp_merge_lower(lk, li, ck, ci);
+                  continue;
+                }
+                while (bal) {
+                  const int src = __ffs(bal) - 1;
+                  bal &= bal - 1;
+                  const float k1 = __shfl_sync(0xFFFFFFFFu, ck, src);
+                  const uint32_t i1 = __shfl_sync(0xFFFFFFFFu, ci, src);
+                  const bool dup = !FIRST && !xcl && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
+                  if (!dup) warp_insert1(lk, li, k1, i1);
+                }
+              }
+              Lk[qq * kLS + lane] = lk;
+              Li[qq * kLS + lane] = li;
+            }
+          }
+          __syncthreads();
+        }
+      }
+    }
+    if (*status != 0) break;
+    if (FIRST && pass == 0) {
+      __syncthreads();
+      // bound per row: the kq-th smallest of its group minima
+      for (int qq = warp; qq < mq; qq += kUThreads / 32) {
+        float a = gm[qq * kGS + lane], b = gm[qq * kGS + 32 + lane];
+        uint32_t ia = lane, ib = 32 + lane;
+        warp_bitonic_sort32(a, ia);
+        warp_bitonic_sort32(b, ib);
+        warp_merge_pair(a, ia, b, ib);
+        const float t = __shfl_sync(0xFFFFFFFFu, a, kq - 1);
+        if (lane == 0) tcap[qq] = t;
+      }
+      __syncthreads();
+      for (int e = tid; e < kBM * kLS; e += kUThreads) {
+        Lk[e] = kInf;
+        Li[e] = kNoId;
+      }
     }
   }
   if (*status == 0) {
@@ -575,10 +640,10 @@ __global__ void __launch_bounds__(256) k_rerank(const float* __restrict__ X, int
 
 size_t umma_smem_bytes(int Kp) {
   // alignment slack + A + B (also the round products) + lists + (qid, cid, qn, cn) + survivor
-  // masks + per-warp norm maxima + listed columns + barrier words
+  // masks + per-warp norm maxima + listed columns + first-tree bounds + barrier words
   const size_t bbytes = std::max((size_t)(Kp / kKC) * kChunkBytes, (size_t)kKsBytes);
   return 1024 + (size_t)(Kp / kKC) * kChunkBytes + bbytes + (size_t)kBM * kLS * 8 +
-         (size_t)(kBM + kBN) * 8 + (size_t)kBM * 2 * 4 + 16 + (size_t)kBM * kXS * 2 + 64;
+         (size_t)(kBM + kBN) * 8 + (size_t)kBM * 2 * 4 + 16 + (size_t)kBM * kXS * 2 + (size_t)kBM * 4 + 64;
 }
 
 int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {

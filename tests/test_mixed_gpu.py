@@ -38,6 +38,8 @@ def lib():
     (9000, 200, 10, 2, 300, 1),     # Kp = 256, three 128-query tiles per leaf
     (5000, 64, 8, 3, 40, 1),        # Kp = 64, short blocks
     (4000, 96, 24, 2, 130, 1),      # kq = 32 for k > 16
+    (20000, 128, 16, 3, 2048, 0),   # first tree with the bounding pass; later trees mask listed ids
+    (24000, 64, 5, 2, 3000, 1),     # bounding pass over more than 64 column slices (groups wrap)
 ])
 def test_mixed_equals_plain_on_exact_integer_data(lib, oracle, n, d, k, trees, leaf, props):
     x = _ints(n, d, n + d)
