@@ -17,15 +17,17 @@
 //   * operands: K-major, 128-byte swizzled shared-memory tiles (8-row atoms of
 //     1024 B), filled by cp.async from the BF16 copy through the tree's order;
 //   * MMA: tcgen05.mma.cta_group::1.kind::f16, M=128 N=128 K=16, issued by one
-//     thread, accumulator 128 lanes x 128 columns of tensor memory;
+//     thread, accumulator 128 lanes x 128 columns of tensor memory, two
+//     accumulators so that one tile's MMA overlaps the previous tile's rounds;
 //   * completion: tcgen05.commit -> mbarrier, waited with an iteration limit
 //     (on expiry the block records an error, drains, frees TMEM and returns);
 //   * epilogue: per 64-column round, tcgen05.ld 32x32b.x32 by all 8 warps (warp
 //     w reads lane quarter w%4, 32 columns); three instructions per key filter
 //     it against a slightly widened bound of the row's current last entry into
-//     a survivor bit mask, then one warp per row computes its few survivors'
-//     keys and inserts them into that query's sorted list (held in shared
-//     memory for the whole block) with one ballot and one lane shift each.
+//     a survivor bit mask, then the warps of each lane quarter read their
+//     rows' few survivors back from tensor memory, compute their exact keys
+//     and insert them into the query's sorted list (held in shared memory for
+//     the whole block) with one ballot and one lane shift each.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -40,7 +42,7 @@ constexpr int kBM = 128;
 constexpr int kBN = 128;
 constexpr int kKC = 64;               // bf16 per 128-byte swizzled row
 constexpr int kChunkBytes = kBM * 128; // one 128 x 64 bf16 operand chunk
-constexpr uint32_t kTmemCols = 128;
+constexpr uint32_t kTmemCols = 256;  // two 128-column accumulators
 constexpr int kUThreads = 256;
 constexpr int kRound = 64;          // tile columns per epilogue round
 constexpr int kBulkMerge = 12;      // first tree: survivors in a half round from which sort + merge pays
@@ -55,9 +57,6 @@ constexpr int kXMaxBlock = 65000;
 constexpr int kPrepassMin = 1024;
 constexpr int kGroups = 64;
 constexpr int kGS = kGroups + 1;
-// Round products live in the B-operand region once the tile's MMA has completed:
-// 128 rows x 64 floats (32 KB).
-constexpr int kKsBytes = kBM * kRound * 4;
 constexpr int kLS = 33;              // list row stride (row owners hit distinct banks)
 // A 128x128x256 tile finishes in about a microsecond; 2^16 polls with 32 ns
 // sleeps (a few ms) is far beyond that, and keeps a failing launch short.
@@ -137,6 +136,13 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
                : "memory");
 }
 
+__device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
+  uint32_t v;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(v) : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+  return v;
+}
+
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -186,17 +192,30 @@ __device__ __forceinline__ uint32_t warp_sort32_u32(uint32_t v) {
   return v;
 }
 
-// One block per (leaf, 128-query tile).  The 128 queries' lists stay in shared
-// memory for the whole loop over candidate tiles (read once, written once);
-// each 128x128 tensor-core tile is emptied in two 64-column rounds: epilogue
-// (tcgen05.ld, a conservative per-row filter packed into survivor bit masks,
-// raw products parked in shared memory) then a per-row merge that computes the
-// survivors' keys and applies the exact rule.  Prologue, MMA issue, bounded
-// wait and the tensor-memory loads follow the single-tile sequence that was
-// checked on its own against a CPU product.
+// One block per (leaf, 128-query tile), stepping over the block's 128-column
+// candidate tiles.  The 128 queries' lists stay in shared memory for the whole
+// block (read once, written once).  Each step empties one 128x128 tensor-core
+// tile (tensor memory, two 128-column buffers) in two 64-column rounds:
+//   * epilogue: thread (row, 32-column half) loads its products
+//     (tcgen05.ld 32x32b.x32), filters them against a conservative bound of
+//     the row's list tail into a survivor bit mask (three instructions per
+//     key), drops the row's own column and listed ids;
+//   * merge: the warps of the rows' lane quarter insert each row's survivors,
+//     reading their products back from tensor memory (tcgen05.ld x1 per
+//     survivor, or x32 and a lane transpose for a bulk batch), computing the
+//     exact keys and applying the exact (key, id) rule.
+// The next step's operand is staged while round 0 runs (its MMA has
+// completed), and its MMA runs into the other tensor-memory buffer during
+// round 1.  MMA issue, bounded waits and the tensor-memory loads follow the
+// single-tile sequence that was checked on its own against a CPU product.
 // FIRST: the launch of the first tree, whose lists start empty; a point then
 // meets every candidate once, so no survivor can already be listed, and a
 // half round with many survivors is sorted and merged into the list in one go.
+// Blocks of kPrepassMin columns or more first run all tiles once (pass 0) to
+// record each row's smallest exact key in each of kGroups column groups
+// (32-column slices, wrapping); the kq-th smallest group minimum is the key of
+// kq distinct candidates, so it bounds the kq-th key of the final list, and
+// pass 1 filters against it from its first tile on.
 // Later trees, with inv (the tree's inverse order): the block's columns that
 // hold an id already in the row's list are found up front (inv of each listed
 // id) and masked out of the survivors, so the merge needs no duplicate check;
@@ -214,18 +233,16 @@ __global__ void __launch_bounds__(kUThreads, 2)
   const int nchunks = Kp / kKC;
   unsigned char* opA = smem;
   unsigned char* opB = opA + nchunks * kChunkBytes;
-  const int bbytes = max(nchunks * kChunkBytes, kKsBytes);
-  float* Ks = reinterpret_cast<float*>(opB);                           // round products (reuses B)
-  float* Lk = reinterpret_cast<float*>(opB + bbytes);                  // [128][kLS] list keys
+  float* Lk = reinterpret_cast<float*>(opB + nchunks * kChunkBytes);  // [128][kLS] list keys
   uint32_t* Li = reinterpret_cast<uint32_t*>(Lk + kBM * kLS);         // [128][kLS] list ids
   int32_t* qid = reinterpret_cast<int32_t*>(Li + kBM * kLS);
-  int32_t* cid = qid + kBM;
-  float* qn = reinterpret_cast<float*>(cid + kBN);
-  float* cn = qn + kBM;  // candidate norms (EUCLIDEAN) or 0; +inf for padding columns
-  uint32_t* msk = reinterpret_cast<uint32_t*>(cn + kBN);  // [128][2] survivor bits of the round
-  float* cmax = reinterpret_cast<float*>(msk + kBM * 2);  // [4] largest candidate norm per warp
-  uint16_t* xp = reinterpret_cast<uint16_t*>(cmax + 4);   // [128][kXS] listed columns
-  float* tcap = reinterpret_cast<float*>(xp + kBM * kXS);  // [128] first tree: bound on the kq-th key
+  float* qn = reinterpret_cast<float*>(qid + kBM);
+  int32_t* cid2 = reinterpret_cast<int32_t*>(qn + kBM);  // [2][128] candidate ids per step parity
+  float* cn2 = reinterpret_cast<float*>(cid2 + 2 * kBN);  // [2][128] norms (EUCLIDEAN) or 0; +inf: padding
+  uint32_t* msk = reinterpret_cast<uint32_t*>(cn2 + 2 * kBN);  // [128][2] survivor bits of the round
+  float* cmax2 = reinterpret_cast<float*>(msk + kBM * 2);      // [2][4] largest candidate norm per warp
+  uint16_t* xp = reinterpret_cast<uint16_t*>(cmax2 + 8);       // [128][kXS] listed columns
+  float* tcap = reinterpret_cast<float*>(xp + kBM * kXS);      // [128] first tree: bound on the kq-th key
   uint64_t* mbar = reinterpret_cast<uint64_t*>(tcap + kBM);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
   int* status = reinterpret_cast<int*>(tmem_slot + 1);
@@ -250,10 +267,14 @@ __global__ void __launch_bounds__(kUThreads, 2)
   if (q0 >= nq) return;  // whole block, before any barrier or allocation
   const int mq = min(kBM, nq - q0);
   const int nb = (int)(bhi - blo);
+  const int ntiles = (nb + kBN - 1) / kBN;
   const bool xcl = !FIRST && inv != nullptr && nb <= kXMaxBlock;  // block-uniform
+  const bool pre = FIRST && nb >= kPrepassMin;
+  const int nsteps = pre ? 2 * ntiles : ntiles;
   const float kInf = __int_as_float(0x7F800000);
   const float kMaxF = __int_as_float(0x7F7FFFFF);
   const uint32_t bar = smem_u32(mbar);
+  float* gm = Lk;  // [128][kGS] group minima during pass 0 (spans Lk and Li)
 
   if (warp == 0) {
     if (lane == 0) {
@@ -270,112 +291,136 @@ __global__ void __launch_bounds__(kUThreads, 2)
     const int32_t id = tid < mq ? perm[lo + q0 + tid] : -1;
     qid[tid] = id;
     qn[tid] = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
+    tcap[tid] = kInf;
   }
-  // First tree, blocks of kPrepassMin columns or more: pass 0 runs the tiles
-  // once to record each row's smallest exact key in each of kGroups groups of
-  // columns (32-column slices, wrapping).  The kq-th smallest group minimum is
-  // the key of kq distinct candidates, so it bounds the kq-th key of the
-  // final list; pass 1 filters against it from the first tile on, which
-  // leaves a few dozen survivors per row instead of ~kq ln(columns / kq).
-  const bool pre = FIRST && nb >= kPrepassMin;
-  float* gm = Lk;  // [128][kGS] group minima during pass 0 (spans Lk and Li)
-  if (tid < kBM) tcap[tid] = kInf;
+  // candidates of step s (warps 0-3, whole warps) into parity slot s & 1
+  auto load_cols = [&](int s) {
+    const int c0 = (s % ntiles) * kBN, mc = min(kBN, nb - c0);
+    const int32_t id = tid < mc ? perm[blo + c0 + tid] : -1;
+    cid2[(s & 1) * kBN + tid] = id;
+    const float nv = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
+    cn2[(s & 1) * kBN + tid] = id >= 0 ? nv : kInf;
+    // norms are >= 0, so their bit patterns order as unsigned integers
+    const uint32_t wm = __reduce_max_sync(0xFFFFFFFFu, __float_as_uint(nv));
+    if (lane == 0) cmax2[(s & 1) * 4 + warp] = __uint_as_float(wm);
+  };
+  if (tid < kBN) load_cols(0);
   __syncthreads();
+  stage_operand(opA, Xb, Kp, qid);
+  stage_operand(opB, Xb, Kp, cid2);
   if (pre) {
     for (int e = tid; e < kBM * kGS; e += kUThreads) gm[e] = kInf;
   } else {
-    for (int e = tid; e < kBM * 32; e += kUThreads) {
-      const int r = e >> 5, s = e & 31;
-      const int32_t id = qid[r];
-      const bool live = id >= 0 && s < kq;
-      Lk[r * kLS + s] = live ? akey[(size_t)id * kq + s] : kInf;
-      Li[r * kLS + s] = live ? aid[(size_t)id * kq + s] : kNoId;
-    }
-  }
-  stage_operand(opA, Xb, Kp, qid);
-  if (xcl) {
-    // warp w: rows w, w + 8, ...; lane s: the row's s-th listed id
-    uint32_t pos[kBM / 8];
+    // warp w: rows w + 8 i, lane s: entry s; all loads issued before use
+    float lkr[kBM / 8];
+    uint32_t lir[kBM / 8];
 #pragma unroll
     for (int i = 0; i < kBM / 8; ++i) {
       const int32_t id = qid[warp + 8 * i];
-      pos[i] = (id >= 0 && lane < kq) ? aid[(size_t)id * kq + lane] : kNoId;
+      const bool live = id >= 0 && lane < kq;
+      lkr[i] = live ? akey[(size_t)id * kq + lane] : kInf;
+      lir[i] = live ? aid[(size_t)id * kq + lane] : kNoId;
     }
 #pragma unroll
     for (int i = 0; i < kBM / 8; ++i) {
-      uint32_t p = kXEnd;
-      if (pos[i] != kNoId) {
-        const int64_t q = (int64_t)inv[pos[i]] - blo;
-        if (q >= 0 && q < nb) p = (uint32_t)q;
+      Lk[(warp + 8 * i) * kLS + lane] = lkr[i];
+      Li[(warp + 8 * i) * kLS + lane] = lir[i];
+    }
+    if (xcl) {
+      // the listed ids' columns in this block, sorted per row (the 16
+      // rows' bitonic networks interleaved stage by stage)
+      uint32_t pos[kBM / 8];
+#pragma unroll
+      for (int i = 0; i < kBM / 8; ++i) {
+        uint32_t p = kXEnd;
+        if (lir[i] != kNoId) {
+          const int64_t q = (int64_t)inv[lir[i]] - blo;
+          if (q >= 0 && q < nb) p = (uint32_t)q;
+        }
+        pos[i] = p;
       }
-      pos[i] = p;
-    }
 #pragma unroll
-    for (int i = 0; i < kBM / 8; ++i) {
-      const uint32_t v = warp_sort32_u32(pos[i]);
-      xp[(warp + 8 * i) * kXS + lane] = (uint16_t)v;
-      if (lane == 0) xp[(warp + 8 * i) * kXS + 32] = (uint16_t)kXEnd;
+      for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (int m = size >> 1; m >= 1; m >>= 1) {
+          const bool keep_min = ((lane & size) == 0) == ((lane & m) == 0);
+#pragma unroll
+          for (int i = 0; i < kBM / 8; ++i) {
+            const uint32_t o = __shfl_xor_sync(0xFFFFFFFFu, pos[i], m);
+            pos[i] = keep_min ? min(pos[i], o) : max(pos[i], o);
+          }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < kBM / 8; ++i) {
+        xp[(warp + 8 * i) * kXS + lane] = (uint16_t)pos[i];
+        if (lane == 0) xp[(warp + 8 * i) * kXS + 32] = (uint16_t)kXEnd;
+      }
     }
   }
   int xptr = 0;  // this thread's next entry of its row's listed columns
 
-  uint32_t phase = 0;
-  for (int pass = pre ? 0 : 1; pass < 2; ++pass) {
-    for (int c0 = 0; c0 < nb; c0 += kBN) {
-      const int mc = min(kBN, nb - c0);
-      if (tid < kBN) {  // warps 0-3, whole warps
-        const int32_t id = tid < mc ? perm[blo + c0 + tid] : -1;
-        cid[tid] = id;
-        const float nv = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
-        cn[tid] = id >= 0 ? nv : kInf;
-        // norms are >= 0, so their bit patterns order as unsigned integers
-        const uint32_t wm = __reduce_max_sync(0xFFFFFFFFu, __float_as_uint(nv));
-        if (lane == 0) cmax[warp] = __uint_as_float(wm);
-      }
-      __syncthreads();
-      stage_operand(opB, Xb, Kp, cid);
-      asm volatile("cp.async.wait_all;\n" ::: "memory");
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      __syncthreads();
-      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const uint32_t tmem = *tmem_slot;
-      if (tid == 0) {
-        if (*reinterpret_cast<volatile int*>(err) != 0) {
-          *status = 2;  // another block failed: issue nothing more
-        } else {
-          const uint32_t a0 = smem_u32(opA), b0 = smem_u32(opB);
-          for (int ch = 0; ch < nchunks; ++ch)
+  // step 0's MMA
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  auto issue_mma = [&](int s) {  // thread 0: operands staged, previous MMA waited for
+    if (*reinterpret_cast<volatile int*>(err) != 0) {
+      *status = 2;  // another block failed: issue nothing more
+      return;
+    }
+    const uint32_t a0 = smem_u32(opA), b0 = smem_u32(opB);
+    const uint32_t d = tmem + (uint32_t)((s & 1) * kBN);
+    for (int ch = 0; ch < nchunks; ++ch)
 #pragma unroll
-            for (int kk = 0; kk < kKC / 16; ++kk) {
-              const uint32_t off = ch * kChunkBytes + kk * 32;
-              umma_bf16(tmem, desc_sw128(a0 + off), desc_sw128(b0 + off), (ch | kk) != 0 ? 1u : 0u);
-            }
-          umma_commit(bar);
-          if (!mbar_wait_bounded(bar, phase)) {
-            *status = 1;
-            atomicExch(err, 1);
-            mbar_wait_bounded(bar, phase);  // let the MMAs drain before TMEM is freed
-          }
-        }
+      for (int kk = 0; kk < kKC / 16; ++kk) {
+        const uint32_t off = ch * kChunkBytes + kk * 32;
+        umma_bf16(d, desc_sw128(a0 + off), desc_sw128(b0 + off), (ch | kk) != 0 ? 1u : 0u);
       }
-      __syncthreads();
-      phase ^= 1u;
-      if (*status != 0) break;  // uniform: read after the barrier
+    umma_commit(bar);
+  };
+  if (tid == 0) issue_mma(0);
 
-      const float cm = fmaxf(fmaxf(cmax[0], cmax[1]), fmaxf(cmax[2], cmax[3]));
-      for (int rb = 0; rb < mc; rb += kRound) {
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  uint32_t phase = 0;
+  for (int s = 0; s < nsteps; ++s) {
+    const int pass = pre && s < ntiles ? 0 : 1;
+    const int c0 = (s % ntiles) * kBN, mc = min(kBN, nb - c0);
+    const bool has_next = s + 1 < nsteps;
+    if (has_next && tid < kBN) load_cols(s + 1);
+    if (tid == 0 && *status == 0 && !mbar_wait_bounded(bar, phase)) {
+      *status = 1;
+      atomicExch(err, 1);
+      mbar_wait_bounded(bar, phase);  // let the MMAs drain before TMEM is freed
+    }
+    phase ^= 1u;
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (*status != 0) break;  // uniform: read after the barrier
+    // step s's MMA has completed: B is free for step s + 1
+    if (has_next) stage_operand(opB, Xb, Kp, cid2 + ((s + 1) & 1) * kBN);
+    const int32_t* cid = cid2 + (s & 1) * kBN;
+    const float* cn = cn2 + (s & 1) * kBN;
+    const float* cmx = cmax2 + (s & 1) * 4;
+    const float cm = fmaxf(fmaxf(cmx[0], cmx[1]), fmaxf(cmx[2], cmx[3]));
+    const uint32_t tbuf = tmem + (uint32_t)((s & 1) * kBN);
+    const int quarter = warp & 3, half = warp >> 2;
+    const uint32_t tq = tbuf + ((uint32_t)(quarter * 32) << 16);  // this warp's lane quarter
+
+    for (int ri = 0; ri < 2; ++ri) {
+      const int rb = ri * kRound;
+      if (rb < mc) {
         {
-          const int quarter = warp & 3, half = warp >> 2;
           const int r = quarter * 32 + lane;
           const int col0 = rb + half * 32;
           uint32_t v[32];
-          tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)col0, v);
+          tmem_ld32(tq + (uint32_t)col0, v);
+          const float4* cn4 = reinterpret_cast<const float4*>(cn + col0);
           if (FIRST && pass == 0) {
             // smallest exact key of these 32 columns (the row's own column
             // left out) into the slice's group
-            const float4* cn4 = reinterpret_cast<const float4*>(cn + col0);
             const float myn = qn[r];
             const int64_t sb = (lo + q0 + r) - blo - c0 - col0;
             float m = kInf;
@@ -391,22 +436,16 @@ __global__ void __launch_bounds__(kUThreads, 2)
                 m = (sb == 4 * q + e) ? m : fminf(m, key);
               }
             }
-            const int g = ((c0 / kBN) * 4 + (rb / kRound) * 2 + half) & (kGroups - 1);
+            const int g = ((c0 / kBN) * 4 + ri * 2 + half) & (kGroups - 1);
             gm[r * kGS + g] = fminf(gm[r * kGS + g], m);
           } else {
-            // raw products for the merge: 16-byte chunks xor-swizzled by the row,
-            // so that row-parallel writes and column-parallel reads hit distinct banks
-            float4* ks4 = reinterpret_cast<float4*>(Ks) + r * (kRound / 4);
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-              ks4[(half * 8 + q) ^ (r & 7)] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
-                                                           __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
             // Row filter, a superset of what the exact rule (key <= the row's
-            // current last entry tk) can admit: key' = |y|^2 - 2 x.y (EUCLIDEAN)
-            // or -x.y (COSINE) against thr = tk - |x|^2 (or tk - 1) widened by
-            // 2^-21 (|tk| + |x|^2 + max|y|^2), which bounds the rounding of both
-            // the key and the threshold.  Padding columns have key' = +inf, a row
-            // outside the block thr = -inf, a list with free slots thr = FLT_MAX.
+            // list tail tk) can admit: key' = |y|^2 - 2 x.y (EUCLIDEAN) or
+            // -x.y (COSINE) against thr = tk - |x|^2 (or tk - 1) widened by
+            // 2^-21 (|tk| + |x|^2 + max|y|^2), which bounds the rounding of
+            // both the key and the threshold.  Padding columns have key' =
+            // +inf, a row outside the block thr = -inf, a list with free slots
+            // thr = FLT_MAX.
             const float tk = FIRST ? fminf(Lk[r * kLS + kq - 1], tcap[r]) : Lk[r * kLS + kq - 1];
             float thr;
             if (r >= mq) thr = -kInf;
@@ -418,7 +457,6 @@ __global__ void __launch_bounds__(kUThreads, 2)
               thr = fminf((tk - 1.f) + kSlack * (fabsf(tk) + 2.f), kMaxF);
             }
             // bit j of neg = sign of thr - key'_j, shifted in from column 31 down
-            const float4* cn4 = reinterpret_cast<const float4*>(cn + col0);
             uint32_t neg = 0;
 #pragma unroll
             for (int q = 7; q >= 0; --q) {
@@ -427,7 +465,8 @@ __global__ void __launch_bounds__(kUThreads, 2)
 #pragma unroll
               for (int e = 3; e >= 0; --e) {
                 const float dot = __uint_as_float(v[4 * q + e]);
-                const float kp = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, cc[e]) : __fsub_rn(cc[e], dot);
+                const float kp =
+                    METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, cc[e]) : __fsub_rn(cc[e], dot);
                 neg = __funnelshift_l(__float_as_uint(__fsub_rn(thr, kp)), neg, 1);
               }
             }
@@ -452,62 +491,80 @@ __global__ void __launch_bounds__(kUThreads, 2)
         }
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
         __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         if (pass == 1) {
-          // one warp per query row with survivors (found by one ballot over the
-          // warp's 16 rows); lane l holds the round's columns l and 32 + l.  The
-          // survivor's exact key is computed here; few survivors are placed one
-          // by one by warp_insert1 (which drops a candidate behind all 32
-          // entries), many (first tree) by one sort and merge.
-          {
-            const int myrow = warp + (kUThreads / 32) * (lane & 15);
-            const bool has = lane < 16 && myrow < mq && (msk[myrow * 2] | msk[myrow * 2 + 1]) != 0;
-            uint32_t rows = __ballot_sync(0xFFFFFFFFu, has);
-            while (rows) {
-              const int qq = warp + (kUThreads / 32) * (__ffs(rows) - 1);
-              rows &= rows - 1;
-              const uint32_t m0 = msk[qq * 2], m1 = msk[qq * 2 + 1];
-              float lk = Lk[qq * kLS + lane];
-              uint32_t li = Li[qq * kLS + lane];
-              const float myn = qn[qq];
+          // Warp (quarter, half) takes the quarter's rows of parity half
+          // (found by one ballot); survivors' products come from this warp's
+          // lane quarter of tensor memory.
+          const int myrow = quarter * 32 + half + 2 * (lane & 15);
+          const bool has = lane < 16 && myrow < mq && (msk[myrow * 2] | msk[myrow * 2 + 1]) != 0;
+          uint32_t rows = __ballot_sync(0xFFFFFFFFu, has);
+          while (rows) {
+            const int ql = half + 2 * (__ffs(rows) - 1);  // row within the quarter
+            const int qq = quarter * 32 + ql;
+            rows &= rows - 1;
+            const uint32_t m0 = msk[qq * 2], m1 = msk[qq * 2 + 1];
+            float lk = Lk[qq * kLS + lane];
+            uint32_t li = Li[qq * kLS + lane];
+            const float myn = qn[qq];
 #pragma unroll
-              for (int h = 0; h < 2; ++h) {
-                uint32_t bal = h ? m1 : m0;
-                if (bal == 0) continue;
-                const int col = h * 32 + lane;
+            for (int h = 0; h < 2; ++h) {
+              uint32_t bal = h ? m1 : m0;
+              if (bal == 0) continue;
+              const int cb = rb + h * 32;  // the half's first column in the tile
+              if (FIRST && __popc(bal) >= kBulkMerge) {
+                // lane j <- product of column cb + j of row qq
+                uint32_t v[32];
+                tmem_ld32(tq + (uint32_t)cb, v);
+                float dot = 0.f;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                  const float t = __shfl_sync(0xFFFFFFFFu, __uint_as_float(v[j]), ql);
+                  if (lane == j) dot = t;
+                }
                 float ck = kInf;
                 uint32_t ci = kNoId;
                 if ((bal >> lane) & 1u) {
-                  const float dot = Ks[qq * kRound + ((((col >> 2) ^ (qq & 7)) << 2) | (col & 3))];
-                  ck = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[rb + col]))
+                  ck = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[cb + lane]))
                                                       : __fsub_rn(1.f, dot);
-                  ci = (uint32_t)cid[rb + col];
+                  ci = (uint32_t)cid[cb + lane];
                 }
-                if (FIRST && __popc(bal) >= kBulkMerge) {
-                  warp_bitonic_sort32(ck, ci);
-                  warp_merge_lower(lk, li, ck, ci);
-                  continue;
-                }
-                while (bal) {
-                  const int src = __ffs(bal) - 1;
-                  bal &= bal - 1;
-                  const float k1 = __shfl_sync(0xFFFFFFFFu, ck, src);
-                  const uint32_t i1 = __shfl_sync(0xFFFFFFFFu, ci, src);
-                  const bool dup = !FIRST && !xcl && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
-                  if (!dup) warp_insert1(lk, li, k1, i1);
-                }
+                warp_bitonic_sort32(ck, ci);
+                warp_merge_lower(lk, li, ck, ci);
+                continue;
               }
-              Lk[qq * kLS + lane] = lk;
-              Li[qq * kLS + lane] = li;
+              while (bal) {
+                const int j = __ffs(bal) - 1;
+                bal &= bal - 1;
+                const float dot = __shfl_sync(0xFFFFFFFFu, __uint_as_float(tmem_ld1(tq + (uint32_t)(cb + j))), ql);
+                const float k1 = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[cb + j]))
+                                                                : __fsub_rn(1.f, dot);
+                const uint32_t i1 = (uint32_t)cid[cb + j];
+                const bool dup = !FIRST && !xcl && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
+                if (!dup) warp_insert1(lk, li, k1, i1);
+              }
             }
+            Lk[qq * kLS + lane] = lk;
+            Li[qq * kLS + lane] = li;
           }
+          asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
           __syncthreads();
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         }
       }
+      if (ri == 0 && has_next) {
+        // step s + 1's operand has landed: its MMA runs during round 1
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        if (tid == 0) issue_mma(s + 1);
+      }
     }
-    if (*status != 0) break;
-    if (FIRST && pass == 0) {
-      __syncthreads();
-      // bound per row: the kq-th smallest of its group minima
+    if (FIRST && pass == 0 && s == ntiles - 1) {
+      // bound per row: the kq-th smallest of its group minima; then the
+      // lists start empty for pass 1
       for (int qq = warp; qq < mq; qq += kUThreads / 32) {
         float a = gm[qq * kGS + lane], b = gm[qq * kGS + 32 + lane];
         uint32_t ia = lane, ib = 32 + lane;
@@ -639,11 +696,10 @@ __global__ void __launch_bounds__(256) k_rerank(const float* __restrict__ X, int
 }
 
 size_t umma_smem_bytes(int Kp) {
-  // alignment slack + A + B (also the round products) + lists + (qid, cid, qn, cn) + survivor
-  // masks + per-warp norm maxima + listed columns + first-tree bounds + barrier words
-  const size_t bbytes = std::max((size_t)(Kp / kKC) * kChunkBytes, (size_t)kKsBytes);
-  return 1024 + (size_t)(Kp / kKC) * kChunkBytes + bbytes + (size_t)kBM * kLS * 8 +
-         (size_t)(kBM + kBN) * 8 + (size_t)kBM * 2 * 4 + 16 + (size_t)kBM * kXS * 2 + (size_t)kBM * 4 + 64;
+  // alignment slack + A + B + lists + (qid, qn) + two steps' (cid, cn) + survivor masks + two
+  // steps' norm maxima + listed columns + first-tree bounds + barrier words
+  return 1024 + 2 * (size_t)(Kp / kKC) * kChunkBytes + (size_t)kBM * kLS * 8 + (size_t)kBM * 8 +
+         (size_t)kBN * 16 + (size_t)kBM * 2 * 4 + 32 + (size_t)kBM * kXS * 2 + (size_t)kBM * 4 + 64;
 }
 
 int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
