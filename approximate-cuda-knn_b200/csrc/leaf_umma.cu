@@ -563,16 +563,49 @@ __global__ void __launch_bounds__(kUThreads, 2)
       }
     }
     if (FIRST && pass == 0 && s == ntiles - 1) {
-      // bound per row: the kq-th smallest of its group minima; then the
-      // lists start empty for pass 1
-      for (int qq = warp; qq < mq; qq += kUThreads / 32) {
-        float a = gm[qq * kGS + lane], b = gm[qq * kGS + 32 + lane];
-        uint32_t ia = lane, ib = 32 + lane;
-        warp_bitonic_sort32(a, ia);
-        warp_bitonic_sort32(b, ib);
-        warp_merge_pair(a, ia, b, ib);
-        const float t = __shfl_sync(0xFFFFFFFFu, a, kq - 1);
-        if (lane == 0) tcap[qq] = t;
+      // bound per row: the kq-th smallest of its group minima (warp w: rows
+      // w + 8 i, four rows' networks interleaved).  Each row's 64 minima:
+      // lanes' first halves sorted ascending, second halves descending, their
+      // lane-wise minima are the 32 smallest (a bitonic sequence), merged.
+      // Then the lists start empty for pass 1.
+      for (int i0 = 0; i0 < kBM / 8; i0 += 4) {
+        float a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int qq = warp + 8 * (i0 + i);
+          a[i] = gm[qq * kGS + lane];
+          b[i] = gm[qq * kGS + 32 + lane];
+        }
+#pragma unroll
+        for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+          for (int m = size >> 1; m >= 1; m >>= 1) {
+            const bool keep_min = ((lane & size) == 0) == ((lane & m) == 0);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              const float oa = __shfl_xor_sync(0xFFFFFFFFu, a[i], m);
+              const float ob = __shfl_xor_sync(0xFFFFFFFFu, b[i], m);
+              a[i] = keep_min ? fminf(a[i], oa) : fmaxf(a[i], oa);
+              b[i] = keep_min ? fmaxf(b[i], ob) : fminf(b[i], ob);
+            }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = fminf(a[i], b[i]);
+#pragma unroll
+        for (int m = 16; m >= 1; m >>= 1) {
+          const bool keep_min = (lane & m) == 0;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float o = __shfl_xor_sync(0xFFFFFFFFu, a[i], m);
+            a[i] = keep_min ? fminf(a[i], o) : fmaxf(a[i], o);
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const float t = __shfl_sync(0xFFFFFFFFu, a[i], kq - 1);
+          if (lane == 0) tcap[warp + 8 * (i0 + i)] = t;
+        }
       }
       __syncthreads();
       for (int e = tid; e < kBM * kLS; e += kUThreads) {
