@@ -96,7 +96,7 @@ class KnnStats(ctypes.Structure):
         ("ms_learn", ctypes.c_float),
         ("leaf_tile", ctypes.c_int32),
         ("prop_warps", ctypes.c_int32),
-        ("reserved_pad", ctypes.c_int32),
+        ("ms_leaf_tiles", ctypes.c_float),
         ("reserved", ctypes.c_int64 * 6),
     ]
 
@@ -106,6 +106,7 @@ class KnnStats(ctypes.Structure):
             "depth": self.depth, "ms_total": self.ms_total, "ms_upload": self.ms_upload,
             "ms_learn": self.ms_learn, "ms_trees": self.ms_trees, "ms_leaf": self.ms_leaf,
             "ms_propagate": self.ms_propagate, "ms_download": self.ms_download,
+            "ms_leaf_tiles": self.ms_leaf_tiles,
             "launches": self.launches, "leaf_pairs": self.leaf_pairs,
             "leaf_tile": self.leaf_tile, "prop_warps": self.prop_warps,
             "prop_candidates": [self.prop_candidates[i] for i in range(n)],

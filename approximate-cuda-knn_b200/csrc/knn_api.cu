@@ -76,6 +76,16 @@ struct knn_context {
   // Autotuned launch shapes by workload key: (FP32 leaf tile, propagation warps).
   std::map<std::string, std::pair<int, int>> tuned;
   cudaEvent_t tev[2] = {};
+  // Events around each tree's leaf-tile kernel (statistics only), grown on demand.
+  std::vector<cudaEvent_t> kev;
+  cudaEvent_t* kernel_events(int trees) {
+    while ((int)kev.size() < 2 * trees) {
+      cudaEvent_t e = nullptr;
+      if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+      kev.push_back(e);
+    }
+    return kev.data();
+  }
 
   // Device buffer `name` of at least `bytes`; grows by reallocation.
   int get(const char* name, size_t bytes, void** out) {
@@ -120,6 +130,8 @@ struct knn_context {
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     for (auto& e : tev)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : kev)
       if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
     if (cur != device) cudaSetDevice(cur);
@@ -352,7 +364,8 @@ Layout single_layout(int64_t n, int depth) {
 
 int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, int trees,
              const Layout& lay, int metric, const int32_t* perm, const float* norms, Lists* L,
-             unsigned long long* counter, cudaStream_t st, knn::LaunchLog& log, int tile = 0) {
+             unsigned long long* counter, cudaStream_t st, knn::LaunchLog& log, int tile = 0,
+             cudaEvent_t* kev = nullptr) {
   const int kw = (k + 31) / 32;
   knn::launch_init_lists(L->key[L->cur], L->id[L->cur], L->flags[L->cur], n, k, kw, st);
   log.add(2);
@@ -372,6 +385,7 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
   a.rid = L->id[L->cur];
   a.pair_counter = counter;
   a.tile = tile;
+  a.kev = kev;
   a.ftable = lay.ftable;
   a.foff = lay.foff;
   a.fcount = lay.fcount;
@@ -386,7 +400,7 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
 // approximate candidates over all trees; FP32 re-rank keeps the exact best k.
 int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, int trees,
                   const Layout& lay, int metric, const int32_t* perm, const float* norms, Lists* L,
-                  int* err_flag, cudaStream_t st, knn::LaunchLog& log) {
+                  int* err_flag, cudaStream_t st, knn::LaunchLog& log, cudaEvent_t* kev = nullptr) {
   const int kw = (k + 31) / 32;
   const int kq = k <= 16 ? 2 * k : 32;
   const int Kp = ((d + 63) / 64) * 64;
@@ -409,6 +423,7 @@ int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, in
   a.norms = norms;
   a.err = err_flag;
   a.stream = st;
+  a.kev = kev;
   a.rkey = L->key[L->cur];
   a.rid = L->id[L->cur];
   int rc = C->get("Xb", (size_t)n * Kp * 2, &a.Xb);
@@ -778,11 +793,16 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
   rc = pick_shapes(C, o, cs == cudaStreamCaptureStatusNone, !tensor_leaf, props, P.X, n, d, P.dpad, k, lay,
                    metric, T.perm, norms, &L, st, &sh, &tune_prop);
   if (rc) return rc;
+  cudaEvent_t* kev = nullptr;  // per-tree tile-kernel events for the statistics
+  if (timed && cs == cudaStreamCaptureStatusNone) {
+    kev = C->kernel_events(trees);
+    if (!kev) return fail_cuda(cudaGetLastError(), "event creation");
+  }
   if (tensor_leaf) {
-    rc = run_leaf_umma(C, P.X, n, d, P.dpad, k, trees, lay, metric, T.perm, norms, &L, err_flag, st, log);
+    rc = run_leaf_umma(C, P.X, n, d, P.dpad, k, trees, lay, metric, T.perm, norms, &L, err_flag, st, log, kev);
   } else {
     rc = run_leaf(C, P.X, n, d, P.dpad, k, trees, lay, metric, T.perm, norms, &L, stats ? counters : nullptr, st,
-                  log, sh.leaf_tile);
+                  log, sh.leaf_tile, kev);
   }
   if (rc) return rc;
   if (tune_prop) {
@@ -848,6 +868,14 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
     stats->ms_propagate = ms;
     KNN_CK(cudaEventElapsedTime(&ms, C->ev[4], C->ev[5]));
     stats->ms_download = ms;
+    if (kev) {
+      float sum = 0;
+      for (int t = 0; t < trees; ++t) {
+        KNN_CK(cudaEventElapsedTime(&ms, kev[2 * t], kev[2 * t + 1]));
+        sum += ms;
+      }
+      stats->ms_leaf_tiles = sum;
+    }
     stats->launches = log.count;
     stats->props_run = props;
     stats->leaf_tile = tensor_leaf ? 128 : (sh.leaf_tile ? sh.leaf_tile : 64);

@@ -103,6 +103,7 @@ struct LeafArgs {
   unsigned long long* pair_counter;  // optional
   int tile;              // 32 or 64 (0: 64): query x candidate tile, results identical
   int first_tree;        // trees [first_tree, first_tree + trees) of perm
+  cudaEvent_t* kev;      // [2 * trees] events around each tree's tile kernel, or null
   const int64_t* ftable;
   const int64_t* foff;
   const int64_t* fcount;
@@ -122,6 +123,7 @@ struct UmmaLeafArgs {
   void* Xb;              // [n][Kp] bf16 scratch (Kp = d rounded up to 64)
   float* norms2;         // [n] scratch
   int32_t* inv;          // [n] scratch: a tree's inverse order (null: duplicate checks in the merge)
+  cudaEvent_t* kev;      // [2 * trees] events around each tree's tile kernel, or null
   float* akey;           // [n][kq] approximate lists (in: empty)
   uint32_t* aid;
   float* rkey;           // [n][k] out: exact keys, sorted

@@ -223,9 +223,11 @@ static void launch_leaf_metric(const LeafArgs& a, int t, int kpl) {
 int leaf_stage(const LeafArgs& a, LaunchLog& log) {
   const int kpl = kpl_for(a.k);
   for (int t = a.first_tree; t < a.first_tree + a.trees; ++t) {
+    if (a.kev) cudaEventRecord(a.kev[2 * (t - a.first_tree)], a.stream);
     if (a.metric == KNN_METRIC_EUCLIDEAN) launch_leaf_metric<KNN_METRIC_EUCLIDEAN>(a, t, kpl);
     else if (a.metric == KNN_METRIC_TAXICAB) launch_leaf_metric<KNN_METRIC_TAXICAB>(a, t, kpl);
     else launch_leaf_metric<KNN_METRIC_COSINE>(a, t, kpl);
+    if (a.kev) cudaEventRecord(a.kev[2 * (t - a.first_tree) + 1], a.stream);
     log.add();
   }
   return cudaPeekAtLastError() == cudaSuccess ? KNN_OK : KNN_ERR_CUDA;

@@ -751,7 +751,13 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
     const int32_t* perm = a.perm + (size_t)t * a.n;
     const int64_t* ftab = a.ftable ? a.ftable + 4 * a.foff[t] : nullptr;
     const int64_t tleaves = a.ftable ? a.fcount[t] : leaves;
-    if (tleaves <= 0) continue;
+    if (tleaves <= 0) {
+      if (a.kev) {
+        cudaEventRecord(a.kev[2 * t], st);
+        cudaEventRecord(a.kev[2 * t + 1], st);
+      }
+      continue;
+    }
     const unsigned grid = (unsigned)(tleaves * qtiles);
     const int32_t* inv = nullptr;
     if (t > 0 && a.inv) {
@@ -765,6 +771,7 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
     k_leaf_tc<M, F><<<grid, kUThreads, smem, st>>>(Xb, Kp, a.segs, ftab, a.k, a.kq, qtiles, perm, inv, a.norms2, \
                                                    a.akey, a.aid, a.err);                                \
   } while (0)
+    if (a.kev) cudaEventRecord(a.kev[2 * t], st);
     if (a.metric == KNN_METRIC_EUCLIDEAN) {
       if (t == 0) KNN_TC_LAUNCH(KNN_METRIC_EUCLIDEAN, true);
       else KNN_TC_LAUNCH(KNN_METRIC_EUCLIDEAN, false);
@@ -772,6 +779,7 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
       if (t == 0) KNN_TC_LAUNCH(KNN_METRIC_COSINE, true);
       else KNN_TC_LAUNCH(KNN_METRIC_COSINE, false);
     }
+    if (a.kev) cudaEventRecord(a.kev[2 * t + 1], st);
 #undef KNN_TC_LAUNCH
     log.add();
   }

@@ -114,7 +114,7 @@ typedef struct knn_stats {
   float ms_learn;            /* learned splits: sample graph, training and embedding    */
   int32_t leaf_tile;         /* leaf tile used: 32/64 FP32, 128 tensor-core             */
   int32_t prop_warps;        /* propagation warps per block used (0: the default)       */
-  int32_t reserved_pad;
+  float ms_leaf_tiles;       /* summed device time of the leaf-tile kernel launches     */
   int64_t reserved[6];
 } knn_stats;
 
