@@ -294,17 +294,26 @@ __global__ void __launch_bounds__(kUThreads, 2)
     tcap[tid] = kInf;
   }
   // candidates of step s (warps 0-3, whole warps) into parity slot s & 1
-  auto load_cols = [&](int s) {
+  // fetch_cols loads them into registers (a step ahead), put_cols stores them
+  int32_t nid = -1;
+  float nnv = 0.f;
+  auto fetch_cols = [&](int s) {
     const int c0 = (s % ntiles) * kBN, mc = min(kBN, nb - c0);
-    const int32_t id = tid < mc ? perm[blo + c0 + tid] : -1;
-    cid2[(s & 1) * kBN + tid] = id;
-    const float nv = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
-    cn2[(s & 1) * kBN + tid] = id >= 0 ? nv : kInf;
+    nid = tid < mc ? perm[blo + c0 + tid] : -1;
+    nnv = (METRIC == KNN_METRIC_EUCLIDEAN && nid >= 0) ? norms2[nid] : 0.f;
+  };
+  auto put_cols = [&](int s) {
+    cid2[(s & 1) * kBN + tid] = nid;
+    cn2[(s & 1) * kBN + tid] = nid >= 0 ? nnv : kInf;
     // norms are >= 0, so their bit patterns order as unsigned integers
-    const uint32_t wm = __reduce_max_sync(0xFFFFFFFFu, __float_as_uint(nv));
+    const uint32_t wm = __reduce_max_sync(0xFFFFFFFFu, __float_as_uint(nnv));
     if (lane == 0) cmax2[(s & 1) * 4 + warp] = __uint_as_float(wm);
   };
-  if (tid < kBN) load_cols(0);
+  if (tid < kBN) {
+    fetch_cols(0);
+    put_cols(0);
+    if (nsteps > 1) fetch_cols(1);
+  }
   __syncthreads();
   stage_operand(opA, Xb, Kp, qid);
   stage_operand(opB, Xb, Kp, cid2);
@@ -389,7 +398,10 @@ __global__ void __launch_bounds__(kUThreads, 2)
     const int pass = pre && s < ntiles ? 0 : 1;
     const int c0 = (s % ntiles) * kBN, mc = min(kBN, nb - c0);
     const bool has_next = s + 1 < nsteps;
-    if (has_next && tid < kBN) load_cols(s + 1);
+    if (has_next && tid < kBN) {
+      put_cols(s + 1);
+      if (s + 2 < nsteps) fetch_cols(s + 2);
+    }
     if (tid == 0 && *status == 0 && !mbar_wait_bounded(bar, phase)) {
       *status = 1;
       atomicExch(err, 1);
@@ -489,18 +501,27 @@ __global__ void __launch_bounds__(kUThreads, 2)
             msk[r * 2 + half] = mask;
           }
         }
+        // Round 0 completes step s + 1's operand (staged since the top of the
+        // step) before its last barrier; its MMA is issued after that barrier.
+        const bool stage_here = ri == 0 && has_next;
+        if (stage_here && pass == 0) {
+          asm volatile("cp.async.wait_all;\n" ::: "memory");
+          asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        }
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         if (pass == 1) {
-          // Warp (quarter, half) takes the quarter's rows of parity half
-          // (found by one ballot); survivors' products come from this warp's
-          // lane quarter of tensor memory.
-          const int myrow = quarter * 32 + half + 2 * (lane & 15);
-          const bool has = lane < 16 && myrow < mq && (msk[myrow * 2] | msk[myrow * 2 + 1]) != 0;
-          uint32_t rows = __ballot_sync(0xFFFFFFFFu, has);
+          // The quarter's rows with survivors (one ballot) alternate between
+          // its two warps; survivors' products come from the warp's lane
+          // quarter of tensor memory.
+          const int rowq = quarter * 32 + lane;
+          const bool has = rowq < mq && (msk[rowq * 2] | msk[rowq * 2 + 1]) != 0;
+          const uint32_t all = __ballot_sync(0xFFFFFFFFu, has);
+          const bool mine = has && (__popc(all & ((1u << lane) - 1u)) & 1) == half;
+          uint32_t rows = __ballot_sync(0xFFFFFFFFu, mine);
           while (rows) {
-            const int ql = half + 2 * (__ffs(rows) - 1);  // row within the quarter
+            const int ql = __ffs(rows) - 1;  // row within the quarter
             const int qq = quarter * 32 + ql;
             rows &= rows - 1;
             const uint32_t m0 = msk[qq * 2], m1 = msk[qq * 2 + 1];
@@ -547,19 +568,16 @@ __global__ void __launch_bounds__(kUThreads, 2)
             Lk[qq * kLS + lane] = lk;
             Li[qq * kLS + lane] = li;
           }
+          if (stage_here) {
+            asm volatile("cp.async.wait_all;\n" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+          }
           asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
           __syncthreads();
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         }
-      }
-      if (ri == 0 && has_next) {
         // step s + 1's operand has landed: its MMA runs during round 1
-        asm volatile("cp.async.wait_all;\n" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        if (tid == 0) issue_mma(s + 1);
+        if (stage_here && tid == 0) issue_mma(s + 1);
       }
     }
     if (FIRST && pass == 0 && s == ntiles - 1) {
