@@ -1,4 +1,4 @@
-// Exact k-NN in FP64 on the GPU: the judge of recall and distance error.
+// Exact k-NN in FP64 on the GPU: the yardstick of recall and distance error.
 // No counterpart in the reference (which never checks its own output; its
 // VALIDATION file is written unconditionally, euclideandistancematrixgpu.cu:2967-2971).
 //

@@ -1,4 +1,4 @@
-// Allocation-free variant of the FP64 exact k-NN judge (knn_exact_fp64_noalloc).
+// Allocation-free variant of the FP64 exact k-NN (knn_exact_fp64_noalloc).
 //
 // Some callers cannot allocate device memory once they are running: a serving
 // process whose whole device memory is handed to its own pool at start-up, or
@@ -47,7 +47,7 @@ unsigned char* g_scratch_addr[kMaxDevices] = {};
 inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 // Copies the query ids into the scratch, replacing any id outside [0, n) by 0
-// and raising the status word, so the judge kernels never read out of bounds.
+// and raising the status word, so the exact kernels never read out of bounds.
 __global__ void k_sanitize_queries(const int64_t* __restrict__ q, int64_t nq, int64_t n,
                                    int64_t* __restrict__ out, int* __restrict__ status) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;

@@ -256,7 +256,7 @@ __device__ __forceinline__ float self_dot_chunked(const float* __restrict__ a, i
 // ------------------------------------------------------ warp top-k lists --
 // A sorted list of 32*KPL (key, id) entries held by one warp: entry e lives in
 // register e/32 of lane e%32.  Bit 31 of an id is a caller-defined flag and is
-// ignored by comparisons.  K is float (keys) or double (exact judge).
+// ignored by comparisons.  K is float (keys) or double (exact k-NN).
 __device__ __forceinline__ bool cand_less(double ka, uint32_t ia, double kb, uint32_t ib) {
   return ka < kb || (!(kb < ka) && (ia & kIdMask) < (ib & kIdMask));
 }

@@ -240,7 +240,7 @@ int knn_propagate_step(knn_context* ctx, const float* points, int64_t n, int32_t
 
 /*
  * knn_exact_fp64 -- exact k-NN of `nq` query rows against all n points in
- * FP64 on the GPU (self excluded, ties by index).  The judge of recall and
+ * FP64 on the GPU (self excluded, ties by index).  The yardstick of recall and
  * distance error; no counterpart in the reference.
  *   points host or device (opt->points_on_device) float32 [n][d]
  *   queries host int64 [nq] row ids;  out_idx host int32 [nq][k];

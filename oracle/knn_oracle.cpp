@@ -7,16 +7,16 @@
 //   points -> random-projection trees -> leaf-block all-pairs k-NN
 //          -> neighbour-of-neighbour propagation (Jacobi) -> k-NN graph
 //
-// plus an FP64 exact brute-force k-NN used as the recall / distance-error judge,
+// plus an FP64 exact brute-force k-NN used as the recall / distance-error yardstick,
 // and the learned split network's forward pass and triplet-loss gradient in
 // FP64 (no reference counterpart; the tests pin it by central finite
-// differences, then use it as the judge of the GPU backward kernels).
+// differences, then check the GPU backward kernels against it).
 //
 // Parity: the reference ships no tests, golden vectors or fixtures, and its GPU
 // output is non-deterministic (atomic scatter order, atomic tie fill, unstable
 // std::sort).  Parity of THIS restatement with the reference is therefore pinned
 // only through the hand-built known-answer cases under tests/ (analytic grids,
-// duplicates, ties, N = k+1, d = 1, d = 257) and the FP64 exact judge; the
+// duplicates, ties, N = k+1, d = 1, d = 257) and the FP64 exact k-NN; the
 // reference's own sm_100a build is compared by recall only.
 //
 // Deterministic rules (each departs from the reference only where the reference

@@ -132,7 +132,7 @@ def _ab_cases(acknn):
 @pytest.mark.parametrize("case", range(3))
 def test_learned_splits_ab(acknn, capsys, case):
     """A/B of the trained network against random-projection splits at equal
-    trees, leaf size and propagations; recall against the FP64 exact judge.
+    trees, leaf size and propagations; recall against the FP64 exact k-NN.
 
     The network gains where raw coordinates misrepresent the metric (COSINE on
     rows whose norms spread over two decades: the unit-row input plus the

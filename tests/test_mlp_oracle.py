@@ -1,5 +1,5 @@
 """The learned split network's FP64 oracle (forward pass and triplet-loss
-gradient) pinned by central finite differences on the CPU; it is then the judge
+gradient) pinned by central finite differences on the CPU; it is then the reference
 of the GPU forward and backward kernels (test_mlp_gpu.py)."""
 from __future__ import annotations
 

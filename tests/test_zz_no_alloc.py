@@ -1,4 +1,4 @@
-"""knn_exact_fp64_noalloc: the FP64 exact judge for callers that cannot allocate
+"""knn_exact_fp64_noalloc: the FP64 exact k-NN for callers that cannot allocate
 device memory while they run (for example a process that hands all device
 memory to its own pool at start-up).  It works from caller-owned device buffers
 and one fixed scratch array compiled into the library.
@@ -25,7 +25,7 @@ def _noalloc(lib, xd, n, d, k, metric, qd, nq, torch):
     return rc, idx.cpu().numpy(), dist.cpu().numpy()
 
 
-def test_noalloc_matches_allocating_judge_twice():
+def test_noalloc_matches_allocating_entry_twice():
     torch = pytest.importorskip("torch")
     acknn = load_package()
     lib = acknn.load_library()
