@@ -97,7 +97,9 @@ class KnnStats(ctypes.Structure):
         ("leaf_tile", ctypes.c_int32),
         ("prop_warps", ctypes.c_int32),
         ("ms_leaf_tiles", ctypes.c_float),
-        ("reserved", ctypes.c_int64 * 6),
+        ("leaf_path", ctypes.c_int32),
+        ("leaf_fallback", ctypes.c_int32),
+        ("reserved", ctypes.c_int64 * 5),
     ]
 
     def as_dict(self) -> dict:
@@ -109,6 +111,7 @@ class KnnStats(ctypes.Structure):
             "ms_leaf_tiles": self.ms_leaf_tiles,
             "launches": self.launches, "leaf_pairs": self.leaf_pairs,
             "leaf_tile": self.leaf_tile, "prop_warps": self.prop_warps,
+            "leaf_path": self.leaf_path, "leaf_fallback": self.leaf_fallback,
             "prop_candidates": [self.prop_candidates[i] for i in range(n)],
         }
 
@@ -138,6 +141,8 @@ EXPORTS = {
     "knn_context_create": (_P, [_I32]),
     "knn_context_destroy": (None, [_P]),
     "knn_context_scratch_bytes": (_I64, [_P]),
+    "knn_context_status": (ctypes.c_int, [_P, _P]),
+    "knn_test_fail_next_tile_wait": (ctypes.c_int, [_P]),
     "knn_build": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _I32, _I32, _I32, _U64, _P, _P]),
     "knn_build_ex": (ctypes.c_int, [_P, _P, _I64, _I32, _I32, _I32, _I32, _I32, _I32, _U64, _P,
                                     _P, _P, _P]),

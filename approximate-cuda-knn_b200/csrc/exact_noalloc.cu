@@ -14,6 +14,11 @@
 //   * the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (once per device, with that device current), so make
 //     that first call before any stream capture begins;
+//   * with CUDA's lazy module loading (the default) the array itself is
+//     reserved on a device only when this code first runs there, so a caller
+//     that hands its device memory to a pool at start-up makes one warm-up call
+//     on each device before that; if the reservation fails the call returns
+//     KNN_ERR_OOM with a message saying so;
 //   * every call shares the one array and leaves its contents behind: calls
 //     that overlap on the GPU (two streams, two host threads) race on it;
 //   * requests whose scratch would not fit are rejected with KNN_ERR_ARGS.
@@ -72,6 +77,12 @@ int scratch_for_device(unsigned char** out) {
   if (!g_scratch_addr[dev]) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e == cudaErrorMemoryAllocation) {
+      cudaGetLastError();
+      return fail(KNN_ERR_OOM,
+                  "the 16 MiB scratch of knn_exact_fp64_noalloc could not be reserved on this device; make a "
+                  "first call on each device before device memory is handed to a pool");
+    }
     if (e != cudaSuccess || !p)
       return fail(KNN_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     g_scratch_addr[dev] = static_cast<unsigned char*>(p);

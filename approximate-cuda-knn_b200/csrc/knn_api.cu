@@ -76,6 +76,14 @@ struct knn_context {
   // Autotuned launch shapes by workload key: (FP32 leaf tile, propagation warps).
   std::map<std::string, std::pair<int, int>> tuned;
   cudaEvent_t tev[2] = {};
+  // Device error words: [0] is cleared at the start of every build and tells
+  // the tensor-core tile kernels of that build to stop issuing work; [1] is
+  // sticky -- set with [0] by a kernel whose bounded wait gave up, and cleared
+  // only when a synchronising call or knn_context_status() reports it, so an
+  // asynchronous build's failure reaches the caller.
+  int* err_words = nullptr;
+  // Test hook: the next build starts with both error words set.
+  bool preset_err = false;
   // Events around each tree's leaf-tile kernel (statistics only), grown on demand.
   std::vector<cudaEvent_t> kev;
   cudaEvent_t* kernel_events(int trees) {
@@ -127,6 +135,7 @@ struct knn_context {
     for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
     for (auto& kv : bufs)
       if (kv.second.p) cudaFree(kv.second.p);
+    if (err_words) cudaFree(err_words);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     for (auto& e : tev)
@@ -155,6 +164,8 @@ int make_context(int device, knn_context** out) {
   KNN_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   for (auto& ev : c->ev) KNN_CK(cudaEventCreate(&ev));
   for (auto& ev : c->tev) KNN_CK(cudaEventCreate(&ev));
+  KNN_CK(cudaMalloc(&c->err_words, 2 * sizeof(int)));
+  KNN_CK(cudaMemset(c->err_words, 0, 2 * sizeof(int)));
   *out = c.release();
   return KNN_OK;
 }
@@ -716,6 +727,28 @@ int enter_device(knn_context** ctx, const knn_options& o) {
   return KNN_OK;
 }
 
+// Start of a build: clear the per-build error word (or set both words for the
+// test hook) on the build's stream.
+int reset_error_word(knn_context* C, cudaStream_t st) {
+  if (C->preset_err) {
+    C->preset_err = false;
+    KNN_CK(cudaMemsetAsync(C->err_words, 0x01, 2 * sizeof(int), st));
+  } else {
+    KNN_CK(cudaMemsetAsync(C->err_words, 0, sizeof(int), st));
+  }
+  return KNN_OK;
+}
+
+// After the stream has finished: KNN_ERR_TIMEOUT (and the sticky word
+// cleared) when a tile wait of this or an earlier asynchronous build gave up.
+int check_error_words(knn_context* C) {
+  int host[2] = {0, 0};
+  KNN_CK(cudaMemcpy(host, C->err_words, sizeof(host), cudaMemcpyDeviceToHost));
+  if (host[0] == 0 && host[1] == 0) return KNN_OK;
+  KNN_CK(cudaMemset(C->err_words + 1, 0, sizeof(int)));
+  return fail(KNN_ERR_TIMEOUT, "a tensor-core tile wait exceeded its time limit");
+}
+
 int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t k,
                int32_t trees, int32_t leaf, int32_t props, int32_t metric, uint64_t seed,
                int32_t* out_idx, float* out_dist, const knn_options& o, knn_stats* stats) {
@@ -773,10 +806,9 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
   Lists L;
   rc = get_lists(C, n, k, &L);
   if (rc) return rc;
-  int* err_flag = nullptr;
-  rc = C->get("err_flag", 1, &err_flag);
+  int* err_flag = C->err_words;
+  rc = reset_error_word(C, st);
   if (rc) return rc;
-  KNN_CK(cudaMemsetAsync(err_flag, 0, sizeof(int), st));
   const bool tensor_leaf = o.precision == KNN_PREC_BF16_RERANK && metric != KNN_METRIC_TAXICAB &&
                            d <= 256 && k <= 32;
   Layout lay = single_layout(n, T.depth);
@@ -839,9 +871,8 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
   const bool async_ok = o.stream && o.outputs_on_device && !stats;
   if (!async_ok) {
     KNN_CK(cudaStreamSynchronize(st));
-    int host_err = 0;
-    KNN_CK(cudaMemcpy(&host_err, err_flag, sizeof(int), cudaMemcpyDeviceToHost));
-    if (host_err) return fail(KNN_ERR_TIMEOUT, "a tensor-core tile wait exceeded its iteration limit");
+    rc = check_error_words(C);
+    if (rc) return rc;
   }
 
   if (stats) {
@@ -879,6 +910,8 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
     stats->launches = log.count;
     stats->props_run = props;
     stats->leaf_tile = tensor_leaf ? 128 : (sh.leaf_tile ? sh.leaf_tile : 64);
+    stats->leaf_path = tensor_leaf ? 1 : 0;
+    stats->leaf_fallback = (o.precision == KNN_PREC_BF16_RERANK && !tensor_leaf) ? 1 : 0;
     stats->prop_warps = sh.prop_warps;
     unsigned long long host[2 + KNN_MAX_PROPS];
     KNN_CK(cudaMemcpy(host, counters, sizeof(host), cudaMemcpyDeviceToHost));
@@ -1027,10 +1060,9 @@ int batch_impl(knn_context* C, const knn_dataset* sets, int count, int32_t k, in
   std::map<int, std::vector<int>> by_d;
   for (int i = 0; i < count; ++i) by_d[sets[i].d].push_back(i);
   int max_depth = 0;
-  int* err_flag = nullptr;
-  int rc = C->get("err_flag", 1, &err_flag);
+  int* err_flag = C->err_words;
+  int rc = reset_error_word(C, st);
   if (rc) return rc;
-  KNN_CK(cudaMemsetAsync(err_flag, 0, sizeof(int), st));
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   KNN_CK(cudaStreamIsCapturing(st, &cs));
   if (cs != cudaStreamCaptureStatusNone || timed) use_graphs = false;
@@ -1145,9 +1177,8 @@ int batch_impl(knn_context* C, const knn_dataset* sets, int count, int32_t k, in
   const bool async_ok = o.stream && o.outputs_on_device && !stats;
   if (!async_ok) {
     KNN_CK(cudaStreamSynchronize(st));
-    int host_err = 0;
-    KNN_CK(cudaMemcpy(&host_err, err_flag, sizeof(int), cudaMemcpyDeviceToHost));
-    if (host_err) return fail(KNN_ERR_TIMEOUT, "a tensor-core tile wait exceeded its iteration limit");
+    rc = check_error_words(C);
+    if (rc) return rc;
   }
   if (stats) {
     const int32_t sz = stats->struct_size;
@@ -1162,6 +1193,13 @@ int batch_impl(knn_context* C, const knn_dataset* sets, int count, int32_t k, in
     stats->ms_propagate = stage_ms[2];
     stats->launches = log.count;
     stats->props_run = props;
+    // per group of equal d: tensor-core tiles when the request allows them
+    for (const auto& kv : by_d) {
+      const bool tc = o.precision == KNN_PREC_BF16_RERANK && metric != KNN_METRIC_TAXICAB && kv.first <= 256 &&
+                      k <= 32;
+      if (tc) stats->leaf_path = 1;
+      if (o.precision == KNN_PREC_BF16_RERANK && !tc) stats->leaf_fallback = 1;
+    }
   }
   return KNN_OK;
 }
@@ -1223,6 +1261,24 @@ knn_context* knn_context_create(int32_t device) {
 void knn_context_destroy(knn_context* ctx) { delete ctx; }
 
 int64_t knn_context_scratch_bytes(const knn_context* ctx) { return ctx ? ctx->bytes_held() : 0; }
+
+int knn_context_status(knn_context* ctx, void* stream) {
+  knn_options o;
+  knn_default_options(&o);
+  int rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  KNN_CK(cudaStreamSynchronize(stream ? static_cast<cudaStream_t>(stream) : ctx->stream));
+  return check_error_words(ctx);
+}
+
+int knn_test_fail_next_tile_wait(knn_context* ctx) {
+  knn_options o;
+  knn_default_options(&o);
+  int rc = enter_device(&ctx, o);
+  if (rc) return rc;
+  ctx->preset_err = true;
+  return KNN_OK;
+}
 
 int knn_build(const void* points, int64_t n, int32_t d, int32_t k, int32_t trees, int32_t leaf,
               int32_t props, int32_t metric, uint64_t seed, int32_t* out_idx, float* out_dist) {

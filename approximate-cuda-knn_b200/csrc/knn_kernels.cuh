@@ -128,7 +128,7 @@ struct UmmaLeafArgs {
   uint32_t* aid;
   float* rkey;           // [n][k] out: exact keys, sorted
   uint32_t* rid;
-  int* err;              // set when a bounded wait expires
+  int* err;              // [2]: [0] stop word of this build, [1] sticky; both set when a bounded wait expires
   const int64_t* ftable; // as in LeafArgs
   const int64_t* foff;
   const int64_t* fcount;

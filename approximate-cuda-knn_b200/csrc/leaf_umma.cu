@@ -404,7 +404,8 @@ __global__ void __launch_bounds__(kUThreads, 2)
     }
     if (tid == 0 && *status == 0 && !mbar_wait_bounded(bar, phase)) {
       *status = 1;
-      atomicExch(err, 1);
+      atomicExch(err, 1);     // this build's blocks stop issuing MMAs
+      atomicOr(err + 1, 1);   // sticky until the host reports it
       mbar_wait_bounded(bar, phase);  // let the MMAs drain before TMEM is freed
     }
     phase ^= 1u;

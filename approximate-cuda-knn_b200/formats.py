@@ -100,6 +100,29 @@ def write_csv(path: str, x: np.ndarray, labels: np.ndarray | None = None) -> Non
             f.write(line + "\n")
 
 
+def write_csv_integers(path: str, x: np.ndarray) -> None:
+    """CSV in the reference's input format for non-negative integer values
+    below 1000 (the integer-mixture points), written without per-value
+    formatting: every value takes three characters, left-padded with spaces,
+    which the reference's reader trims before atof (trim, .cu:1987-1995)."""
+    x = np.asarray(x)
+    n, d = x.shape
+    v = np.rint(x).astype(np.int64)
+    if v.size and (v.min() < 0 or v.max() > 999 or not np.array_equal(v, x)):
+        raise ValueError("write_csv_integers takes integers in [0, 999]")
+    table = np.frombuffer(b"".join(b"%3d" % i for i in range(1000)), dtype=np.uint8).reshape(1000, 3)
+    with open(path, "wb") as f:
+        f.write(f"{n}\n{d}\n".encode())
+        step = 1 << 16
+        for s in range(0, n, step):
+            blk = v[s:s + step]
+            out = np.empty((blk.shape[0], d, 4), dtype=np.uint8)
+            out[:, :, :3] = table[blk]
+            out[:, :, 3] = ord(",")
+            out[:, -1, 3] = ord("\n")
+            f.write(out.tobytes())
+
+
 def stored_distance(dist: np.ndarray, metric: int) -> np.ndarray:
     """Value the reference stores for a returned distance (see module doc)."""
     dist = np.asarray(dist, dtype=np.float32)

@@ -158,9 +158,11 @@ def make_points(acknn, n: int, seed: int) -> np.ndarray:
 
 
 # ------------------------------------------------------------- accuracy --
-def accuracy(acknn, x, idx, dist, k, metric, exact, q) -> dict:
+def accuracy(acknn, x, idx, dist, k, metric, exact, q, gathered: bool = False) -> dict:
+    """Recall@k (tie-aware and by id) and distance error against the FP64 exact
+    graph on the query rows q; ``gathered``: idx/dist hold only those rows."""
     ei, ed = exact
-    ai, ad = idx[q], dist[q]
+    ai, ad = (idx, dist) if gathered else (idx[q], dist[q])
     a = x[q].astype(np.float64)
     pair = np.empty(ai.shape, dtype=np.float64)
     for s in range(k):
@@ -710,6 +712,288 @@ def run_config(args):
     return 0
 
 
+# ------------------------------------------------ the reference's own build --
+REF_BIN = ROOT / "oracle" / "_ref" / "hello"
+
+
+def reference_gpu_runs(acknn, x, k, q, exact_ids, settings, limit_s: float) -> dict:
+    """The reference's own CUDA program, built unmodified from its sources for
+    sm_100a (oracle/Makefile `ref`), run through its CLI on the same points as
+    CSV: per setting its self-reported device time of calculate()
+    (euclideandistancematrixgpu.cu:2867, :2889-2893), the wall time of the
+    whole process (CSV parse and file write included), and recall@k by id on
+    the query rows from its output file.  A run past ``limit_s`` seconds is
+    killed and recorded as not run."""
+    import re
+    import shutil
+    import tempfile
+
+    if not REF_BIN.exists():
+        return {"not_run": "reference build absent (oracle/_ref/hello)"}
+    tmp = Path(tempfile.mkdtemp(prefix="acknn_ref_"))
+    out = {}
+    try:
+        csv = tmp / "points.csv"
+        t = time.perf_counter()
+        acknn.formats.write_csv_integers(str(csv), x)
+        out["csv_write_s"] = time.perf_counter() - t
+        out["csv_bytes"] = csv.stat().st_size
+        for name, p in settings.items():
+            res = tmp / f"{name}.bin"
+            cmd = [str(REF_BIN), str(csv), str(res), str(k), str(p["trees"]), str(p["leaf"]),
+                   str(p["props"]), "EUCLIDEAN", "0", "F"]
+            t = time.perf_counter()
+            try:
+                r = subprocess.run(cmd, capture_output=True, text=True, timeout=limit_s)
+            except subprocess.TimeoutExpired:
+                out[name] = {"params": p, "not_run": f"exceeded {limit_s:.0f} s"}
+                continue
+            wall = time.perf_counter() - t
+            m = re.search(r"has done task in: ([0-9.eE+-]+) ms", r.stdout)
+            if r.returncode != 0 or not m:
+                out[name] = {"params": p, "not_run": f"exit {r.returncode}: {r.stdout[-300:]}"}
+                continue
+            _, _, ids, _ = acknn.formats.read_result(str(res))
+            ai = ids[q]
+            rec = sum(len(np.intersect1d(a, b)) for a, b in zip(ai, exact_ids)) / (k * len(q))
+            ms = float(m.group(1))
+            out[name] = {"params": p, "ms_calculate": ms, "points_per_s": x.shape[0] / (ms / 1e3),
+                         "process_wall_s": wall, "recall_id": rec}
+            res.unlink(missing_ok=True)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return out
+
+
+def run_reference_gpu(args, w):
+    """The reference's own build on the integer mixture at the configuration's
+    literal parameters and at the headline setting (one run each)."""
+    import torch
+
+    torch.cuda.set_device(0)
+    acknn = load_package()
+    acknn.load_library()
+    n, k = w["n"], w["k"]
+    x = make_points(acknn, n, seed=0)
+    rng = np.random.Generator(np.random.PCG64(12345))
+    q = np.sort(rng.choice(n, size=min(10_000, n), replace=False)).astype(np.int64)
+    ei, _ = acknn.exact_fp64(x, k, q, w["metric"])
+    settings = {"literal": CONFIG_PARAMS, "headline": TARGET_PARAMS}
+    if args.trees or args.leaf or args.props is not None:
+        settings = {"custom": dict(trees=args.trees or 8, leaf=args.leaf or 2048,
+                                   props=args.props if args.props is not None else 0)}
+    r = reference_gpu_runs(acknn, x, k, q, ei, settings, args.ref_limit)
+    print(json.dumps({"reference_gpu": r, "workload": workload_desc(w, TARGET_PARAMS)}), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------ setting sweep --
+# Grids searched per workload: trees x leaf, and for each pair propagations
+# 0..max_props until the recall target is met.
+SWEEP_GRIDS = {
+    "integer_mixture": dict(trees=[6, 8, 10, 12, 16], leaf=[256, 512, 1024, 2048], max_props=3),
+    "sparse_prototypes": dict(trees=[4, 8, 16], leaf=[128, 512, 2048, 8192], max_props=12),
+    "normalized_mixture": dict(trees=[4, 6, 8, 12], leaf=[64, 128, 256, 512, 1024, 2048], max_props=8),
+    "dataset_batch": dict(trees=[4, 8, 12], leaf=[48, 128, 256, 512, 1024, 2048], max_props=6),
+}
+
+
+class _SingleRunner:
+    """One configuration's points resident in HBM, its FP64 exact graph on
+    10,000 seeded queries, and builds of any (path, trees, leaf, props)."""
+
+    def __init__(self, acknn, lib, torch, name: str, n: int | None):
+        cfg = acknn.workloads.CONFIGS[name]
+        self.acknn, self.lib, self.torch = acknn, lib, torch
+        self.n = n or cfg["n"]
+        self.k, self.metric = cfg["k"], cfg["metric"]
+        self.x = cfg["gen"](0, n=self.n)
+        self.d = self.x.shape[1]
+        self.dtype = acknn.F16 if self.x.dtype == np.float16 else acknn.F32
+        self.xd = torch.from_numpy(self.x).cuda()
+        self.idx = torch.empty((self.n, self.k), dtype=torch.int32, device="cuda")
+        self.dist = torch.empty((self.n, self.k), dtype=torch.float32, device="cuda")
+        self.ctx = acknn.Context(0)
+        self.stream = torch.cuda.current_stream()
+        rng = np.random.Generator(np.random.PCG64(12345))
+        self.q = np.sort(rng.choice(self.n, size=min(10_000, self.n), replace=False)).astype(np.int64)
+        self.exact = acknn.exact_fp64(self.x, self.k, self.q, self.metric)
+        self.qt = torch.from_numpy(self.q).cuda()
+        self.points = self.n
+
+    def build(self, kw: dict, T: int, L: int, P: int, stats=None):
+        opt = self.acknn.default_options(points_on_device=1, outputs_on_device=1, dtype=self.dtype,
+                                         stream=self.stream.cuda_stream, **kw)
+        rc = self.lib.knn_build_ex(self.ctx.handle, self.xd.data_ptr(), self.n, self.d, self.k, T, L, P,
+                                   self.metric, 0, self.idx.data_ptr(), self.dist.data_ptr(),
+                                   ctypes.byref(opt), ctypes.byref(stats) if stats is not None else None)
+        if rc:
+            raise self.acknn.KnnError(rc, self.lib.knn_last_error().decode())
+
+    def accuracy(self) -> dict:
+        return accuracy(self.acknn, self.x, self.idx[self.qt].cpu().numpy(), self.dist[self.qt].cpu().numpy(),
+                        self.k, self.metric, self.exact, self.q, gathered=True)
+
+    def close(self):
+        self.ctx.close()
+
+
+class _BatchRunner:
+    """The 256-dataset batch resident in HBM; per-set FP64 exact graphs on up to
+    500 seeded queries per set; one knn_build_batch per build."""
+
+    def __init__(self, acknn, lib, torch, count: int | None):
+        cfg = acknn.workloads.CONFIGS["dataset_batch"]
+        self.acknn, self.lib, self.torch = acknn, lib, torch
+        self.count = count or cfg["count"]
+        self.k, self.metric = cfg["k"], cfg["metric"]
+        self.xs = [acknn.workloads.batch_dataset(s) for s in range(self.count)]
+        self.points = sum(x.shape[0] for x in self.xs)
+        self.xd = [torch.from_numpy(x).cuda() for x in self.xs]
+        self.oi = [torch.empty((x.shape[0], self.k), dtype=torch.int32, device="cuda") for x in self.xs]
+        self.od = [torch.empty((x.shape[0], self.k), dtype=torch.float32, device="cuda") for x in self.xs]
+        self.ctx = acknn.Context(0)
+        self.stream = torch.cuda.current_stream()
+        arr = (acknn.KnnDataset * self.count)()
+        for i, x in enumerate(self.xs):
+            arr[i].points = self.xd[i].data_ptr()
+            arr[i].n, arr[i].d, arr[i].seed = x.shape[0], x.shape[1], i
+            arr[i].out_idx = self.oi[i].data_ptr()
+            arr[i].out_dist = self.od[i].data_ptr()
+        self.table = arr
+        rng = np.random.Generator(np.random.PCG64(7))
+        self.qs, self.exact = [], []
+        for x in self.xs:
+            q = np.sort(rng.choice(x.shape[0], size=min(500, x.shape[0]), replace=False)).astype(np.int64)
+            self.qs.append(q)
+            self.exact.append(acknn.exact_fp64(x, self.k, q, self.metric))
+
+    def build(self, kw: dict, T: int, L: int, P: int, stats=None):
+        opt = self.acknn.default_options(points_on_device=1, outputs_on_device=1,
+                                         stream=self.stream.cuda_stream, autotune=1, **kw)
+        rc = self.lib.knn_build_batch(self.ctx.handle, self.table, self.count, self.k, T, L, P, self.metric,
+                                      ctypes.byref(opt), ctypes.byref(stats) if stats is not None else None)
+        if rc:
+            raise self.acknn.KnnError(rc, self.lib.knn_last_error().decode())
+
+    def accuracy(self) -> dict:
+        per, hits, total = [], 0, 0
+        for i, x in enumerate(self.xs):
+            ai = self.oi[i].cpu().numpy()[self.qs[i]]
+            ei = self.exact[i][0]
+            h = sum(len(np.intersect1d(a, b)) for a, b in zip(ai, ei))
+            per.append(h / (self.k * len(ai)))
+            hits += h
+            total += self.k * len(ai)
+        return {"recall": hits / total, "recall_id": hits / total, "recall_min": min(per),
+                "recall_mean_of_sets": sum(per) / len(per),
+                "sets_below_0.95": int(sum(r < 0.95 for r in per)), "queries": total // self.k}
+
+    def close(self):
+        self.ctx.close()
+
+
+def _sweep_paths(acknn, workload: str, metric: int, n: int) -> dict:
+    paths = {"plain_fp32": dict(precision=acknn.PREC_FP32)}
+    if metric != 1:
+        paths["mixed"] = dict(precision=acknn.PREC_BF16_RERANK)
+    if metric == 2 and workload != "dataset_batch":
+        paths["mixed_learned"] = dict(precision=acknn.PREC_BF16_RERANK, learned_splits=1,
+                                      mlp_sample=min(n, 1_000_000))
+    return paths
+
+
+def run_sweep(args):
+    """Cheapest (trees, leaf, propagations) reaching recall@k >= --target per
+    path.  For each (trees, leaf), in order of growing leaf work, propagations
+    rise from 0 until the target is met; a setting is timed (warm-up build,
+    then --steps builds under CUDA events, points resident in HBM) only once
+    it meets the target, and a pair is abandoned once an untimed build already
+    takes longer than the best timed setting.  One JSON line per tried setting,
+    then a summary line per path and the equal-recall ratios."""
+    import torch
+
+    torch.cuda.set_device(0)
+    acknn = load_package()
+    lib = acknn.load_library()
+    name = args.workload
+    grid = dict(SWEEP_GRIDS[name])
+    if args.grid_trees:
+        grid["trees"] = [int(v) for v in args.grid_trees.split(",")]
+    if args.grid_leaf:
+        grid["leaf"] = [int(v) for v in args.grid_leaf.split(",")]
+    if args.max_props is not None:
+        grid["max_props"] = args.max_props
+    if name == "dataset_batch":
+        R = _BatchRunner(acknn, lib, torch, args.count)
+    else:
+        R = _SingleRunner(acknn, lib, torch, name, args.n)
+    paths = _sweep_paths(acknn, name, R.metric, R.points)
+    if args.paths:
+        paths = {p: paths[p] for p in args.paths.split(",")}
+    stream = R.stream
+
+    def timed(fn, steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    pairs = sorted(((T, L) for T in grid["trees"] for L in grid["leaf"]), key=lambda tl: (tl[0] * tl[1], tl[0]))
+    summary = {}
+    for pname, kw in paths.items():
+        best = None
+        top = None  # highest recall seen, for a path that never meets the target
+        for T, L in pairs:
+            for P in range(grid["max_props"] + 1):
+                t0 = time.perf_counter()
+                try:
+                    R.build(kw, T, L, P)
+                    torch.cuda.synchronize()
+                except acknn.KnnError as e:
+                    print(json.dumps({"trial": pname, "trees": T, "leaf": L, "props": P, "error": str(e)}),
+                          flush=True)
+                    break
+                wall_ms = (time.perf_counter() - t0) * 1e3
+                acc = R.accuracy()
+                rec = acc["recall"]
+                row = {"trial": pname, "trees": T, "leaf": L, "props": P, "recall": rec, "wall_ms_untimed": wall_ms}
+                if top is None or rec > top["recall"]:
+                    top = dict(row)
+                if rec >= args.target:
+                    R.build(kw, T, L, P)
+                    ms = timed(lambda: R.build(kw, T, L, P), args.steps)
+                    st = acknn.KnnStats()
+                    st.struct_size = ctypes.sizeof(acknn.KnnStats)
+                    R.build(kw, T, L, P, stats=st)
+                    torch.cuda.synchronize()
+                    sd = st.as_dict()
+                    row.update(ms=ms, points_per_s=R.points / (ms / 1e3), accuracy=acc,
+                               stages_ms={kk: sd[kk] for kk in ("ms_learn", "ms_trees", "ms_leaf", "ms_propagate")},
+                               leaf_tile=sd["leaf_tile"])
+                    print(json.dumps(row), flush=True)
+                    if best is None or ms < best["ms"]:
+                        best = row
+                    break
+                print(json.dumps(row), flush=True)
+                if best is not None and wall_ms > 1.5 * best["ms"]:
+                    break
+        summary[pname] = best if best is not None else {"target_not_met": True, "best_recall_seen": top}
+    out = {"sweep": name, "target": args.target, "points": R.points, "k": R.k,
+           "metric": METRIC_NAMES[R.metric], "grid": grid, "steps": args.steps, "cheapest": summary}
+    if "plain_fp32" in summary and summary["plain_fp32"].get("ms"):
+        for pname, row in summary.items():
+            if pname != "plain_fp32" and row.get("ms"):
+                out[f"{pname}_vs_plain_at_equal_recall"] = summary["plain_fp32"]["ms"] / row["ms"]
+    print(json.dumps(out), flush=True)
+    R.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -728,6 +1012,16 @@ def main():
     ap.add_argument("--trees", type=int, default=None)
     ap.add_argument("--leaf", type=int, default=None)
     ap.add_argument("--props", type=int, default=None)
+    ap.add_argument("--sweep", action="store_true",
+                    help="search the cheapest setting reaching --target recall per path")
+    ap.add_argument("--target", type=float, default=0.95)
+    ap.add_argument("--grid-trees", default=None, help="comma-separated trees to sweep")
+    ap.add_argument("--grid-leaf", default=None, help="comma-separated leaf sizes to sweep")
+    ap.add_argument("--max-props", type=int, default=None)
+    ap.add_argument("--paths", default=None, help="comma-separated paths to sweep")
+    ap.add_argument("--reference-gpu", action="store_true",
+                    help="time the reference's own sm_100a build (oracle/_ref/hello) on the workload")
+    ap.add_argument("--ref-limit", type=float, default=300.0, help="seconds per reference run")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -736,6 +1030,10 @@ def main():
         w["n"] = args.n
     if args.impl == "reference":
         return run_reference(args, w)
+    if args.sweep:
+        return run_sweep(args)
+    if args.reference_gpu:
+        return run_reference_gpu(args, w)
     if args.workload == "dataset_batch":
         return run_batch(args)
     if args.workload in ("sparse_prototypes", "normalized_mixture"):

@@ -56,7 +56,10 @@ extern "C" {
 #define KNN_PREC_FP32 0        /* every key in FP32 CUDA-core arithmetic          */
 #define KNN_PREC_BF16_RERANK 1 /* leaf blocks as BF16 tensor-core tiles in the
                                   |x|^2+|y|^2-2x.y form, each point's best 2k
-                                  re-ranked with exact FP32 keys                 */
+                                  re-ranked with exact FP32 keys.  TAXICAB, and
+                                  requests the tiles cannot hold, run the FP32
+                                  leaf stage instead; knn_stats.leaf_path and
+                                  leaf_fallback say which ran                     */
 
 /* Tree split rules.  MEDIAN: each node splits at the median of its points'
  * projections (balanced trees of static shape).  REFERENCE: the split of
@@ -115,7 +118,9 @@ typedef struct knn_stats {
   int32_t leaf_tile;         /* leaf tile used: 32/64 FP32, 128 tensor-core             */
   int32_t prop_warps;        /* propagation warps per block used (0: the default)       */
   float ms_leaf_tiles;       /* summed device time of the leaf-tile kernel launches     */
-  int64_t reserved[6];
+  int32_t leaf_path;         /* leaf stage that ran: 0 FP32 CUDA cores, 1 tensor cores  */
+  int32_t leaf_fallback;     /* 1: tensor-core precision was asked for, FP32 ran        */
+  int64_t reserved[5];
 } knn_stats;
 
 typedef struct knn_context knn_context;
@@ -142,6 +147,23 @@ knn_context* knn_context_create(int32_t device);
 void knn_context_destroy(knn_context* ctx);
 /* Bytes of device scratch the context currently holds. */
 int64_t knn_context_scratch_bytes(const knn_context* ctx);
+
+/* Outcome of the context's asynchronous calls.  A build given a caller stream,
+ * device outputs and no statistics returns as soon as its work is queued, so a
+ * tensor-core tile wait that gives up inside it cannot change its return
+ * value.  The failure is kept in a per-context error word that only a read
+ * clears: this call waits for `stream` (NULL: the context's own stream), then
+ * returns KNN_ERR_TIMEOUT once for every such failure since the last report,
+ * else KNN_OK.  The next synchronising build on the context reports it too.
+ * ctx NULL: the calling thread's default context of the current device. */
+int knn_context_status(knn_context* ctx, void* stream);
+
+/* Test hook: the next build on `ctx` (NULL: the thread's default context)
+ * starts with its tile-wait error word already set, as if a wait had given
+ * up.  Its tensor-core tile kernels then issue no MMA, free their tensor
+ * memory and return, and the build returns KNN_ERR_TIMEOUT.  One-shot; the
+ * build after it runs normally. */
+int knn_test_fail_next_tile_wait(knn_context* ctx);
 
 /*
  * knn_build -- the drop-in call.  Replaces EuclideanDistanceMatrixGPU::initialize
@@ -262,7 +284,11 @@ int knn_exact_fp64(knn_context* ctx, const void* points, int64_t n, int32_t d, i
  *   stream  cudaStream_t (NULL: legacy default stream); the call returns once
  *           the stream has finished.
  * Results equal knn_exact_fp64's.  The first call on a device looks up the
- * scratch address, so make it before any stream capture.  All calls share the
+ * scratch address, so make it before any stream capture; with CUDA's lazy
+ * module loading that first call is also when the array is reserved on the
+ * device, so a caller that hands its device memory to a pool makes one
+ * warm-up call per device before that (a failed reservation returns
+ * KNN_ERR_OOM).  All calls share the
  * scratch: calls that overlap on the GPU race.  Requests whose scratch exceeds
  * 16 MiB (about 16 bytes per (query, neighbour) pair, plus 8 bytes per point
  * for COSINE) return KNN_ERR_ARGS; so does a query id outside [0, n).

@@ -30,9 +30,10 @@ def test_noalloc_matches_allocating_entry_twice():
     acknn = load_package()
     lib = acknn.load_library()
     rng = np.random.Generator(np.random.PCG64(42))
-    cases = [  # (n, d, k, metric): two calls in a row, different shapes and metrics
+    cases = [  # (n, d, k, metric): calls in a row, different shapes and metrics
         (5000, 24, 10, 0),
         (3000, 7, 16, 2),
+        (4000, 33, 12, 1),
     ]
     for n, d, k, metric in cases:
         x = rng.standard_normal((n, d), dtype=np.float32)
@@ -66,3 +67,31 @@ def test_noalloc_rejects_oversize_and_bad_ids():
     wi, wd = acknn.exact_fp64(x.cpu().numpy(), k, good.cpu().numpy(), 0)
     np.testing.assert_array_equal(gi, wi)
     np.testing.assert_array_equal(gd, wd)
+
+
+def test_noalloc_allocates_no_device_memory():
+    """After a warm-up call, further calls (the same request and a larger one
+    that still fits) leave the device's free memory unchanged: the outputs
+    are the caller's and the scratch is the library's fixed array."""
+    torch = pytest.importorskip("torch")
+    acknn = load_package()
+    lib = acknn.load_library()
+    n, d, k = 20_000, 40, 16
+    x = torch.randn((n, d), dtype=torch.float32, device="cuda")
+    small = torch.arange(0, n, 40, dtype=torch.int64, device="cuda")
+    large = torch.arange(0, n, 4, dtype=torch.int64, device="cuda")
+    outs = {q.numel(): (torch.empty((q.numel(), k), dtype=torch.int32, device="cuda"),
+                        torch.empty((q.numel(), k), dtype=torch.float64, device="cuda")) for q in (small, large)}
+
+    def call(q, metric):
+        oi, od = outs[q.numel()]
+        return lib.knn_exact_fp64_noalloc(x.data_ptr(), n, d, k, metric, q.data_ptr(), q.numel(),
+                                          oi.data_ptr(), od.data_ptr(), None)
+
+    assert call(small, 0) == 0, lib.knn_last_error()  # warm-up: module and scratch set up
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for q, metric in ((small, 0), (large, 1), (large, 2), (small, 0)):
+        assert call(q, metric) == 0, lib.knn_last_error()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
