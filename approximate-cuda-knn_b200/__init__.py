@@ -34,7 +34,7 @@ METRIC_COSINE = 2
 METRICS = {"EUCLIDEAN": 0, "TAXICAB": 1, "COSINE": 2}
 
 F32, F16, BF16 = 0, 1, 2
-PREC_FP32, PREC_BF16_RERANK = 0, 1
+PREC_FP32, PREC_BF16_RERANK, PREC_F16_RERANK = 0, 1, 2
 MAX_K = 128
 MAX_PROPS = 64
 

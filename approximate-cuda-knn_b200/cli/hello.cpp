@@ -21,7 +21,6 @@
 #include <cstring>
 #include <fstream>
 #include <iostream>
-#include <sstream>
 #include <string>
 #include <thread>
 #include <vector>
@@ -44,62 +43,96 @@ void usage() {
                "T, otherwise F\n";
 }
 
-// One CSV point line: tokens split on ',' (empty tokens skipped, as strtok
-// does), each parsed like atof (leading blanks, longest numeric prefix, 0 when
-// none) and narrowed to float; with `klaster` the last token is the cluster id.
+// One CSV point line [s, e): tokens split on ',' (empty tokens skipped, as
+// strtok does), each parsed like atof (leading blanks, longest numeric
+// prefix, 0 when none) and narrowed to float; with `klaster` the last token is
+// the cluster id and is not a feature.  Tokens are copied into a terminated
+// buffer first so that the parse cannot run past the token.
 void parse_line(const char* s, const char* e, int d, bool klaster, float* row) {
-  std::vector<std::pair<const char*, const char*>> toks;
-  const char* p = s;
-  while (p < e) {
+  int ntok = 0;
+  for (const char* p = s; p < e;) {  // tokens on the line
     while (p < e && *p == ',') ++p;
     if (p >= e) break;
+    ++ntok;
+    while (p < e && *p != ',') ++p;
+  }
+  const int nfeat = std::min(klaster && ntok > 0 ? ntok - 1 : ntok, d);
+  char buf[128];
+  const char* p = s;
+  for (int i = 0; i < nfeat; ++i) {
+    while (*p == ',') ++p;
     const char* q = p;
     while (q < e && *q != ',') ++q;
-    toks.emplace_back(p, q);
-    p = q;
-  }
-  size_t nfeat = toks.size();
-  if (klaster && nfeat > 0) --nfeat;
-  char buf[128];
-  for (size_t i = 0; i < nfeat && (int)i < d; ++i) {
-    size_t len = std::min<size_t>(toks[i].second - toks[i].first, sizeof(buf) - 1);
-    std::memcpy(buf, toks[i].first, len);
+    const size_t len = std::min<size_t>(q - p, sizeof(buf) - 1);
+    std::memcpy(buf, p, len);
     buf[len] = 0;
     row[i] = (float)std::atof(buf);
+    p = q;
   }
 }
 
+// The whole file in one buffer; the point lines after the two header lines
+// are cut into one newline-aligned byte range per thread, each thread counts
+// its lines, and after a prefix sum parses them into their rows (at most n;
+// missing lines and values stay 0, as in the reference's zero-filled table).
 bool load_csv(const std::string& path, int64_t n, int d, bool klaster, std::vector<float>& x) {
-  std::ifstream f(path, std::ios::binary);
-  if (!f.is_open()) return false;
-  std::stringstream ss;
-  ss << f.rdbuf();
-  const std::string text = ss.str();
-  // skip the two header lines, then index the point lines
-  size_t pos = 0;
-  for (int h = 0; h < 2 && pos < text.size(); ++h) {
-    size_t nl = text.find('\n', pos);
-    pos = nl == std::string::npos ? text.size() : nl + 1;
+  std::FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) return false;
+  std::vector<char> text;
+  if (std::fseek(f, 0, SEEK_END) == 0) {
+    const long size = std::ftell(f);
+    if (size > 0) text.resize((size_t)size);
+    std::fseek(f, 0, SEEK_SET);
   }
-  std::vector<std::pair<size_t, size_t>> lines;
-  lines.reserve((size_t)n);
-  while (pos < text.size() && (int64_t)lines.size() < n) {
-    size_t nl = text.find('\n', pos);
-    size_t end = nl == std::string::npos ? text.size() : nl;
-    lines.emplace_back(pos, end);
-    pos = end + 1;
+  const size_t got = text.empty() ? 0 : std::fread(text.data(), 1, text.size(), f);
+  std::fclose(f);
+  text.resize(got);
+  const char* const b = text.data();
+  const char* const e = b + text.size();
+  const char* body = b;
+  for (int h = 0; h < 2 && body < e; ++h) {
+    const char* nl = static_cast<const char*>(std::memchr(body, '\n', e - body));
+    body = nl ? nl + 1 : e;
   }
   x.assign((size_t)n * d, 0.0f);
-  const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  const unsigned hw = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+  const size_t span = (size_t)(e - body);
+  std::vector<const char*> cut(hw + 1, e);
+  cut[0] = body;
+  for (unsigned t = 1; t < hw; ++t) {  // range t starts after the newline at or past its share
+    const char* p = body + span * t / hw;
+    if (p < cut[t - 1]) p = cut[t - 1];
+    const char* nl = p > body ? static_cast<const char*>(std::memchr(p - 1, '\n', e - (p - 1))) : nullptr;
+    cut[t] = p == body ? body : (nl ? nl + 1 : e);
+  }
+  auto lines_in = [](const char* p, const char* q) {
+    int64_t c = 0;
+    while (p < q) {
+      const char* nl = static_cast<const char*>(std::memchr(p, '\n', q - p));
+      ++c;
+      p = nl ? nl + 1 : q;
+    }
+    return c;
+  };
+  std::vector<int64_t> first(hw + 1, 0);
+  {
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < hw; ++t)
+      pool.emplace_back([&, t] { first[t + 1] = lines_in(cut[t], cut[t + 1]); });
+    for (auto& th : pool) th.join();
+  }
+  for (unsigned t = 0; t < hw; ++t) first[t + 1] += first[t];
   std::vector<std::thread> pool;
-  const size_t per = (lines.size() + hw - 1) / hw;
   for (unsigned t = 0; t < hw; ++t) {
-    const size_t a = t * per, b = std::min(lines.size(), a + per);
-    if (a >= b) break;
-    pool.emplace_back([&, a, b] {
-      for (size_t i = a; i < b; ++i)
-        parse_line(text.data() + lines[i].first, text.data() + lines[i].second, d, klaster,
-                   x.data() + i * d);
+    if (first[t] >= n) break;
+    pool.emplace_back([&, t] {
+      int64_t row = first[t];
+      for (const char* p = cut[t]; p < cut[t + 1] && row < n; ++row) {
+        const char* nl = static_cast<const char*>(std::memchr(p, '\n', cut[t + 1] - p));
+        const char* q = nl ? nl : cut[t + 1];
+        parse_line(p, q, d, klaster, x.data() + (size_t)row * d);
+        p = nl ? nl + 1 : cut[t + 1];
+      }
     });
   }
   for (auto& th : pool) th.join();
@@ -144,6 +177,8 @@ bool save_result(const std::string& out, const std::vector<int32_t>& idx, const 
 //   ACKNN_PRECISION  fp32 (default) | bf16   leaf blocks in FP32 or BF16 tiles + FP32 re-rank
 //   ACKNN_SPLITS     median (default) | reference | learned
 //   ACKNN_SEED       unsigned integer, default 0
+//   ACKNN_TIMING     1: report the wall time of CSV ingest, build and file
+//                    write on stderr (stdout stays the reference's)
 // An unknown value is reported and fails the initialisation (exit code 8).
 bool env_knobs(knn_options& opt, uint64_t& seed) {
   if (const char* v = std::getenv("ACKNN_PRECISION")) {
@@ -243,11 +278,16 @@ int main(int argc, char** argv) {
   const int d = std::atoi(line.c_str());
   head.close();
 
+  const char* timing_env = std::getenv("ACKNN_TIMING");
+  const bool timing = timing_env && std::string(timing_env) == "1";
+  using clock = std::chrono::steady_clock;
+  const auto t_load = clock::now();
   std::vector<float> x;
   if (devices.empty() || n < 1 || d < 1 || !load_csv(input, n, d, klaster, x)) {
     std::cout << "Initialization failed.\n";
     return 8;
   }
+  const double load_ms = std::chrono::duration<double, std::milli>(clock::now() - t_load).count();
   std::cout << "The datafile has been opened\n";
   std::cout << "I begin analysis.\n";
   knn_options opt;
@@ -272,9 +312,15 @@ int main(int argc, char** argv) {
   }
   std::cout << "The device " << devices[0] << ": has done task in: " << ms << " ms\n";
   std::cout << "I am writing the solution to a file.\n";
+  const auto t_write = clock::now();
   if (!save_result(output, idx, dist, n, k, metric, debug)) {
     std::cout << "Deinitialization failed.\n";
     return 9;
+  }
+  if (timing) {
+    const double write_ms = std::chrono::duration<double, std::milli>(clock::now() - t_write).count();
+    std::fprintf(stderr, "acknn timing: load_ms=%.1f build_ms=%.1f write_ms=%.1f threads=%u\n", load_ms, ms,
+                 write_ms, std::max(1u, std::min(64u, std::thread::hardware_concurrency())));
   }
   std::cout << "The end\n";
   return 0;

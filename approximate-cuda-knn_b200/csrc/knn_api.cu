@@ -208,6 +208,8 @@ inline int round4(int d) { return (d + 3) & ~3; }
 struct Prepared {
   const float* X = nullptr;
   int dpad = 0;
+  const void* Xh = nullptr;  // FP16 input: its rows zero padded to ldh (a multiple of 8), for gathers
+  int ldh = 0;
 };
 
 // Points -> zero-padded float32 rows on the device.
@@ -218,6 +220,10 @@ int prepare_points(knn_context* C, const void* points, int64_t n, int d, const k
   if (ld < d) return fail(KNN_ERR_ARGS, "ld < d");
   P->dpad = dpad;
   const size_t esz = o.dtype == KNN_F32 ? 4 : 2;
+  if (o.dtype == KNN_F16) {
+    P->ldh = (d + 7) & ~7;
+    if (o.points_on_device && ld == d && (d & 7) == 0 && ((uintptr_t)points & 15) == 0) P->Xh = points;
+  }
   if (o.points_on_device) {
     if (o.dtype == KNN_F32 && ld == d && (d & 3) == 0 && ((uintptr_t)points & 15) == 0) {
       P->X = static_cast<const float*>(points);
@@ -229,6 +235,14 @@ int prepare_points(knn_context* C, const void* points, int64_t n, int d, const k
     knn::launch_pad_rows(points, o.dtype, n, d, ld, X, dpad, st);
     log.add();
     P->X = X;
+    if (o.dtype == KNN_F16 && !P->Xh) {
+      void* Xh = nullptr;
+      rc = C->get("Xh", (size_t)n * P->ldh * 2, &Xh);
+      if (rc) return rc;
+      knn::launch_pad_rows_f16(points, n, d, ld, Xh, P->ldh, st);
+      log.add();
+      P->Xh = Xh;
+    }
     return KNN_OK;
   }
   float* X = nullptr;
@@ -246,6 +260,14 @@ int prepare_points(knn_context* C, const void* points, int64_t n, int d, const k
     KNN_CK(cudaMemcpyAsync(stage, points, (size_t)n * ld * esz, cudaMemcpyHostToDevice, st));
     knn::launch_pad_rows(stage, o.dtype, n, d, ld, X, dpad, st);
     log.add();
+    if (o.dtype == KNN_F16) {
+      void* Xh = nullptr;
+      rc = C->get("Xh", (size_t)n * P->ldh * 2, &Xh);
+      if (rc) return rc;
+      knn::launch_pad_rows_f16(stage, n, d, ld, Xh, P->ldh, st);
+      log.add();
+      P->Xh = Xh;
+    }
   }
   P->X = X;
   return KNN_OK;
@@ -359,11 +381,21 @@ int get_lists(knn_context* C, int64_t n, int k, Lists* L) {
 struct Layout {
   knn::SegView segs;
   int64_t leaves = 1, maxleaf = 1;
+  int64_t maxblock = 0;  // bound on the points of a leaf block (0: unknown)
   // reference-rule trees: explicit leaf table (device) and per-tree offsets / counts (host)
   const int64_t* ftable = nullptr;
   const int64_t* foff = nullptr;
   const int64_t* fcount = nullptr;
 };
+
+// Bound on the leaf blocks of a median tree of n points and this depth: node
+// sizes at level l are floor or ceil of n / 2^l, and a leaf climbs at most to
+// the deepest level whose smallest node holds k+1 points.
+int64_t host_max_block(int64_t n, int depth, int k) {
+  int l = depth;
+  while (l > 0 && (n >> l) < k + 1) --l;
+  return (n + (int64_t(1) << l) - 1) >> l;
+}
 
 Layout single_layout(int64_t n, int depth) {
   Layout y;
@@ -407,11 +439,11 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
   return KNN_OK;
 }
 
-// Mixed precision: BF16 tensor-core tiles select each point's best min(2k, 32)
+// Mixed precision: BF16 or FP16 tensor-core tiles select each point's best min(2k, 32)
 // approximate candidates over all trees; FP32 re-rank keeps the exact best k.
 int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, int trees,
-                  const Layout& lay, int metric, const int32_t* perm, const float* norms, Lists* L,
-                  int* err_flag, cudaStream_t st, knn::LaunchLog& log, cudaEvent_t* kev = nullptr) {
+                  const Layout& lay, int metric, int precision, const int32_t* perm, const float* norms,
+                  Lists* L, int* err_flag, cudaStream_t st, knn::LaunchLog& log, cudaEvent_t* kev = nullptr) {
   const int kw = (k + 31) / 32;
   const int kq = k <= 16 ? 2 * k : 32;
   const int Kp = ((d + 63) / 64) * 64;
@@ -426,6 +458,7 @@ int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, in
   a.segs = lay.segs;
   a.leaves = lay.leaves;
   a.maxleaf = lay.maxleaf;
+  a.maxblock = lay.maxblock > 0 ? lay.maxblock : INT64_MAX;
   a.ftable = lay.ftable;
   a.foff = lay.foff;
   a.fcount = lay.fcount;
@@ -437,7 +470,9 @@ int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, in
   a.kev = kev;
   a.rkey = L->key[L->cur];
   a.rid = L->id[L->cur];
+  a.f16 = precision == KNN_PREC_F16_RERANK;
   int rc = C->get("Xb", (size_t)n * Kp * 2, &a.Xb);
+  if (!rc) rc = C->get("maxabs", 1, &a.maxabs);
   if (!rc) rc = C->get("norms2", (size_t)n, &a.norms2);
   if (!rc && trees > 1) rc = C->get("linv", (size_t)n, &a.inv);
   if (!rc) rc = C->get("akey", (size_t)n * kq, &a.akey);
@@ -455,9 +490,11 @@ int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, in
 
 int run_prop(const float* X, int64_t n, int d, int dpad, int k, int metric, const float* norms,
              const int32_t* order, Lists* L, bool with_flags, unsigned long long* counter,
-             cudaStream_t st, knn::LaunchLog& log, int warps = 0) {
+             cudaStream_t st, knn::LaunchLog& log, int warps = 0, const void* Xh = nullptr, int ldh = 0) {
   knn::PropArgs a{};
   a.X = X;
+  a.Xh = Xh;
+  a.ldh = ldh;
   a.n = n;
   a.d = d;
   a.dpad = dpad;
@@ -701,7 +738,7 @@ int resolve_options(const knn_options* opt, knn_options* o) {
     *o = *opt;
   }
   if (o->dtype < 0 || o->dtype > 2) return fail(KNN_ERR_ARGS, "unknown dtype");
-  if (o->precision < 0 || o->precision > 1) return fail(KNN_ERR_ARGS, "unknown precision mode");
+  if (o->precision < 0 || o->precision > 2) return fail(KNN_ERR_ARGS, "unknown precision mode");
   if (o->learned_splits < 0 || o->learned_splits > 1) return fail(KNN_ERR_ARGS, "learned_splits must be 0 or 1");
   if (o->mlp_sample < 0 || o->mlp_steps < 0) return fail(KNN_ERR_ARGS, "negative learned-split setting");
   if (o->autotune < 0 || o->autotune > 1) return fail(KNN_ERR_ARGS, "autotune must be 0 or 1");
@@ -809,9 +846,10 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
   int* err_flag = C->err_words;
   rc = reset_error_word(C, st);
   if (rc) return rc;
-  const bool tensor_leaf = o.precision == KNN_PREC_BF16_RERANK && metric != KNN_METRIC_TAXICAB &&
+  const bool tensor_leaf = o.precision != KNN_PREC_FP32 && metric != KNN_METRIC_TAXICAB &&
                            d <= 256 && k <= 32;
   Layout lay = single_layout(n, T.depth);
+  lay.maxblock = host_max_block(n, T.depth, k);
   if (ftab_d) {
     lay.ftable = ftab_d;
     lay.foff = foff_h.data();
@@ -831,7 +869,8 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
     if (!kev) return fail_cuda(cudaGetLastError(), "event creation");
   }
   if (tensor_leaf) {
-    rc = run_leaf_umma(C, P.X, n, d, P.dpad, k, trees, lay, metric, T.perm, norms, &L, err_flag, st, log, kev);
+    rc = run_leaf_umma(C, P.X, n, d, P.dpad, k, trees, lay, metric, o.precision, T.perm, norms, &L, err_flag, st,
+                       log, kev);
   } else {
     rc = run_leaf(C, P.X, n, d, P.dpad, k, trees, lay, metric, T.perm, norms, &L, stats ? counters : nullptr, st,
                   log, sh.leaf_tile, kev);
@@ -845,7 +884,7 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
 
   for (int p = 0; p < props; ++p) {
     rc = run_prop(P.X, n, d, P.dpad, k, metric, norms, T.perm, &L, true,
-                  stats ? counters + 2 + p : nullptr, st, log, sh.prop_warps);
+                  stats ? counters + 2 + p : nullptr, st, log, sh.prop_warps, P.Xh, P.ldh);
     if (rc) return rc;
   }
   if (timed) KNN_CK(cudaEventRecord(C->ev[4], st));
@@ -910,8 +949,8 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
     stats->launches = log.count;
     stats->props_run = props;
     stats->leaf_tile = tensor_leaf ? 128 : (sh.leaf_tile ? sh.leaf_tile : 64);
-    stats->leaf_path = tensor_leaf ? 1 : 0;
-    stats->leaf_fallback = (o.precision == KNN_PREC_BF16_RERANK && !tensor_leaf) ? 1 : 0;
+    stats->leaf_path = tensor_leaf ? o.precision : 0;
+    stats->leaf_fallback = (o.precision != KNN_PREC_FP32 && !tensor_leaf) ? 1 : 0;
     stats->prop_warps = sh.prop_warps;
     unsigned long long host[2 + KNN_MAX_PROPS];
     KNN_CK(cudaMemcpy(host, counters, sizeof(host), cudaMemcpyDeviceToHost));
@@ -1013,7 +1052,8 @@ int group_compute(knn_context* C, const BatchGroup& g, int k, int trees, int pro
   lay.segs = view;
   lay.leaves = g.leaves;
   lay.maxleaf = g.maxleaf;
-  const bool tensor_leaf = precision == KNN_PREC_BF16_RERANK && metric != KNN_METRIC_TAXICAB && g.d <= 256 &&
+  for (const auto& e : g.hsegs) lay.maxblock = std::max(lay.maxblock, host_max_block(e.n, e.depth, k));
+  const bool tensor_leaf = precision != KNN_PREC_FP32 && metric != KNN_METRIC_TAXICAB && g.d <= 256 &&
                            k <= 32;
   Shapes sh;
   bool tune_prop = false;
@@ -1021,7 +1061,8 @@ int group_compute(knn_context* C, const BatchGroup& g, int k, int trees, int pro
                    st, &sh, &tune_prop);
   if (rc) return rc;
   if (tensor_leaf)
-    rc = run_leaf_umma(C, X, g.ntot, g.d, g.dpad, k, trees, lay, metric, T.perm, norms, &L, err_flag, st, log);
+    rc = run_leaf_umma(C, X, g.ntot, g.d, g.dpad, k, trees, lay, metric, precision, T.perm, norms, &L, err_flag,
+                       st, log);
   else
     rc = run_leaf(C, X, g.ntot, g.d, g.dpad, k, trees, lay, metric, T.perm, norms, &L, nullptr, st, log,
                   sh.leaf_tile);
@@ -1195,10 +1236,9 @@ int batch_impl(knn_context* C, const knn_dataset* sets, int count, int32_t k, in
     stats->props_run = props;
     // per group of equal d: tensor-core tiles when the request allows them
     for (const auto& kv : by_d) {
-      const bool tc = o.precision == KNN_PREC_BF16_RERANK && metric != KNN_METRIC_TAXICAB && kv.first <= 256 &&
-                      k <= 32;
-      if (tc) stats->leaf_path = 1;
-      if (o.precision == KNN_PREC_BF16_RERANK && !tc) stats->leaf_fallback = 1;
+      const bool tc = o.precision != KNN_PREC_FP32 && metric != KNN_METRIC_TAXICAB && kv.first <= 256 && k <= 32;
+      if (tc) stats->leaf_path = o.precision;
+      if (o.precision != KNN_PREC_FP32 && !tc) stats->leaf_fallback = 1;
     }
   }
   return KNN_OK;
@@ -1586,6 +1626,8 @@ int knn_propagate_range(knn_context* ctx, const void* points, int64_t n, int32_t
   if (r1 > r0) {
     knn::PropArgs a{};
     a.X = P.X;
+    a.Xh = P.Xh;
+    a.ldh = P.ldh;
     a.n = n;
     a.d = d;
     a.dpad = P.dpad;

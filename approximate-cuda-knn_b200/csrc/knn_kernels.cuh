@@ -118,9 +118,12 @@ struct UmmaLeafArgs {
   int d, dpad, k, kq, trees, metric;
   SegView segs;
   int64_t leaves, maxleaf;  // leaf blocks per tree; points in the largest leaf
+  int64_t maxblock;         // points in the largest leaf block (median trees)
   const int32_t* perm;   // [trees][n]
   const float* norms;    // [n] FP32 norms (COSINE) or null
-  void* Xb;              // [n][Kp] bf16 scratch (Kp = d rounded up to 64)
+  bool f16;              // operands FP16 (else BF16)
+  void* Xb;              // [n][Kp] 16-bit operand scratch (Kp = d rounded up to 64)
+  unsigned int* maxabs;  // [1] scratch: largest |x| (FP16 EUCLIDEAN row scale)
   float* norms2;         // [n] scratch
   int32_t* inv;          // [n] scratch: a tree's inverse order (null: duplicate checks in the merge)
   cudaEvent_t* kev;      // [2 * trees] events around each tree's tile kernel, or null
@@ -138,6 +141,8 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log);
 
 struct PropArgs {
   const float* X;
+  const void* Xh;            // FP16 rows [n][ldh] (ldh % 8 == 0, zero padded), gathered instead of X; or null
+  int ldh;
   int64_t n;
   int d, dpad, k, metric;
   const float* norms;
@@ -198,6 +203,8 @@ void launch_set_flags(uint32_t* flags, int64_t n, int k, int kw, cudaStream_t st
 void launch_norms(const float* X, int64_t n, int d, int dpad, float* norms, cudaStream_t st);
 void launch_pad_rows(const void* src, int dtype, int64_t n, int d, int64_t ld, float* dst,
                      int dpad, cudaStream_t st);
+// FP16 rows [n][ld] -> zero-padded [n][dh] (dh % 8 == 0), for FP16 gathers.
+void launch_pad_rows_f16(const void* src, int64_t n, int d, int64_t ld, void* dst, int dh, cudaStream_t st);
 void launch_finalize(const float* key, const uint32_t* id, int64_t n, int k, int metric,
                      float* out_dist, int32_t* out_idx, cudaStream_t st);
 void launch_keys_from_dist(const float* dist, int64_t count, int metric, float* key,

@@ -53,6 +53,16 @@ __global__ void k_pad_rows(const T* __restrict__ src, int64_t n, int d, int64_t 
   dst[g] = c < d ? to_f32<T>(src[i * ld + c]) : 0.0f;
 }
 
+// FP16 rows [n][ld] -> [n][dh] (dh % 8 == 0), zero padded.
+__global__ void k_pad_rows_f16(const __half* __restrict__ src, int64_t n, int d, int64_t ld,
+                               __half* __restrict__ dst, int dh) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n * dh) return;
+  const int64_t i = g / dh;
+  const int c = (int)(g - i * dh);
+  dst[g] = c < d ? src[i * ld + c] : __float2half_rn(0.0f);
+}
+
 // Rows of many device point sets into one padded float32 array: block (x, y)
 // copies rows y, y + gridDim.y, ... of set x.
 template <typename T>
@@ -176,6 +186,10 @@ void launch_pad_rows(const void* src, int dtype, int64_t n, int d, int64_t ld, f
     k_pad_rows<__nv_bfloat16><<<b, 256, 0, st>>>(static_cast<const __nv_bfloat16*>(src), n, d, ld, dst, dpad);
   else
     k_pad_rows<float><<<b, 256, 0, st>>>(static_cast<const float*>(src), n, d, ld, dst, dpad);
+}
+void launch_pad_rows_f16(const void* src, int64_t n, int d, int64_t ld, void* dst, int dh, cudaStream_t st) {
+  k_pad_rows_f16<<<blocks_for(n * dh, 256), 256, 0, st>>>(static_cast<const __half*>(src), n, d, ld,
+                                                           static_cast<__half*>(dst), dh);
 }
 void launch_finalize(const float* key, const uint32_t* id, int64_t n, int k, int metric,
                      float* out_dist, int32_t* out_idx, cudaStream_t st) {

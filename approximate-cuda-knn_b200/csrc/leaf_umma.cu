@@ -29,6 +29,7 @@
 //     and insert them into the query's sorted list (held in shared memory for
 //     the whole block) with one ballot and one lane shift each.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
 
@@ -62,10 +63,13 @@ constexpr int kLS = 33;              // list row stride (row owners hit distinct
 // sleeps (a few ms) is far beyond that, and keeps a failing launch short.
 constexpr uint32_t kSpinLimit = 1u << 16;
 
-// Instruction descriptor: D f32 (bits 4-5 = 1), A bf16 (7-9 = 1), B bf16
-// (10-12 = 1), A and B K-major (15, 16 = 0), N>>3 at 17-22, M>>4 at 24-28.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kBN >> 3) << 17) |
-                            ((uint32_t)(kBM >> 4) << 24);
+// Instruction descriptor of kind::f16: D f32 (bits 4-5 = 1), A and B format
+// at 7-9 and 10-12 (0 f16, 1 bf16; A and B always the same type), A and B
+// K-major (15, 16 = 0), N>>3 at 17-22, M>>4 at 24-28.
+constexpr uint32_t idesc_for(bool f16) {
+  return (1u << 4) | ((f16 ? 0u : 1u) << 7) | ((f16 ? 0u : 1u) << 10) | ((uint32_t)(kBN >> 3) << 17) |
+         ((uint32_t)(kBM >> 4) << 24);
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -123,12 +127,13 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
   return false;
 }
 
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                         uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
@@ -159,7 +164,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 
 // Stage `rows` gathered rows (ids in `ids`, <0: zero row) of the BF16 copy into
 // a K-major 128B-swizzled operand of Kp/64 chunks.
-__device__ __forceinline__ void stage_operand(unsigned char* op, const __nv_bfloat16* __restrict__ Xb,
+__device__ __forceinline__ void stage_operand(unsigned char* op, const uint16_t* __restrict__ Xb,
                                               int Kp, const int32_t* ids) {
   const int units = kBM * (Kp / 8);  // 16-byte units
   const uint32_t base = smem_u32(op);
@@ -169,7 +174,7 @@ __device__ __forceinline__ void stage_operand(unsigned char* op, const __nv_bflo
     const int chunk = c16 >> 3, w = c16 & 7;
     const uint32_t dst = base + chunk * kChunkBytes + r * 128 + ((w ^ (r & 7)) << 4);
     const int32_t id = ids[r];
-    const __nv_bfloat16* src = Xb + (size_t)(id < 0 ? 0 : id) * Kp + c16 * 8;
+    const uint16_t* src = Xb + (size_t)(id < 0 ? 0 : id) * Kp + c16 * 8;
     cp_async16(dst, src, id < 0 ? 0 : 16);
   }
   asm volatile("cp.async.commit_group;\n" ::);
@@ -223,8 +228,8 @@ __device__ __forceinline__ uint32_t warp_sort32_u32(uint32_t v) {
 // cannot come back.
 template <int METRIC, bool FIRST>
 __global__ void __launch_bounds__(kUThreads, 2)
-    k_leaf_tc(const __nv_bfloat16* __restrict__ Xb, int Kp, SegView segs, const int64_t* __restrict__ ftab, int k,
-              int kq,
+    k_leaf_tc(const uint16_t* __restrict__ Xb, uint32_t idesc, int Kp, SegView segs,
+              const int64_t* __restrict__ ftab, int k, int kq,
               int qtiles, const int32_t* __restrict__ perm, const int32_t* __restrict__ inv,
               const float* __restrict__ norms2, float* __restrict__ akey, uint32_t* __restrict__ aid,
               int* __restrict__ err) {
@@ -268,7 +273,9 @@ __global__ void __launch_bounds__(kUThreads, 2)
   const int mq = min(kBM, nq - q0);
   const int nb = (int)(bhi - blo);
   const int ntiles = (nb + kBN - 1) / kBN;
-  const bool xcl = !FIRST && inv != nullptr && nb <= kXMaxBlock;  // block-uniform
+  // Listed ids are located up front only in blocks of several tiles: in a
+  // one-tile block the few survivors are cheaper to check by the merge's ballot.
+  const bool xcl = !FIRST && inv != nullptr && nb > kBN && nb <= kXMaxBlock;  // block-uniform
   const bool pre = FIRST && nb >= kPrepassMin;
   const int nsteps = pre ? 2 * ntiles : ntiles;
   const float kInf = __int_as_float(0x7F800000);
@@ -387,7 +394,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
 #pragma unroll
       for (int kk = 0; kk < kKC / 16; ++kk) {
         const uint32_t off = ch * kChunkBytes + kk * 32;
-        umma_bf16(d, desc_sw128(a0 + off), desc_sw128(b0 + off), (ch | kk) != 0 ? 1u : 0u);
+        umma_f16(d, desc_sw128(a0 + off), desc_sw128(b0 + off), idesc, (ch | kk) != 0 ? 1u : 0u);
       }
     umma_commit(bar);
   };
@@ -657,11 +664,31 @@ __global__ void k_inverse_order(const int32_t* __restrict__ order, int64_t n, in
     inv[order[i]] = (int32_t)i;
 }
 
-// BF16 operand copy: rows of Kp bf16 (zero padded), COSINE rows divided by
-// their FP32 norm first; norms2 = |row|^2 of the BF16 values (EUCLIDEAN).
-__global__ void k_to_bf16(const float* __restrict__ X, int64_t n, int d, int dpad, int Kp, int metric,
-                          const float* __restrict__ norms, __nv_bfloat16* __restrict__ Xb,
-                          float* __restrict__ norms2) {
+// Largest |x| over the rows (non-negative floats order as their bit patterns).
+__global__ void k_max_abs(const float* __restrict__ X, int64_t count, unsigned int* __restrict__ out) {
+  float m = 0.f;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+    m = fmaxf(m, fabsf(X[i]));
+  m = __uint_as_float(__reduce_max_sync(0xFFFFFFFFu, __float_as_uint(m)));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+__device__ __forceinline__ uint16_t to_operand(float v, bool f16) {
+  return f16 ? __half_as_ushort(__float2half_rn(v)) : __bfloat16_as_ushort(__float2bfloat16_rn(v));
+}
+__device__ __forceinline__ float from_operand(uint16_t b, bool f16) {
+  return f16 ? __half2float(__ushort_as_half(b)) : __bfloat162float(__ushort_as_bfloat16(b));
+}
+
+// 16-bit operand copy: rows of Kp BF16 or FP16 values (zero padded), COSINE
+// rows divided by their FP32 norm first; norms2 = |row|^2 of the rounded
+// values (EUCLIDEAN).  FP16 EUCLIDEAN rows are first multiplied by the power
+// of two 2^e that brings the largest |x| (maxabs) into [2^14, 2^15), inside
+// the FP16 range: a power-of-two scale is exact, scales every key of the tile
+// stage by the same 2^2e and so keeps its ranking (the re-rank uses X).
+__global__ void k_to_operand(const float* __restrict__ X, int64_t n, int d, int dpad, int Kp, int metric, bool f16,
+                             const unsigned int* __restrict__ maxabs, const float* __restrict__ norms,
+                             uint16_t* __restrict__ Xb, float* __restrict__ norms2) {
   const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (row >= n) return;
@@ -669,13 +696,22 @@ __global__ void k_to_bf16(const float* __restrict__ X, int64_t n, int d, int dpa
   if (metric == KNN_METRIC_COSINE) {
     const float nr = norms[row];
     scale = nr > 0.f ? __frcp_rn(nr) : 0.f;
+  } else if (f16) {
+    const float m = __uint_as_float(*maxabs);
+    int e = 0;
+    if (m > 0.f && m < __int_as_float(0x7F800000)) {
+      frexpf(m, &e);  // m in [2^(e-1), 2^e)
+      e = 15 - e;     // m * 2^(15-e) in [2^14, 2^15)
+      e = max(-126, min(126, e));
+    }
+    scale = ldexpf(1.f, e);
   }
   float s = 0.f;
   for (int c = lane; c < Kp; c += 32) {
     const float v = c < d ? X[(size_t)row * dpad + c] : 0.f;
-    const __nv_bfloat16 b = __float2bfloat16_rn(metric == KNN_METRIC_COSINE ? __fmul_rn(v, scale) : v);
+    const uint16_t b = to_operand(__fmul_rn(v, scale), f16);
     Xb[(size_t)row * Kp + c] = b;
-    const float f = __bfloat162float(b);
+    const float f = from_operand(b, f16);
     s = __fmaf_rn(f, f, s);
   }
 #pragma unroll
@@ -758,11 +794,18 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
   const int Kp = ((a.d + kKC - 1) / kKC) * kKC;
   if (Kp > 256 || a.kq > 32 || a.kq < a.k) return KNN_ERR_UNSUPPORTED;
   cudaStream_t st = a.stream;
-  __nv_bfloat16* Xb = static_cast<__nv_bfloat16*>(a.Xb);
-  // operand copy
-  k_to_bf16<<<(unsigned)((a.n * 32 + 255) / 256), 256, 0, st>>>(a.X, a.n, a.d, a.dpad, Kp, a.metric,
-                                                                 a.norms, Xb, a.norms2);
+  uint16_t* Xb = static_cast<uint16_t*>(a.Xb);
+  // operand copy (FP16 EUCLIDEAN: the largest |x| first, for the row scale)
+  if (a.f16 && a.metric == KNN_METRIC_EUCLIDEAN) {
+    cudaMemsetAsync(a.maxabs, 0, sizeof(unsigned int), st);
+    const int64_t cnt = a.n * (int64_t)a.dpad;
+    k_max_abs<<<(unsigned)std::min<int64_t>((cnt + 255) / 256, 148 * 8), 256, 0, st>>>(a.X, cnt, a.maxabs);
+    log.add();
+  }
+  k_to_operand<<<(unsigned)((a.n * 32 + 255) / 256), 256, 0, st>>>(a.X, a.n, a.d, a.dpad, Kp, a.metric, a.f16,
+                                                                    a.maxabs, a.norms, Xb, a.norms2);
   log.add();
+  const uint32_t idesc = idesc_for(a.f16);
   const size_t smem = umma_smem_bytes(Kp);
   const int64_t leaves = a.leaves;
   const int qtiles = (int)((a.maxleaf + kBM - 1) / kBM);
@@ -779,7 +822,7 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
     }
     const unsigned grid = (unsigned)(tleaves * qtiles);
     const int32_t* inv = nullptr;
-    if (t > 0 && a.inv) {
+    if (t > 0 && a.inv && (a.ftable || a.maxblock > kBN)) {
       k_inverse_order<<<(unsigned)std::min<int64_t>((a.n + 255) / 256, 148 * 16), 256, 0, st>>>(perm, a.n, a.inv);
       log.add();
       inv = a.inv;
@@ -787,7 +830,7 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
 #define KNN_TC_LAUNCH(M, F)                                                                               \
   do {                                                                                                    \
     cudaFuncSetAttribute(k_leaf_tc<M, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);       \
-    k_leaf_tc<M, F><<<grid, kUThreads, smem, st>>>(Xb, Kp, a.segs, ftab, a.k, a.kq, qtiles, perm, inv, a.norms2, \
+    k_leaf_tc<M, F><<<grid, kUThreads, smem, st>>>(Xb, idesc, Kp, a.segs, ftab, a.k, a.kq, qtiles, perm, inv, a.norms2, \
                                                    a.akey, a.aid, a.err);                                \
   } while (0)
     if (a.kev) cudaEventRecord(a.kev[2 * t], st);

@@ -4,17 +4,26 @@
 // (euclideandistancematrixgpu.cu:1033-1935, :1937-1977).  The reference marks
 // N(N(i)) in an N-byte bitmap per point, clears N(i) and i, scans the bitmap and
 // histogram-selects; here one warp owns one point:
-//   * candidates come from the k lists of its neighbours (coalesced 4k-byte
-//     reads) and are deduplicated in a per-warp shared-memory hash set that
-//     is seeded with i and N(i);
-//   * candidate rows are staged 64 dims at a time into shared memory with
-//     cp.async (16-byte, xor-swizzled so the per-lane row reads are
-//     conflict-free) and each lane computes one key in the reference's order;
-//   * survivors are merged into the warp-held sorted list (bitonic via shuffles).
+//   * the k x k neighbour-of-neighbour ids are read all at once (four loads in
+//     flight per lane), deduplicated in a per-warp shared-memory hash set
+//     seeded with i and N(i), and compacted into a candidate array;
+//   * the candidates' rows stream through a two-slot cp.async pipeline in
+//     256-byte row slices (32 rows per stage, xor-swizzled so the per-lane
+//     row reads are conflict-free): stage t+1 is in flight while stage t is
+//     summed, across batch boundaries too; FP16 inputs are gathered as FP16
+//     (the conversion to FP32 is exact, so the keys are unchanged);
+//   * each lane computes one key in the reference's order and the batch's
+//     survivors are merged into the warp-held sorted list (bitonic via shuffles).
 // "New" flags: a pair (a, j) is skipped when a was already in N(i) and j already
 // in N(a) before the previous step.  Such a j was a candidate of i in that step
 // and lost to k better entries (or is listed), and N(i) only improves, so it
-// cannot enter now: the result is identical to evaluating every pair.
+// cannot enter now: the result is identical to evaluating every pair.  The
+// candidate set does not depend on the order of discovery, and the list keeps
+// the k best of the set by (key, id), so the result does not either.
+#include <cuda_fp16.h>
+
+#include <type_traits>
+
 #include "knn_internal.cuh"
 #include "knn_kernels.cuh"
 
@@ -23,7 +32,8 @@ namespace knn {
 namespace {
 constexpr int kPropMaxWarps = 8;
 constexpr size_t kPropSmemBudget = 200 * 1024;
-constexpr int kDCH = 64;  // dims staged per chunk (16 float4)
+constexpr int kSliceBytes = 256;  // bytes of one candidate row per pipeline stage (16 x 16 B)
+constexpr int kGatherUnroll = 4;  // neighbour-list entries in flight per lane
 
 __device__ __forceinline__ bool hash_insert(int32_t* H, int hbits, int32_t id) {
   const uint32_t size = 1u << hbits;
@@ -41,10 +51,13 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src
   const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
 }
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\n" ::);
-  asm volatile("cp.async.wait_group 0;\n" ::);
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
+
+inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
 }  // namespace
 
@@ -55,33 +68,44 @@ int prop_hash_bits(int k) {
   return b;
 }
 
-size_t prop_warp_bytes(int k, int dpad) {
-  const size_t h = (size_t)4 << prop_hash_bits(k);
-  const size_t q = 64 * 4;
-  const size_t xq = (size_t)dpad * 4;
-  const size_t rows = 32 * kDCH * 4;
-  size_t b = h + q + xq + rows;
+// hash set | candidates [k*k] | N(i) ids and flags | query row (float, d
+// rounded to 8) | two row-slice buffers
+size_t prop_warp_bytes(int k, int d) {
+  size_t b = ((size_t)4 << prop_hash_bits(k)) + (size_t)4 * round_up(k * k, 32) + (size_t)8 * round_up(k, 32) +
+             (size_t)4 * round_up(d, 8) + (size_t)2 * 32 * kSliceBytes;
   return (b + 15) & ~(size_t)15;
 }
 
-template <int METRIC, int KPL>
+// HALF: rows are FP16 [n][ldr] (ldr % 8 == 0), else float32 [n][ldr] (ldr % 4 == 0);
+// zero padded beyond d.
+template <int METRIC, int KPL, bool HALF>
 __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
-    const float* __restrict__ X, int64_t n, int64_t r0, int64_t cnt, int d, int dpad, int k, int kw, int hbits,
+    const void* __restrict__ Xrows, int ldr, int64_t n, int64_t r0, int64_t cnt, int d, int k, int kw, int hbits,
     size_t warp_bytes, const float* __restrict__ norms, const int32_t* __restrict__ order,
     const float* __restrict__ key_in, const uint32_t* __restrict__ id_in,
     const uint32_t* __restrict__ flags_in, float* __restrict__ key_out,
     uint32_t* __restrict__ id_out, uint32_t* __restrict__ flags_out,
     unsigned long long* __restrict__ cand_counter) {
+  using Elem = typename std::conditional<HALF, __half, float>::type;
+  constexpr int kEPU = 16 / sizeof(Elem);            // elements per 16-byte unit
+  constexpr int kCH = kSliceBytes / sizeof(Elem);    // dims per row slice (divides 256)
   extern __shared__ __align__(16) unsigned char smem[];
+  const Elem* X = static_cast<const Elem*>(Xrows);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char* base = smem + (size_t)warp * warp_bytes;
   const int hsize = 1 << hbits;
+  const int kk = k * k;
+  const int kr = (k + 31) & ~31;
+  const int dq = (d + 7) & ~7;
   int32_t* H = reinterpret_cast<int32_t*>(base);
   uint32_t* Q = reinterpret_cast<uint32_t*>(base + (size_t)4 * hsize);
-  float* xq = reinterpret_cast<float*>(base + (size_t)4 * hsize + 256);
-  float* rows = xq + dpad;
+  uint32_t* nbid = Q + ((kk + 31) & ~31);
+  uint32_t* nbfl = nbid + kr;
+  float* xq = reinterpret_cast<float*>(nbfl + kr);
+  unsigned char* rows = reinterpret_cast<unsigned char*>(xq + dq);  // [2][32][kSliceBytes]
   const float kInf = __int_as_float(0x7F800000);
   const uint32_t lt_mask = (1u << lane) - 1u;
+  const int nch = (d + kCH - 1) / kCH;
   unsigned long long evaluated = 0;
 
   const int wpb = blockDim.x >> 5;
@@ -90,11 +114,10 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
   for (int64_t w = (int64_t)blockIdx.x * wpb + warp; w < cnt; w += nwarps) {
     const int32_t i = order ? order[r0 + w] : (int32_t)(r0 + w);
     WarpList<KPL> L;
-    uint32_t oid[KPL];
-    bool oflag[KPL];
 #pragma unroll
     for (int r = 0; r < KPL; ++r) {
       const int e = r * 32 + lane;
+      uint32_t nid = kNoId, nfl = 0;
       if (e < k) {
         L.key[r] = key_in[(size_t)i * k + e];
         // an id outside [0, n) is an empty entry: kept out of the list and
@@ -103,110 +126,132 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
         const bool ok = u < (uint64_t)n;
         L.key[r] = ok ? L.key[r] : kInf;
         L.id[r] = ok ? u : kNoId;
-        oid[r] = ok ? u : kNoId;
-        oflag[r] = flags_in ? ((flags_in[(size_t)i * kw + r] >> lane) & 1u) : true;
+        nid = ok ? u : kNoId;
+        nfl = flags_in ? ((flags_in[(size_t)i * kw + r] >> lane) & 1u) : 1u;
       } else {
         L.key[r] = kInf;
         L.id[r] = kNoId;
-        oid[r] = kNoId;
-        oflag[r] = false;
+      }
+      if (e < kr) {
+        nbid[e] = nid;
+        nbfl[e] = nfl;
       }
     }
     for (int s = lane; s < hsize; s += 32) H[s] = -1;
-    const float4* xr = reinterpret_cast<const float4*>(X + (size_t)i * dpad);
-    for (int c = lane; c < (dpad >> 2); c += 32) reinterpret_cast<float4*>(xq)[c] = __ldg(xr + c);
+    {
+      const Elem* xr = X + (size_t)i * ldr;
+      for (int c = lane; c < dq; c += 32) xq[c] = c < d ? (float)xr[c] : 0.f;
+    }
     __syncwarp();
     if (lane == 0) hash_insert(H, hbits, i);
 #pragma unroll
     for (int r = 0; r < KPL; ++r)
-      if (r * 32 + lane < k && oid[r] != kNoId) hash_insert(H, hbits, (int32_t)oid[r]);
+      if (r * 32 + lane < k && L.id[r] != kNoId) hash_insert(H, hbits, (int32_t)L.id[r]);
     __syncwarp();
     const float ni = (METRIC == KNN_METRIC_COSINE) ? norms[i] : 0.f;
 
+    // candidates: entry (s, t) of the flattened k x k neighbour lists, lane-strided
     int qn = 0;
-    auto process = [&](int m) {
-      // keys of the m queued candidates, one per lane
-      const int32_t cj = lane < m ? (int32_t)Q[lane] : 0;
-      float total = 0.f, part = 0.f;
-      for (int cd = 0; cd < d; cd += kDCH) {
-        // stage rows: 16 float4 per row, 2 rows per warp step
-        const int half = lane >> 4, c4 = lane & 15;
-        const int dim = cd + 4 * c4;
-        for (int r = half; r < m; r += 2) {
-          const int32_t jid = (int32_t)Q[r];
-          const float* src = X + (size_t)jid * dpad + (dim < dpad ? dim : 0);
-          float* dst = rows + r * kDCH + ((c4 ^ (r & 7)) << 2);
-          cp_async16(dst, src, dim < dpad ? 16 : 0);
+    for (int e0 = 0; e0 < kk; e0 += 32 * kGatherUnroll) {
+      uint32_t jj[kGatherUnroll];
+      bool ok[kGatherUnroll];
+#pragma unroll
+      for (int u = 0; u < kGatherUnroll; ++u) {
+        const int e = e0 + u * 32 + lane;
+        jj[u] = 0;
+        ok[u] = false;
+        if (e < kk) {
+          const int s = e / k, t = e - s * k;
+          const uint32_t a = nbid[s];
+          if (a != kNoId) {
+            jj[u] = id_in[(size_t)a * k + t] & kIdMask;
+            const bool jf = flags_in ? ((flags_in[(size_t)a * kw + (t >> 5)] >> (t & 31)) & 1u) : true;
+            ok[u] = (nbfl[s] != 0 || jf) && (int64_t)jj[u] < n;
+          }
         }
-        cp_async_wait_all();
-        __syncwarp();
-        if (lane < m) {
-          const float* myrow = rows + lane * kDCH;
-          const int lim = min(kDCH, d - cd);
-          for (int q4 = 0; q4 < (lim + 3) >> 2; ++q4) {
-            const float4 cv = *reinterpret_cast<const float4*>(myrow + ((q4 ^ (lane & 7)) << 2));
-            const float4 qv = *reinterpret_cast<const float4*>(xq + cd + 4 * q4);
+      }
+#pragma unroll
+      for (int u = 0; u < kGatherUnroll; ++u) {
+        const bool cand = ok[u] && hash_insert(H, hbits, (int32_t)jj[u]);
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, cand);
+        if (cand) Q[qn + __popc(bal & lt_mask)] = jj[u];
+        qn += __popc(bal);
+      }
+    }
+    __syncwarp();
+
+    // keys of the candidates, 32 per batch, row slices through two buffers
+    const int stages = ((qn + 31) >> 5) * nch;
+    auto issue = [&](int t) {
+      const int b = t / nch, c = t - b * nch;
+      const int m = min(32, qn - 32 * b);
+      const int half = lane >> 4, c16 = lane & 15;
+      const int dim = c * kCH + kEPU * c16;
+      unsigned char* buf = rows + (size_t)(t & 1) * 32 * kSliceBytes;
+      for (int r = half; r < m; r += 2) {
+        const uint32_t jid = Q[32 * b + r];
+        const Elem* src = X + (size_t)jid * ldr + (dim < ldr ? dim : 0);
+        cp_async16(buf + r * kSliceBytes + ((c16 ^ (r & 7)) << 4), src, dim < ldr ? 16 : 0);
+      }
+      cp_async_commit();
+    };
+    if (stages > 0) issue(0);
+    float total = 0.f, part = 0.f;
+    for (int t = 0; t < stages; ++t) {
+      if (t + 1 < stages) {
+        issue(t + 1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncwarp();
+      const int b = t / nch, c = t - b * nch;
+      const int m = min(32, qn - 32 * b);
+      const int cd = c * kCH;
+      if (lane < m) {
+        const unsigned char* myrow = rows + (size_t)(t & 1) * 32 * kSliceBytes + lane * kSliceBytes;
+        const int lim = min(kCH, d - cd);
+        for (int q = 0; q < (lim + kEPU - 1) / kEPU; ++q) {
+          const uint4 raw = *reinterpret_cast<const uint4*>(myrow + ((q ^ (lane & 7)) << 4));
+          const float* qx = xq + cd + kEPU * q;
+          if (HALF) {
+            const __half2* h2 = reinterpret_cast<const __half2*>(&raw);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const float2 cv = __half22float2(h2[e]);
+              part = acc_step<METRIC>(qx[2 * e], cv.x, part);
+              part = acc_step<METRIC>(qx[2 * e + 1], cv.y, part);
+            }
+          } else {
+            const float4 cv = *reinterpret_cast<const float4*>(&raw);
+            const float4 qv = *reinterpret_cast<const float4*>(qx);
             part = acc_step<METRIC>(qv.x, cv.x, part);
             part = acc_step<METRIC>(qv.y, cv.y, part);
             part = acc_step<METRIC>(qv.z, cv.z, part);
             part = acc_step<METRIC>(qv.w, cv.w, part);
           }
-          if (((cd + kDCH) & 255) == 0 || cd + kDCH >= d) {
-            total = __fadd_rn(total, part);
-            part = 0.f;
-          }
         }
-        __syncwarp();
+        if (((cd + kCH) & 255) == 0 || cd + kCH >= d) {
+          total = __fadd_rn(total, part);
+          part = 0.f;
+        }
       }
-      float key = total;
-      if (METRIC == KNN_METRIC_COSINE) key = lane < m ? cosine_key(total, ni, norms[cj]) : kInf;
-      float tk;
-      uint32_t ti;
-      warp_list_get(L, k - 1, tk, ti);
-      const bool pass = lane < m && cand_less(key, (uint32_t)cj, tk, ti);
-      if (lane == 0) evaluated += (unsigned long long)m;
-      if (__any_sync(0xFFFFFFFFu, pass))
-        warp_list_insert(L, pass ? key : kInf, pass ? ((uint32_t)cj | 0x80000000u) : kNoId);
-    };
-
-    for (int s = 0; s < k; ++s) {
-      // entry s of the old list and its flag, broadcast
-      const int rr = s >> 5, src = s & 31;
-      uint32_t av = 0;
-      int fv = 0;
-#pragma unroll
-      for (int r = 0; r < KPL; ++r)
-        if (r == rr) {
-          av = oid[r];
-          fv = oflag[r] ? 1 : 0;
-        }
-      const uint32_t a = __shfl_sync(0xFFFFFFFFu, av, src);
-      const bool af = __shfl_sync(0xFFFFFFFFu, fv, src) != 0;
-      if (a == kNoId) continue;  // warp-uniform
-      for (int r0 = 0; r0 < k; r0 += 32) {
-        const int e = r0 + lane;
-        bool cand = false;
-        int32_t jj = 0;
-        if (e < k) {
-          jj = (int32_t)(id_in[(size_t)a * k + e] & kIdMask);
-          const bool jf = flags_in ? ((flags_in[(size_t)a * kw + (r0 >> 5)] >> lane) & 1u) : true;
-          cand = (af || jf) && (int64_t)jj < n && hash_insert(H, hbits, jj);
-        }
-        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, cand);
-        if (cand) Q[qn + __popc(bal & lt_mask)] = (uint32_t)jj;
-        qn += __popc(bal);
-        __syncwarp();
-        if (qn >= 32) {
-          process(32);
-          const uint32_t carry = lane < qn - 32 ? Q[32 + lane] : 0;
-          __syncwarp();
-          if (lane < qn - 32) Q[lane] = carry;
-          qn -= 32;
-          __syncwarp();
-        }
+      __syncwarp();  // the slot is refilled by stage t + 2
+      if (c == nch - 1) {
+        const int32_t cj = lane < m ? (int32_t)Q[32 * b + lane] : 0;
+        float key = total;
+        if (METRIC == KNN_METRIC_COSINE) key = lane < m ? cosine_key(total, ni, norms[cj]) : kInf;
+        float tk;
+        uint32_t ti;
+        warp_list_get(L, k - 1, tk, ti);
+        const bool pass = lane < m && cand_less(key, (uint32_t)cj, tk, ti);
+        if (lane == 0) evaluated += (unsigned long long)m;
+        if (__any_sync(0xFFFFFFFFu, pass))
+          warp_list_insert(L, pass ? key : kInf, pass ? ((uint32_t)cj | 0x80000000u) : kNoId);
+        total = 0.f;
+        part = 0.f;
       }
     }
-    if (qn > 0) process(qn);
 
 #pragma unroll
     for (int r = 0; r < KPL; ++r) {
@@ -223,19 +268,20 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
   if (cand_counter && lane == 0 && evaluated) atomicAdd(cand_counter, evaluated);
 }
 
-template <int METRIC>
-static void launch_prop_metric(const PropArgs& a, int kpl, int hbits, size_t wb, int wpb,
-                               unsigned grid) {
+template <int METRIC, bool HALF>
+static void launch_prop_metric(const PropArgs& a, int kpl, int hbits, size_t wb, int wpb, unsigned grid) {
   const int kw = (a.k + 31) / 32;
   const int64_t r0 = a.r0, cnt = (a.r1 > 0 ? a.r1 : a.n) - a.r0;
   const size_t smem = wb * wpb;
-#define KNN_PROP_LAUNCH(KP)                                                                       \
-  do {                                                                                            \
-    cudaFuncSetAttribute(k_propagate<METRIC, KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
-                         (int)kPropSmemBudget);                                                   \
-    k_propagate<METRIC, KP><<<grid, wpb * 32, smem, a.stream>>>(                                  \
-        a.X, a.n, r0, cnt, a.d, a.dpad, a.k, kw, hbits, wb, a.norms, a.order, a.key_in, a.id_in,  \
-        a.flags_in, a.key_out, a.id_out, a.flags_out, a.cand_counter);                            \
+  const void* rows = HALF ? static_cast<const void*>(a.Xh) : static_cast<const void*>(a.X);
+  const int ldr = HALF ? a.ldh : a.dpad;
+#define KNN_PROP_LAUNCH(KP)                                                                         \
+  do {                                                                                              \
+    cudaFuncSetAttribute(k_propagate<METRIC, KP, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                         (int)kPropSmemBudget);                                                     \
+    k_propagate<METRIC, KP, HALF><<<grid, wpb * 32, smem, a.stream>>>(                              \
+        rows, ldr, a.n, r0, cnt, a.d, a.k, kw, hbits, wb, a.norms, a.order, a.key_in, a.id_in,      \
+        a.flags_in, a.key_out, a.id_out, a.flags_out, a.cand_counter);                              \
   } while (0)
   if (kpl == 1) KNN_PROP_LAUNCH(1);
   else if (kpl == 2) KNN_PROP_LAUNCH(2);
@@ -243,10 +289,16 @@ static void launch_prop_metric(const PropArgs& a, int kpl, int hbits, size_t wb,
 #undef KNN_PROP_LAUNCH
 }
 
+template <int METRIC>
+static void launch_prop_rows(const PropArgs& a, int kpl, int hbits, size_t wb, int wpb, unsigned grid) {
+  if (a.Xh) launch_prop_metric<METRIC, true>(a, kpl, hbits, wb, wpb, grid);
+  else launch_prop_metric<METRIC, false>(a, kpl, hbits, wb, wpb, grid);
+}
+
 int propagate_step(const PropArgs& a, LaunchLog& log) {
   const int kpl = kpl_for(a.k);
   const int hbits = prop_hash_bits(a.k);
-  const size_t wb = prop_warp_bytes(a.k, a.dpad);
+  const size_t wb = prop_warp_bytes(a.k, a.d);
   int wpb = (int)(kPropSmemBudget / wb);
   if (wpb > kPropMaxWarps) wpb = kPropMaxWarps;
   if (wpb < 1) return KNN_ERR_UNSUPPORTED;
@@ -261,9 +313,9 @@ int propagate_step(const PropArgs& a, LaunchLog& log) {
   const int64_t want = (cnt + wpb - 1) / wpb;
   const int64_t cap = (int64_t)sms * per_sm;
   const unsigned grid = (unsigned)(want < cap ? want : cap);
-  if (a.metric == KNN_METRIC_EUCLIDEAN) launch_prop_metric<KNN_METRIC_EUCLIDEAN>(a, kpl, hbits, wb, wpb, grid);
-  else if (a.metric == KNN_METRIC_TAXICAB) launch_prop_metric<KNN_METRIC_TAXICAB>(a, kpl, hbits, wb, wpb, grid);
-  else launch_prop_metric<KNN_METRIC_COSINE>(a, kpl, hbits, wb, wpb, grid);
+  if (a.metric == KNN_METRIC_EUCLIDEAN) launch_prop_rows<KNN_METRIC_EUCLIDEAN>(a, kpl, hbits, wb, wpb, grid);
+  else if (a.metric == KNN_METRIC_TAXICAB) launch_prop_rows<KNN_METRIC_TAXICAB>(a, kpl, hbits, wb, wpb, grid);
+  else launch_prop_rows<KNN_METRIC_COSINE>(a, kpl, hbits, wb, wpb, grid);
   log.add();
   return cudaPeekAtLastError() == cudaSuccess ? KNN_OK : KNN_ERR_CUDA;
 }

@@ -123,6 +123,51 @@ def write_csv_integers(path: str, x: np.ndarray) -> None:
             f.write(out.tobytes())
 
 
+def write_csv_fixed(path: str, x: np.ndarray, decimals: int = 9) -> np.ndarray:
+    """CSV in the reference's input format for values in [0, 10): exact zeros
+    as "0", every other value in fixed point with ``decimals`` digits (no
+    per-value formatting, so a multi-GB file takes seconds).  Returns the
+    float32 values a reader parses back (the written decimals, rounded)."""
+    x = np.asarray(x, dtype=np.float32)
+    n, d = x.shape
+    if x.size and (x.min() < 0 or x.max() >= 10):
+        raise ValueError("write_csv_fixed takes values in [0, 10)")
+    scale = 10 ** decimals
+    width = decimals + 2  # "d." + decimals
+    parsed = np.empty_like(x)
+    with open(path, "wb") as f:
+        f.write(f"{n}\n{d}\n".encode())
+        step = 4096
+        for s in range(0, n, step):
+            blk = x[s:s + step].astype(np.float64)
+            m = np.rint(blk * scale).astype(np.int64)
+            zero = m == 0
+            parsed[s:s + step] = (m / scale).astype(np.float32)
+            w = np.where(zero, 1, width) + 1  # token + separator
+            ends = np.cumsum(w, axis=1)
+            starts = ends - w
+            rows = blk.shape[0]
+            row_len = ends[:, -1]
+            row_off = np.concatenate(([0], np.cumsum(row_len)[:-1]))
+            buf = np.empty(int(row_len.sum()), dtype=np.uint8)
+            pos = row_off[:, None] + starts
+            buf[pos[zero]] = ord("0")
+            nz = ~zero
+            pz, mz = pos[nz], m[nz]
+            buf[pz] = (mz // scale + ord("0")).astype(np.uint8)
+            buf[pz + 1] = ord(".")
+            frac = mz % scale
+            for j in range(decimals):
+                buf[pz + 1 + decimals - j] = (frac % 10 + ord("0")).astype(np.uint8)
+                frac //= 10
+            sep = row_off[:, None] + ends - 1
+            buf[sep] = ord(",")
+            buf[sep[:, -1]] = ord("\n")
+            assert rows == sep.shape[0]
+            f.write(buf.tobytes())
+    return parsed
+
+
 def stored_distance(dist: np.ndarray, metric: int) -> np.ndarray:
     """Value the reference stores for a returned distance (see module doc)."""
     dist = np.asarray(dist, dtype=np.float32)

@@ -3,12 +3,16 @@ exchanges, the library's kernels for all compute.
 
 Rank r of G builds the global trees r, r+G, r+2G, ... (the same trees a
 single build would make: a tree's splits depend on its global index and the
-seed only) and the initial lists over them; the G lists of every point are
-all-gathered and merged (the k best distinct ids of their union -- which is
-the initial graph over all trees, since the k best of a union are the k best
-of the union of each part's k best).  Each propagation step then runs on a
-contiguous point range per rank and the ranges are all-gathered.  The graph
-is therefore the single-GPU build's, bit for bit.
+seed only) and the initial lists over them.  The rows of every point range
+then go to the range's owner (one all-to-all: each rank receives the G lists
+of its n/G points), which merges them (the k best distinct ids of their union
+-- the initial graph over all trees, since the k best of a union are the k
+best of the union of each part's k best), and one all-gather of the merged
+ranges gives every rank the whole initial graph: 2 n k 8 bytes received per
+rank instead of the G n k 8 of gathering every rank's full lists, and each
+point merged once instead of on every rank.  Each propagation step then runs
+on a contiguous point range per rank and the ranges are all-gathered.  The
+graph is therefore the single-GPU build's, bit for bit.
 
 The per-rank compute goes through a backend object (`LibraryBackend`: the
 C ABI on device tensors).  The exchange goes through torch.distributed
@@ -42,19 +46,22 @@ class Lists:
 class LibraryBackend:
     """Per-rank compute on one GPU through the C ABI (device tensors)."""
 
-    def __init__(self, acknn, device: int = 0):
+    def __init__(self, acknn, device: int = 0, precision: int = 0):
         import torch
 
         self.torch = torch
         self.acknn = acknn
+        self.precision = precision  # leaf stage of the local trees (knn_options.precision)
         self.lib = acknn.load_library()
         self.device = device
         self.ctx = acknn.Context(device)
 
-    def _opt(self, **kw):
+    def _opt(self, x=None, **kw):
         # torch's current stream: the library's launches are ordered after the
         # torch ops that allocate and fill the tensors it reads and writes
         stream = self.torch.cuda.current_stream(self.device).cuda_stream
+        if x is not None:
+            kw["dtype"] = self.acknn.F16 if x.dtype == self.torch.float16 else self.acknn.F32
         return self.acknn.default_options(device=self.device, points_on_device=1, outputs_on_device=1,
                                           stream=stream, **kw)
 
@@ -70,7 +77,7 @@ class LibraryBackend:
         out = self.empty_lists(n, k)
         if count == 0:
             return out
-        opt = self._opt(tree_offset=rank, tree_stride=world, raw_keys=1)
+        opt = self._opt(x, tree_offset=rank, tree_stride=world, raw_keys=1, precision=self.precision)
         rc = self.lib.knn_build_ex(self.ctx.handle, x.data_ptr(), n, d, k, count, leaf, 0, metric, seed,
                                    out.idx.data_ptr(), out.key.data_ptr(), ctypes.byref(opt), None)
         self._check(rc)
@@ -95,7 +102,7 @@ class LibraryBackend:
         flags = lst.flags.data_ptr() if lst.flags is not None else None
         rc = self.lib.knn_propagate_range(self.ctx.handle, x.data_ptr(), n, d, k, metric, r0, r1,
                                           lst.idx.data_ptr(), lst.key.data_ptr(), flags, out.idx.data_ptr(),
-                                          out.key.data_ptr(), out.flags.data_ptr(), ctypes.byref(self._opt()))
+                                          out.key.data_ptr(), out.flags.data_ptr(), ctypes.byref(self._opt(x)))
         self._check(rc)
         return out
 
@@ -125,19 +132,42 @@ class TorchComm:
 
     def all_gather_rows(self, t, n):
         """Rows [n*r/world, n*(r+1)/world) of t from every rank r, assembled."""
+        r0, r1 = point_range(n, self.rank, self.world)
+        return self.all_gather_range(t[r0:r1], n)
+
+    def all_gather_range(self, part, n):
+        """[n, ...] assembled from every rank's rows of its own point range
+        (`part`: this rank's rows, [r1 - r0, ...])."""
         import torch
 
         chunk = (n + self.world - 1) // self.world
         r0, r1 = point_range(n, self.rank, self.world)
-        pad = torch.zeros((chunk,) + tuple(t.shape[1:]), dtype=t.dtype, device=t.device)
-        pad[: r1 - r0] = t[r0:r1]
+        pad = torch.zeros((chunk,) + tuple(part.shape[1:]), dtype=part.dtype, device=part.device)
+        pad[: r1 - r0] = part
         parts = [torch.empty_like(pad) for _ in range(self.world)]
         self.dist.all_gather(parts, pad, group=self.group)
-        out = torch.empty_like(t)
+        out = torch.empty((n,) + tuple(part.shape[1:]), dtype=part.dtype, device=part.device)
         for r, p in enumerate(parts):
             a, b = point_range(n, r, self.world)
             out[a:b] = p[: b - a]
         return out
+
+    def all_to_all_rows(self, t, n):
+        """Rows of every rank's point range to that rank: returns [world,
+        r1 - r0, ...], the rows of this rank's range [r0, r1) from every rank
+        (t: [n, ...], this rank's rows of all points)."""
+        import torch
+
+        chunk = (n + self.world - 1) // self.world
+        tail = tuple(t.shape[1:])
+        send = torch.zeros((self.world * chunk,) + tail, dtype=t.dtype, device=t.device)
+        for q in range(self.world):
+            a, b = point_range(n, q, self.world)
+            send[q * chunk: q * chunk + (b - a)] = t[a:b]
+        recv = torch.empty_like(send)
+        self.dist.all_to_all_single(recv, send, group=self.group)
+        r0, r1 = point_range(n, self.rank, self.world)
+        return recv.view((self.world, chunk) + tail)[:, : r1 - r0]
 
 
 def build_sharded(backend, comm, x, k: int, trees: int, leaf: int, props: int, metric: int = 0,
@@ -147,9 +177,11 @@ def build_sharded(backend, comm, x, k: int, trees: int, leaf: int, props: int, m
     n = x.shape[0]
     world, rank = comm.world, comm.rank
     local = backend.local_trees(x, k, trees, leaf, metric, seed, rank, world)
-    idx_all = comm.all_gather_stack(local.idx)
-    key_all = comm.all_gather_stack(local.key)
-    lst = backend.merge(idx_all, key_all, k, metric)
+    # this rank's point range: its G lists, merged here, then assembled everywhere
+    idx_mine = comm.all_to_all_rows(local.idx, n).contiguous()
+    key_mine = comm.all_to_all_rows(local.key, n).contiguous()
+    merged = backend.merge(idx_mine, key_mine, k, metric)
+    lst = Lists(comm.all_gather_range(merged.idx, n), comm.all_gather_range(merged.key, n))
     for _ in range(props):
         r0, r1 = point_range(n, rank, world)
         nxt = backend.propagate_range(x, lst, k, metric, r0, r1)

@@ -476,13 +476,27 @@ def run_single(args, w):
     torch.cuda.set_device(0)
     acknn = load_package()
     lib = acknn.load_library()
-    n, d, k, metric = w["n"], w["d"], w["k"], w["metric"]
-    p = dict(TARGET_PARAMS)
+    if args.workload == "integer_mixture":
+        n, k, metric = w["n"], w["k"], w["metric"]
+        p = dict(TARGET_PARAMS)
+        xh = make_points(acknn, n, seed=args.seed)
+        desc = workload_desc
+    else:
+        cfg = acknn.workloads.CONFIGS[args.workload]
+        n, k, metric = args.n or cfg["n"], cfg["k"], cfg["metric"]
+        p = {kk: cfg[kk] for kk in ("trees", "leaf", "props")}
+        xh = cfg["gen"](args.seed, n=n)
+
+        def desc(_w, pp):
+            return (f"{args.workload} N={n:,} d={xh.shape[1]} {xh.dtype}; k={k}, {pp['trees']} trees, leaf "
+                    f"{pp['leaf']}, {pp['props']} propagation(s), {METRIC_NAMES[metric]}")
+    d = xh.shape[1]
+    dtype = acknn.F16 if xh.dtype == np.float16 else acknn.F32
     for key in ("trees", "leaf", "props"):
         if getattr(args, key) is not None:
             p[key] = getattr(args, key)
-    prec = acknn.PREC_BF16_RERANK if args.single == "mixed" else acknn.PREC_FP32
-    x = torch.from_numpy(make_points(acknn, n, seed=args.seed)).cuda()
+    prec = {"mixed": acknn.PREC_BF16_RERANK, "mixed_f16": acknn.PREC_F16_RERANK}.get(args.single, acknn.PREC_FP32)
+    x = torch.from_numpy(xh).cuda()
     idx = torch.empty((n, k), dtype=torch.int32, device="cuda")
     dist = torch.empty((n, k), dtype=torch.float32, device="cuda")
     ctx = acknn.Context(0)
@@ -490,7 +504,7 @@ def run_single(args, w):
 
     def build(stats=None):
         opt = acknn.default_options(points_on_device=1, outputs_on_device=1, stream=stream.cuda_stream,
-                                    precision=prec)
+                                    precision=prec, dtype=dtype)
         rc = lib.knn_build_ex(ctx.handle, x.data_ptr(), n, d, k, p["trees"], p["leaf"], p["props"], metric,
                               args.seed, idx.data_ptr(), dist.data_ptr(), ctypes.byref(opt),
                               ctypes.byref(stats) if stats is not None else None)
@@ -512,9 +526,10 @@ def run_single(args, w):
     build(stats=st)
     torch.cuda.synchronize()
     sd = st.as_dict()
-    print(json.dumps({"case": args.single, "workload": workload_desc(w, p), "ms_per_build": ms,
+    print(json.dumps({"case": args.single, "workload": desc(w, p), "ms_per_build": ms,
                       "points_per_s": n / (ms / 1e3),
                       "stages_ms": {kk: sd[kk] for kk in ("ms_trees", "ms_leaf", "ms_propagate", "ms_total")},
+                      "prop_candidates": sd["prop_candidates"], "ms_leaf_tiles": sd["ms_leaf_tiles"],
                       "launches": sd["launches"], "depth": sd["depth"]}), flush=True)
     ctx.close()
     return 0
@@ -646,12 +661,45 @@ def run_batch(args):
 
 
 # ------------------------------------------------------- other configurations --
+# Cheapest settings reaching recall@k >= 0.95 per path, from `--sweep` runs
+# of each configuration (trees, leaf, propagations); None: the path did not
+# reach the target within the swept grid (its best setting is given instead).
+CONFIG_TARGETS = {
+    "sparse_prototypes": {"plain_fp32": (8, 128, 4)},
+    "normalized_mixture": {"plain_fp32": (12, 64, 4), "mixed_f16": (12, 64, 4),
+                           "mixed_f16_learned": (12, 64, 4)},
+}
+PATH_OPTIONS = {
+    "plain_fp32": dict(precision=0),
+    "mixed": dict(precision=1),
+    "mixed_f16": dict(precision=2),
+    "mixed_learned": dict(precision=1, learned_splits=1),
+    "mixed_f16_learned": dict(precision=2, learned_splits=1),
+}
+
+
+def prop_roofline(n, d, k, s, cands, ms_prop, peak):
+    """Propagation against HBM: algorithmic bytes P N (k^2 4 + 2k 8) + sum over
+    iterations of c-bar N d s (c-bar N = the keys evaluated in that iteration,
+    each reading one candidate row of d elements of s bytes), over the
+    propagation time."""
+    if not cands or ms_prop <= 0:
+        return None
+    by = sum(n * (k * k * 4 + 2 * k * 8) + c * d * s for c in cands)
+    ach = by / (ms_prop / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": "k_propagate", "algorithmic_bytes": by, "ms": ms_prop,
+            "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+            "c_bar": [c / n for c in cands]}
+
+
 def run_config(args):
-    """One named configuration at its literal parameters (sparse prototypes,
-    d=784, TAXICAB; normalised mixture, 10M x 96 FP16, COSINE): time of each
-    applicable path with device-resident points (plain FP32; mixed BF16 +
-    re-rank; for COSINE also learned splits trained on a 1M-point sample), and
-    recall@k against the FP64 exact graph on 10,000 seeded queries."""
+    """One named configuration (sparse prototypes, d=784, TAXICAB; normalised
+    mixture, 10M x 96 FP16, COSINE): each path at its own cheapest setting that
+    reaches recall@k >= 0.95 (CONFIG_TARGETS, from the sweep) and the plain
+    FP32 path at the configuration's literal parameters; points resident in
+    HBM, recall@k and distance error against the FP64 exact graph on 10,000
+    seeded queries, per-stage device times, the propagation kernel's HBM
+    roofline and the ratio to plain FP32 at equal recall."""
     import torch
 
     torch.cuda.set_device(0)
@@ -659,27 +707,30 @@ def run_config(args):
     lib = acknn.load_library()
     cfg = acknn.workloads.CONFIGS[args.workload]
     n = args.n or cfg["n"]
-    k, T, L, P, metric = cfg["k"], cfg["trees"], cfg["leaf"], cfg["props"], cfg["metric"]
+    k, metric = cfg["k"], cfg["metric"]
     x = cfg["gen"](0, n=n)
     d = x.shape[1]
+    s_bytes = 2 if x.dtype == np.float16 else 4
     dtype = acknn.F16 if x.dtype == np.float16 else acknn.F32
     xd = torch.from_numpy(x).cuda()
     idx = torch.empty((n, k), dtype=torch.int32, device="cuda")
     dist = torch.empty((n, k), dtype=torch.float32, device="cuda")
     ctx = acknn.Context(0)
     stream = torch.cuda.current_stream()
-    paths = {"plain_fp32": dict(precision=acknn.PREC_FP32)}
-    if metric != 1:
-        paths["mixed"] = dict(precision=acknn.PREC_BF16_RERANK)
-    if metric == 2:
-        paths["mixed_learned"] = dict(precision=acknn.PREC_BF16_RERANK, learned_splits=1,
-                                      mlp_sample=min(n, 1_000_000))
     rng = np.random.Generator(np.random.PCG64(12345))
     q = np.sort(rng.choice(n, size=min(10_000, n), replace=False)).astype(np.int64)
-    ei, _ = acknn.exact_fp64(x, k, q, metric)
+    qt = torch.from_numpy(q).cuda()
+    exact = acknn.exact_fp64(x, k, q, metric)
+    peak, peak_kind = measured_peaks()
+    runs = {f"{p}@target": (p, tuple(v)) for p, v in CONFIG_TARGETS[args.workload].items() if v}
+    runs["plain_fp32@literal"] = ("plain_fp32", (cfg["trees"], cfg["leaf"], cfg["props"]))
     res = {}
-    for name, kw in paths.items():
-        def build(stats=None, kw=kw):
+    for name, (path, (T, L, P)) in runs.items():
+        kw = dict(PATH_OPTIONS[path])
+        if kw.get("learned_splits"):
+            kw["mlp_sample"] = min(n, 1_000_000)
+
+        def build(stats=None, kw=kw, T=T, L=L, P=P):
             opt = acknn.default_options(points_on_device=1, outputs_on_device=1, dtype=dtype,
                                         stream=stream.cuda_stream, **kw)
             rc = lib.knn_build_ex(ctx.handle, xd.data_ptr(), n, d, k, T, L, P, metric, 0, idx.data_ptr(),
@@ -700,14 +751,22 @@ def run_config(args):
         st.struct_size = ctypes.sizeof(acknn.KnnStats)
         build(stats=st)
         torch.cuda.synchronize()
-        ai = idx.cpu().numpy()[q]
-        rec = sum(len(np.intersect1d(a, b)) for a, b in zip(ai, ei)) / (k * len(q))
+        acc = accuracy(acknn, x, idx[qt].cpu().numpy(), dist[qt].cpu().numpy(), k, metric, exact, q, gathered=True)
         sd = st.as_dict()
-        res[name] = {"ms_per_build": ms, "points_per_s": n / (ms / 1e3), "recall": rec,
-                     "stages_ms": {kk: sd[kk] for kk in ("ms_learn", "ms_trees", "ms_leaf", "ms_propagate")}}
-    print(json.dumps({"workload": args.workload, "n": n, "d": d, "k": k, "trees": T, "leaf": L, "props": P,
-                      "metric": METRIC_NAMES[metric], "dtype": str(x.dtype), "queries": int(len(q)),
-                      "steps": args.steps, "warmup": args.warmup, "paths": res}), flush=True)
+        res[name] = {"params": {"trees": T, "leaf": L, "props": P}, "ms_per_build": ms,
+                     "points_per_s": n / (ms / 1e3), "accuracy": acc, "leaf_path": sd["leaf_path"],
+                     "stages_ms": {kk: sd[kk] for kk in ("ms_learn", "ms_trees", "ms_leaf", "ms_propagate")},
+                     "propagate_roofline": prop_roofline(n, d, k, s_bytes, sd["prop_candidates"],
+                                                         sd["ms_propagate"], peak)}
+    plain = res.get("plain_fp32@target")
+    ratios = {}
+    if plain:
+        for name, r in res.items():
+            if name.endswith("@target") and name != "plain_fp32@target":
+                ratios[name.split("@")[0] + "_vs_plain_at_equal_recall"] = plain["ms_per_build"] / r["ms_per_build"]
+    print(json.dumps({"workload": args.workload, "n": n, "d": d, "k": k, "metric": METRIC_NAMES[metric],
+                      "dtype": str(x.dtype), "queries": int(len(q)), "steps": args.steps, "warmup": args.warmup,
+                      "peak_source": peak_kind, "paths": res, **ratios}), flush=True)
     ctx.close()
     return 0
 
@@ -784,6 +843,141 @@ def run_reference_gpu(args, w):
                                    props=args.props if args.props is not None else 0)}
     r = reference_gpu_runs(acknn, x, k, q, ei, settings, args.ref_limit)
     print(json.dumps({"reference_gpu": r, "workload": workload_desc(w, TARGET_PARAMS)}), flush=True)
+    return 0
+
+
+# ------------------------------------------------------ sharded single dataset --
+def run_sharded(args):
+    """One dataset's graph built by all ranks together (sharded.build_sharded:
+    trees split by rank, one all-to-all + merge + all-gather of the initial
+    lists, propagation by point range with an all-gather per step).  Every
+    rank holds the same points; `value` = n / (max over ranks of the device
+    time of one build): strong scaling, the total work is fixed."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    acknn = load_package()
+    acknn.load_library()
+    name = args.workload if args.workload != "dataset_batch" else "normalized_mixture"
+    cfg = acknn.workloads.CONFIGS[name]
+    n = args.n or cfg["n"]
+    k, metric = cfg["k"], cfg["metric"]
+    T = args.trees or cfg["trees"]
+    L = args.leaf or cfg["leaf"]
+    P = args.props if args.props is not None else cfg["props"]
+    x = cfg["gen"](0, n=n)
+    xd = torch.from_numpy(x).cuda(local)
+    prec = acknn.PREC_FP32 if metric == 1 else acknn.PREC_F16_RERANK
+    sh = acknn.sharded
+    be, comm = sh.LibraryBackend(acknn, local, precision=prec), sh.TorchComm()
+    stream = torch.cuda.current_stream(local)
+
+    def build():
+        return sh.build_sharded(be, comm, xd, k, T, L, P, metric, 0)
+
+    for _ in range(args.warmup):
+        build()
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        gi, gd = build()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    t = torch.tensor([e0.elapsed_time(e1) / args.steps], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    if rank == 0:
+        rng = np.random.Generator(np.random.PCG64(12345))
+        q = np.sort(rng.choice(n, size=min(10_000, n), replace=False)).astype(np.int64)
+        ei, _ = acknn.exact_fp64(x, k, q, metric)
+        ai = gi[torch.from_numpy(q).cuda(local)].cpu().numpy()
+        rec = sum(len(np.intersect1d(a, b)) for a, b in zip(ai, ei)) / (k * len(q))
+        print(json.dumps({
+            "metric": "k-NN graph points/s of one dataset built by all ranks", "value": n / (ms / 1e3),
+            "unit": "points/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f16+f32",
+            "data": "synthetic",
+            "config": {"workload": f"{name} N={n:,} d={x.shape[1]} {x.dtype}; k={k}, {T} trees, leaf {L}, {P} "
+                                   f"propagation(s), {METRIC_NAMES[metric]}", "parallelism": f"sharded x{world}",
+                       "exchange_bytes_received_per_rank": int(2 * n * k * 8 + P * n * (k * 8 + 4 * ((k + 31) // 32)))},
+            "recall_id": rec}), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
+
+
+# ------------------------------------------------------- the hello CLI itself --
+HELLO_BIN = PKG_DIR / "hello"
+
+
+def run_cli(args):
+    """The drop-in CLI end to end on one configuration written as CSV: wall
+    time of the `hello` process and its own split (CSV ingest, normalisation +
+    build, binary write; ACKNN_TIMING=1), and recall@k by id from its output
+    file against the FP64 exact graph of the points it read, normalised as the
+    reference normalises them (10,000 seeded queries)."""
+    import re
+    import shutil
+    import tempfile
+
+    import torch
+
+    torch.cuda.set_device(0)
+    acknn = load_package()
+    acknn.load_library()
+    cfg = acknn.workloads.CONFIGS[args.workload]
+    n = args.n or cfg["n"]
+    k, metric = cfg["k"], cfg["metric"]
+    T = args.trees or cfg["trees"]
+    L = args.leaf or cfg["leaf"]
+    P = args.props if args.props is not None else cfg["props"]
+    x = cfg["gen"](0, n=n)
+    tmp = Path(tempfile.mkdtemp(prefix="acknn_cli_"))
+    try:
+        csv = tmp / "points.csv"
+        t = time.perf_counter()
+        if args.workload == "integer_mixture":
+            acknn.formats.write_csv_integers(str(csv), x)
+            parsed = x
+        elif args.workload == "sparse_prototypes":
+            parsed = acknn.formats.write_csv_fixed(str(csv), x)
+        else:
+            raise SystemExit(f"--cli supports integer_mixture and sparse_prototypes, not {args.workload}")
+        write_s = time.perf_counter() - t
+        out = tmp / "graph.bin"
+        env = dict(os.environ, ACKNN_TIMING="1")
+        cmd = [str(HELLO_BIN), str(csv), str(out), str(k), str(T), str(L), str(P), METRIC_NAMES[metric], "0", "F"]
+        t = time.perf_counter()
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
+        wall = time.perf_counter() - t
+        if r.returncode != 0:
+            raise SystemExit(f"hello exited {r.returncode}: {r.stdout[-500:]} {r.stderr[-500:]}")
+        tm = dict(re.findall(r"(\w+_ms)=([0-9.]+)", r.stderr))
+        thr = re.search(r"threads=(\d+)", r.stderr)
+        _, _, ids, _ = acknn.formats.read_result(str(out))
+        xn = acknn.normalize_reference(parsed)
+        rng = np.random.Generator(np.random.PCG64(12345))
+        q = np.sort(rng.choice(n, size=min(10_000, n), replace=False)).astype(np.int64)
+        ei, _ = acknn.exact_fp64(xn, k, q, metric)
+        rec = sum(len(np.intersect1d(a, b)) for a, b in zip(ids[q], ei)) / (k * len(q))
+        line = {"cli": args.workload, "n": n, "d": x.shape[1], "k": k, "trees": T, "leaf": L, "props": P,
+                "metric": METRIC_NAMES[metric], "csv_bytes": csv.stat().st_size, "csv_write_s": write_s,
+                "hello_wall_s": wall, "load_ms": float(tm.get("load_ms", "nan")),
+                "build_ms": float(tm.get("build_ms", "nan")), "write_ms": float(tm.get("write_ms", "nan")),
+                "parse_threads": int(thr.group(1)) if thr else None,
+                "ingest_gb_per_s": csv.stat().st_size / (float(tm.get("load_ms", "nan")) / 1e3) / 1e9,
+                "recall_id": rec, "queries": int(len(q))}
+        print(json.dumps(line), flush=True)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
     return 0
 
 
@@ -894,12 +1088,20 @@ class _BatchRunner:
 
 
 def _sweep_paths(acknn, workload: str, metric: int, n: int) -> dict:
-    paths = {"plain_fp32": dict(precision=acknn.PREC_FP32)}
-    if metric != 1:
-        paths["mixed"] = dict(precision=acknn.PREC_BF16_RERANK)
-    if metric == 2 and workload != "dataset_batch":
-        paths["mixed_learned"] = dict(precision=acknn.PREC_BF16_RERANK, learned_splits=1,
-                                      mlp_sample=min(n, 1_000_000))
+    """Paths compared at equal recall: plain FP32 always; for EUCLIDEAN the
+    BF16 and FP16 tensor-core leaf tiles; for COSINE (FP16 data) the FP16
+    tiles with and without learned splits."""
+    names = ["plain_fp32"]
+    if metric == 0:
+        names += ["mixed", "mixed_f16"]
+    elif metric == 2:
+        names += ["mixed_f16"] + (["mixed_f16_learned"] if workload != "dataset_batch" else [])
+    paths = {}
+    for nm in names:
+        kw = dict(PATH_OPTIONS[nm])
+        if kw.get("learned_splits"):
+            kw["mlp_sample"] = min(n, 1_000_000)
+        paths[nm] = kw
     return paths
 
 
@@ -974,7 +1176,7 @@ def run_sweep(args):
                     sd = st.as_dict()
                     row.update(ms=ms, points_per_s=R.points / (ms / 1e3), accuracy=acc,
                                stages_ms={kk: sd[kk] for kk in ("ms_learn", "ms_trees", "ms_leaf", "ms_propagate")},
-                               leaf_tile=sd["leaf_tile"])
+                               prop_candidates=sd["prop_candidates"], leaf_path=sd["leaf_path"])
                     print(json.dumps(row), flush=True)
                     if best is None or ms < best["ms"]:
                         best = row
@@ -1007,7 +1209,7 @@ def main():
     ap.add_argument("--workload", choices=["integer_mixture", "dataset_batch", "sparse_prototypes",
                                            "normalized_mixture"], default="integer_mixture")
     ap.add_argument("--count", type=int, default=None, help="datasets in the batch workload")
-    ap.add_argument("--single", choices=["mixed", "plain"], default=None,
+    ap.add_argument("--single", choices=["mixed", "mixed_f16", "plain"], default=None,
                     help="time one configuration only (the profiling case)")
     ap.add_argument("--trees", type=int, default=None)
     ap.add_argument("--leaf", type=int, default=None)
@@ -1022,6 +1224,10 @@ def main():
     ap.add_argument("--reference-gpu", action="store_true",
                     help="time the reference's own sm_100a build (oracle/_ref/hello) on the workload")
     ap.add_argument("--ref-limit", type=float, default=300.0, help="seconds per reference run")
+    ap.add_argument("--sharded", action="store_true",
+                    help="one dataset built by all ranks together (strong scaling; launch with torchrun for N > 1)")
+    ap.add_argument("--cli", action="store_true",
+                    help="time the hello CLI end to end (CSV ingest, build, binary write) on the workload")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -1034,12 +1240,16 @@ def main():
         return run_sweep(args)
     if args.reference_gpu:
         return run_reference_gpu(args, w)
+    if args.cli:
+        return run_cli(args)
+    if args.sharded:
+        return run_sharded(args)
     if args.workload == "dataset_batch":
         return run_batch(args)
-    if args.workload in ("sparse_prototypes", "normalized_mixture"):
-        return run_config(args)
     if args.single:
         return run_single(args, w)
+    if args.workload in ("sparse_prototypes", "normalized_mixture"):
+        return run_config(args)
     return run_ours(args, w)
 
 

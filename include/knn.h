@@ -60,6 +60,11 @@ extern "C" {
                                   requests the tiles cannot hold, run the FP32
                                   leaf stage instead; knn_stats.leaf_path and
                                   leaf_fallback say which ran                     */
+#define KNN_PREC_F16_RERANK 2  /* the same with FP16 tiles: 11 significant bits
+                                  instead of 8, exact for FP16 input; EUCLIDEAN
+                                  rows are scaled by a power of two into the FP16
+                                  range inside the tile stage (keys are ranked
+                                  the same; the re-rank uses the input rows)     */
 
 /* Tree split rules.  MEDIAN: each node splits at the median of its points'
  * projections (balanced trees of static shape).  REFERENCE: the split of
@@ -118,7 +123,8 @@ typedef struct knn_stats {
   int32_t leaf_tile;         /* leaf tile used: 32/64 FP32, 128 tensor-core             */
   int32_t prop_warps;        /* propagation warps per block used (0: the default)       */
   float ms_leaf_tiles;       /* summed device time of the leaf-tile kernel launches     */
-  int32_t leaf_path;         /* leaf stage that ran: 0 FP32 CUDA cores, 1 tensor cores  */
+  int32_t leaf_path;         /* leaf stage that ran: 0 FP32 CUDA cores, 1 BF16 tensor-core
+                                tiles, 2 FP16 tensor-core tiles                        */
   int32_t leaf_fallback;     /* 1: tensor-core precision was asked for, FP32 ran        */
   int64_t reserved[5];
 } knn_stats;

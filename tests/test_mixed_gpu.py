@@ -79,3 +79,46 @@ def test_taxicab_request_falls_back_to_fp32(lib):
     b = lib.knn_build(x, 6, 2, 40, 1, 1)
     np.testing.assert_array_equal(a[0], b[0])
     np.testing.assert_array_equal(a[1], b[1])
+
+
+@pytest.mark.parametrize("n,d,k,trees,leaf,props", [
+    (20000, 128, 16, 4, 64, 0),
+    (20000, 128, 16, 3, 2048, 0),
+    (9000, 200, 10, 2, 300, 1),
+])
+def test_f16_tiles_equal_plain_on_exact_integer_data(lib, n, d, k, trees, leaf, props):
+    """FP16 tiles (11 significant bits) hold integers up to 2048 exactly; the
+    EUCLIDEAN rows are scaled by a power of two into [2^14, 2^15), which keeps
+    them exact, so the graph equals the plain one bit for bit."""
+    x = _ints(n, d, n + d + 1)
+    mi, md = lib.knn_build(x, k, trees, leaf, props, 0, seed=4, precision=lib.PREC_F16_RERANK)
+    pi, pd = lib.knn_build(x, k, trees, leaf, props, 0, seed=4)
+    np.testing.assert_array_equal(mi, pi)
+    np.testing.assert_array_equal(md.view(np.uint32), pd.view(np.uint32))
+
+
+@pytest.mark.parametrize("scale", [1e-6, 1.0, 1e6])
+def test_f16_tiles_any_euclidean_scale(lib, scale):
+    """Rows far outside the FP16 range (or deep in its subnormals) still rank
+    as the plain path does: on integer data times a power of two the graph is
+    identical; on float data times any scale, recall stays within 0.02."""
+    n, d, k = 12000, 64, 10
+    x = _ints(n, d, 5) * np.float32(2.0 ** round(np.log2(scale)))
+    mi, md = lib.knn_build(x, k, 4, 128, 1, 0, seed=2, precision=lib.PREC_F16_RERANK)
+    pi, pd = lib.knn_build(x, k, 4, 128, 1, 0, seed=2)
+    np.testing.assert_array_equal(mi, pi)
+    np.testing.assert_array_equal(md.view(np.uint32), pd.view(np.uint32))
+    y = lib.workloads.gaussian_mixture(n, d, 20, seed=9) * np.float32(scale)
+    mi, _ = lib.knn_build(y, k, 4, 128, 1, 0, seed=2, precision=lib.PREC_F16_RERANK)
+    pi, _ = lib.knn_build(y, k, 4, 128, 1, 0, seed=2)
+    q = np.arange(0, n, 7)
+    ei, _ = lib.exact_fp64(y, k, q, 0)
+    assert recall_at_k(mi[q], ei) >= recall_at_k(pi[q], ei) - 0.02
+
+
+def test_precision_stats_report_the_leaf_path(lib):
+    x = lib.workloads.gaussian_mixture(3000, 32, 6, seed=1)
+    for prec, metric, path, fallback in ((lib.PREC_FP32, 0, 0, 0), (lib.PREC_BF16_RERANK, 0, 1, 0),
+                                         (lib.PREC_F16_RERANK, 2, 2, 0), (lib.PREC_BF16_RERANK, 1, 0, 1)):
+        _, _, st = lib.knn_build(x, 6, 2, 64, 1, metric, precision=prec, stats=True)
+        assert (st["leaf_path"], st["leaf_fallback"]) == (path, fallback)

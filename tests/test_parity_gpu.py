@@ -147,11 +147,16 @@ def test_exact_fp64_matches_cpu(lib, oracle, metric):
     np.testing.assert_array_equal(gd, od)
 
 
-def test_float16_input_matches_float32_of_same_values(lib, oracle):
-    x16 = _rand(2000, 16, 12).astype(np.float16)
-    got = lib.knn_build(x16, 7, 3, 32, 2, 2)
-    want = oracle.knn_build(x16.astype(np.float32), 7, 3, 32, 2, 2)
-    _same(got, want, "f16")
+@pytest.mark.parametrize("metric", [0, 1, 2])
+@pytest.mark.parametrize("n,d,k", [(2000, 16, 7), (3000, 37, 12), (2500, 130, 33), (4000, 300, 5)])
+def test_float16_input_matches_float32_of_same_values(lib, oracle, metric, n, d, k):
+    """FP16 input: propagation gathers the FP16 rows themselves (row slices of
+    128 dims, rows padded to 8); the FP16 -> FP32 conversion is exact, so the
+    graph equals the oracle's on the same values as float32."""
+    x16 = _rand(n, d, 12 + d).astype(np.float16)
+    got = lib.knn_build(x16, k, 3, 32 + k, 2, metric)
+    want = oracle.knn_build(x16.astype(np.float32), k, 3, 32 + k, 2, metric)
+    _same(got, want, f"f16 d={d} metric={metric}")
 
 
 def test_device_pointers_and_stats(lib, oracle):

@@ -22,7 +22,14 @@ def _virtual_sharded(acknn, x, k, trees, leaf, props, metric, seed, world):
     xd = torch.from_numpy(x).cuda()
     n = x.shape[0]
     parts = [be.local_trees(xd, k, trees, leaf, metric, seed, r, world) for r in range(world)]
-    lst = be.merge(torch.stack([p.idx for p in parts]), torch.stack([p.key for p in parts]), k, metric)
+    # as build_sharded: each rank merges the G lists of its own point range
+    idx_all, key_all = torch.stack([p.idx for p in parts]), torch.stack([p.key for p in parts])
+    idx, key = torch.empty_like(parts[0].idx), torch.empty_like(parts[0].key)
+    for r in range(world):
+        a, b = sh.point_range(n, r, world)
+        m = be.merge(idx_all[:, a:b].contiguous(), key_all[:, a:b].contiguous(), k, metric)
+        idx[a:b], key[a:b] = m.idx, m.key
+    lst = sh.Lists(idx, key)
     for _ in range(props):
         nxt = [be.propagate_range(xd, lst, k, metric, *sh.point_range(n, r, world)) for r in range(world)]
         idx, key, flags = lst.idx.clone(), lst.key.clone(), nxt[0].flags.clone()
