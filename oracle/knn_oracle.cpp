@@ -179,6 +179,34 @@ inline float key_cosine_from(float dot, float na, float nb) {
   return 1.0f - dot / (na * nb);
 }
 
+// Sums of one query row against eight candidate rows at once: eight
+// independent sums, each in the order of key_euclid / key_taxicab /
+// dot_chunked (sequential within 256-dim chunks, chunk partials added to the
+// total), so every result has the bits of the one-pair function.
+template <int METRIC>
+void sums8(const float* a, const float* const* b, int d, float* out) {
+  float total[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int c0 = 0; c0 < d; c0 += 256) {
+    float part[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int c1 = std::min(d, c0 + 256);
+    for (int i = c0; i < c1; ++i) {
+      const float av = a[i];
+      for (int j = 0; j < 8; ++j) {
+        if (METRIC == kEuclidean) {
+          const float df = av - b[j][i];
+          part[j] = std::fmaf(df, df, part[j]);
+        } else if (METRIC == kTaxicab) {
+          part[j] = part[j] + std::fabs(av - b[j][i]);
+        } else {
+          part[j] = std::fmaf(av, b[j][i], part[j]);
+        }
+      }
+    }
+    for (int j = 0; j < 8; ++j) total[j] = total[j] + part[j];
+  }
+  for (int j = 0; j < 8; ++j) out[j] = total[j];
+}
+
 struct Data {
   const float* X;
   int64_t n;
@@ -191,7 +219,34 @@ struct Data {
     if (metric == kTaxicab) return key_taxicab(row(i), row(j), d);
     return key_cosine_from(dot_chunked(row(i), row(j), d), norms[i], norms[j]);
   }
+  // out[c] = key(i, ids[c]) for c < m, eight candidates at a time
+  void keys(int64_t i, const int32_t* ids, int64_t m, float* out) const {
+    int64_t c = 0;
+    const float* b[8];
+    for (; c + 8 <= m; c += 8) {
+      for (int j = 0; j < 8; ++j) b[j] = row(ids[c + j]);
+      if (metric == kEuclidean) sums8<kEuclidean>(row(i), b, d, out + c);
+      else if (metric == kTaxicab) sums8<kTaxicab>(row(i), b, d, out + c);
+      else {
+        sums8<kCosine>(row(i), b, d, out + c);
+        for (int j = 0; j < 8; ++j) out[c + j] = key_cosine_from(out[c + j], norms[i], norms[ids[c + j]]);
+      }
+    }
+    for (; c < m; ++c) out[c] = key(i, ids[c]);
+  }
 };
+
+// Candidates (ids, keys) that can still enter a full sorted list of k: those
+// below its last entry (the rest cannot be among the k best of the union).
+void add_below_tail(const std::vector<Cand>& list, int k, const int32_t* ids, const float* keys, int64_t m,
+                    std::vector<Cand>& add) {
+  add.clear();
+  const bool full = (int)list.size() >= k;
+  for (int64_t c = 0; c < m; ++c) {
+    const Cand cd{keys[c], ids[c]};
+    if (!full || cand_less(cd, list[k - 1])) add.push_back(cd);
+  }
+}
 
 void prepare(Data& D) {
   if (D.metric == kCosine) {
@@ -387,14 +442,16 @@ int oracle_leaf_stage(const float* X, int64_t n, int32_t d, int32_t k, int32_t t
       }
       const int64_t blo = node_lo(n, bl, bj), bhi = node_lo(n, bl, bj + 1);
       std::vector<Cand> add;
+      std::vector<int32_t> ids;
+      std::vector<float> keys;
       for (int64_t q = lo; q < hi; ++q) {
         const int32_t i = pm[q];
-        add.clear();
-        for (int64_t c = blo; c < bhi; ++c) {
-          const int32_t jj = pm[c];
-          if (jj == i) continue;
-          add.push_back({D.key(i, jj), jj});
-        }
+        ids.clear();
+        for (int64_t c = blo; c < bhi; ++c)
+          if (pm[c] != i) ids.push_back(pm[c]);
+        keys.resize(ids.size());
+        D.keys(i, ids.data(), (int64_t)ids.size(), keys.data());
+        add_below_tail(lists[i], k, ids.data(), keys.data(), (int64_t)ids.size(), add);
         merge_topk(lists[i], add, k);
       }
     }
@@ -418,7 +475,8 @@ int oracle_propagate(const float* X, int64_t n, int32_t d, int32_t k, int32_t me
 #pragma omp parallel
   {
     std::vector<Cand> list, add;
-    std::vector<int32_t> ids;
+    std::vector<int32_t> ids, fresh;
+    std::vector<float> keys;
 #pragma omp for schedule(dynamic, 64)
     for (int64_t i = 0; i < n; ++i) {
       list.clear();
@@ -434,12 +492,15 @@ int oracle_propagate(const float* X, int64_t n, int32_t d, int32_t k, int32_t me
       }
       std::sort(ids.begin(), ids.end());
       ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
-      add.clear();
+      fresh.clear();
       for (int32_t jj : ids) {
         bool in_list = false;
         for (int s = 0; s < k; ++s) in_list |= (list[s].id == jj);
-        if (!in_list) add.push_back({D.key(i, jj), jj});
+        if (!in_list) fresh.push_back(jj);
       }
+      keys.resize(fresh.size());
+      D.keys(i, fresh.data(), (int64_t)fresh.size(), keys.data());
+      add_below_tail(list, k, fresh.data(), keys.data(), (int64_t)fresh.size(), add);
       merge_topk(list, add, k);
       for (int s = 0; s < k; ++s) {
         idx_out[i * k + s] = list[s].id;
