@@ -74,7 +74,8 @@ class KnnOptions(ctypes.Structure):
         ("tree_stride", ctypes.c_int32),
         ("raw_keys", ctypes.c_int32),
         ("split_rule", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 3),
+        ("tc_group", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 2),
     ]
 
 
@@ -99,7 +100,9 @@ class KnnStats(ctypes.Structure):
         ("ms_leaf_tiles", ctypes.c_float),
         ("leaf_path", ctypes.c_int32),
         ("leaf_fallback", ctypes.c_int32),
-        ("reserved", ctypes.c_int64 * 5),
+        ("tc_group", ctypes.c_int32),
+        ("reserved32", ctypes.c_int32),
+        ("reserved", ctypes.c_int64 * 4),
     ]
 
     def as_dict(self) -> dict:
@@ -111,7 +114,7 @@ class KnnStats(ctypes.Structure):
             "ms_leaf_tiles": self.ms_leaf_tiles,
             "launches": self.launches, "leaf_pairs": self.leaf_pairs,
             "leaf_tile": self.leaf_tile, "prop_warps": self.prop_warps,
-            "leaf_path": self.leaf_path, "leaf_fallback": self.leaf_fallback,
+            "leaf_path": self.leaf_path, "leaf_fallback": self.leaf_fallback, "tc_group": self.tc_group,
             "prop_candidates": [self.prop_candidates[i] for i in range(n)],
         }
 
@@ -215,7 +218,7 @@ def knn_build(points, k: int, trees: int, leaf: int, props: int, metric: int = 0
               seed: int = 0, precision: int = PREC_FP32, learned: bool = False,
               stats: bool = False, context=None, mlp_sample: int = 0, mlp_steps: int = 0,
               autotune: bool = False, leaf_tile: int = 0, prop_warps: int = 0,
-              split_rule: int = 0):
+              split_rule: int = 0, tc_group: int = 0):
     """k-NN graph of ``points`` ([n, d] float32/float16, host memory).
 
     ``learned`` builds the trees on the learned split network's embedding
@@ -230,7 +233,7 @@ def knn_build(points, k: int, trees: int, leaf: int, props: int, metric: int = 0
     opt = default_options(dtype=F16 if x.dtype == np.float16 else F32, precision=precision,
                           learned_splits=int(bool(learned)), mlp_sample=mlp_sample,
                           mlp_steps=mlp_steps, autotune=int(bool(autotune)), leaf_tile=leaf_tile,
-                          prop_warps=prop_warps, split_rule=split_rule)
+                          prop_warps=prop_warps, split_rule=split_rule, tc_group=tc_group)
     st = KnnStats()
     st.struct_size = ctypes.sizeof(KnnStats)
     rc = lib.knn_build_ex(context, _ptr(x), n, d, k, trees, leaf, props, metric, seed,
@@ -242,7 +245,7 @@ def knn_build(points, k: int, trees: int, leaf: int, props: int, metric: int = 0
 
 def knn_build_batch(datasets, k: int, trees: int, leaf: int, props: int, metric: int = 0,
                     seeds=None, precision: int = PREC_FP32, stats: bool = False, context=None,
-                    autotune: bool = False, leaf_tile: int = 0, prop_warps: int = 0):
+                    autotune: bool = False, leaf_tile: int = 0, prop_warps: int = 0, tc_group: int = 0):
     """k-NN graphs of many independent point sets in one call.
 
     ``datasets``: sequence of [n_i, d_i] arrays (all float32 or all float16);
@@ -267,7 +270,8 @@ def knn_build_batch(datasets, k: int, trees: int, leaf: int, props: int, metric:
         arr[i].out_dist = _ptr(dist)
     f16 = bool(xs) and xs[0].dtype == np.float16
     opt = default_options(dtype=F16 if f16 else F32, precision=precision,
-                          autotune=int(bool(autotune)), leaf_tile=leaf_tile, prop_warps=prop_warps)
+                          autotune=int(bool(autotune)), leaf_tile=leaf_tile, prop_warps=prop_warps,
+                          tc_group=tc_group)
     st = KnnStats()
     st.struct_size = ctypes.sizeof(KnnStats)
     _check(load_library().knn_build_batch(context, arr, len(xs), k, trees, leaf, props, metric,

@@ -174,7 +174,8 @@ bool save_result(const std::string& out, const std::vector<int32_t>& idx, const 
 
 // Knobs the reference does not have come from the environment so that the
 // positional command line stays the reference's:
-//   ACKNN_PRECISION  fp32 (default) | bf16   leaf blocks in FP32 or BF16 tiles + FP32 re-rank
+//   ACKNN_PRECISION  fp32 (default) | bf16 | f16   leaf blocks in FP32, or in BF16 / FP16
+//                    tensor-core tiles + FP32 re-rank
 //   ACKNN_SPLITS     median (default) | reference | learned
 //   ACKNN_SEED       unsigned integer, default 0
 //   ACKNN_TIMING     1: report the wall time of CSV ingest, build and file
@@ -185,8 +186,9 @@ bool env_knobs(knn_options& opt, uint64_t& seed) {
     const std::string s = v;
     if (s == "fp32") opt.precision = KNN_PREC_FP32;
     else if (s == "bf16") opt.precision = KNN_PREC_BF16_RERANK;
+    else if (s == "f16") opt.precision = KNN_PREC_F16_RERANK;
     else {
-      std::cout << "ACKNN_PRECISION must be fp32 or bf16\n";
+      std::cout << "ACKNN_PRECISION must be fp32, bf16 or f16\n";
       return false;
     }
   }

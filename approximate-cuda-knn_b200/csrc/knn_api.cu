@@ -75,6 +75,8 @@ struct knn_context {
   std::vector<std::string> seen;
   // Autotuned launch shapes by workload key: (FP32 leaf tile, propagation warps).
   std::map<std::string, std::pair<int, int>> tuned;
+  // Tuned sibling leaves per tensor-core tile, by workload key and precision.
+  std::map<std::string, int> tuned_group;
   cudaEvent_t tev[2] = {};
   // Device error words: [0] is cleared at the start of every build and tells
   // the tensor-core tile kernels of that build to stop issuing work; [1] is
@@ -382,6 +384,7 @@ struct Layout {
   knn::SegView segs;
   int64_t leaves = 1, maxleaf = 1;
   int64_t maxblock = 0;  // bound on the points of a leaf block (0: unknown)
+  int tc_group_max = 1;  // sibling leaves a tensor-core tile may hold (1, 2 or 4)
   // reference-rule trees: explicit leaf table (device) and per-tree offsets / counts (host)
   const int64_t* ftable = nullptr;
   const int64_t* foff = nullptr;
@@ -395,6 +398,24 @@ int64_t host_max_block(int64_t n, int depth, int k) {
   int l = depth;
   while (l > 0 && (n >> l) < k + 1) --l;
   return (n + (int64_t(1) << l) - 1) >> l;
+}
+
+// Largest group of sibling leaves (1, 2 or 4) that one 128-row tensor-core
+// tile can take with every leaf its own block: leaves of at most 128 / G
+// points, the smallest leaf of every segment (floor(n / 2^depth) points)
+// holding k+1, and every segment at least log2 G levels deep so that groups
+// never straddle two sets.
+int tc_group_max(const knn::SegEntry* hsegs, int nseg, int k, int64_t maxleaf) {
+  int g = 1;
+  for (int cand = 2, lg = 1; cand <= 4; cand *= 2, ++lg) {
+    if (maxleaf * cand > 128) break;
+    bool ok = true;
+    for (int i = 0; i < nseg && ok; ++i)
+      ok = hsegs[i].depth >= lg && (hsegs[i].n >> hsegs[i].depth) >= k + 1;
+    if (!ok) break;
+    g = cand;
+  }
+  return g;
 }
 
 Layout single_layout(int64_t n, int depth) {
@@ -443,7 +464,8 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
 // approximate candidates over all trees; FP32 re-rank keeps the exact best k.
 int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, int trees,
                   const Layout& lay, int metric, int precision, const int32_t* perm, const float* norms,
-                  Lists* L, int* err_flag, cudaStream_t st, knn::LaunchLog& log, cudaEvent_t* kev = nullptr) {
+                  Lists* L, int* err_flag, cudaStream_t st, knn::LaunchLog& log, cudaEvent_t* kev = nullptr,
+                  int tc_group = 1) {
   const int kw = (k + 31) / 32;
   const int kq = k <= 16 ? 2 * k : 32;
   const int Kp = ((d + 63) / 64) * 64;
@@ -459,6 +481,7 @@ int run_leaf_umma(knn_context* C, const float* X, int64_t n, int d, int dpad, in
   a.leaves = lay.leaves;
   a.maxleaf = lay.maxleaf;
   a.maxblock = lay.maxblock > 0 ? lay.maxblock : INT64_MAX;
+  a.tc_group = std::min(std::max(tc_group, 1), lay.tc_group_max);
   a.ftable = lay.ftable;
   a.foff = lay.foff;
   a.fcount = lay.fcount;
@@ -588,16 +611,62 @@ int tune_prop_warps(knn_context* C, const float* X, int64_t n, int d, int dpad, 
 // cached, or tuned now (when allowed).
 struct Shapes {
   int leaf_tile = 0, prop_warps = 0;
+  int tc_group = 0;  // tensor-core tiles: sibling leaves per tile
 };
+
+// Sibling leaves per tensor-core tile (results identical for every choice):
+// each allowed group is run twice over the first tree into the spare lists,
+// the second run timed.
+int tune_tc_group(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, const Layout& lay,
+                  int metric, int precision, const int32_t* perm, const float* norms, const Lists& L,
+                  int* err_flag, cudaStream_t st, int* best) {
+  Lists S = L;
+  S.cur = 1 - L.cur;
+  float best_ms = 3.4e38f;
+  *best = lay.tc_group_max;
+  for (int g = lay.tc_group_max; g >= 1; g /= 2) {
+    float ms = 0;
+    for (int rep = 0; rep < 2; ++rep) {
+      knn::LaunchLog tl;
+      KNN_CK(cudaEventRecord(C->tev[0], st));
+      int rc = run_leaf_umma(C, X, n, d, dpad, k, 1, lay, metric, precision, perm, norms, &S, err_flag, st, tl,
+                             nullptr, g);
+      if (!rc) rc = time_since(C, st, &ms);
+      if (rc) return rc;
+    }
+    if (ms < best_ms) {
+      best_ms = ms;
+      *best = g;
+    }
+  }
+  return KNN_OK;
+}
 
 int pick_shapes(knn_context* C, const knn_options& o, bool may_tune, bool fp32_leaf, int props, const float* X,
                 int64_t n, int d, int dpad, int k, const Layout& lay, int metric, const int32_t* perm,
-                const float* norms, Lists* L, cudaStream_t st, Shapes* sh, bool* tune_prop_after) {
+                const float* norms, Lists* L, cudaStream_t st, Shapes* sh, bool* tune_prop_after,
+                int* err_flag) {
   sh->leaf_tile = o.leaf_tile;
   sh->prop_warps = o.prop_warps;
   *tune_prop_after = false;
-  if (!o.autotune) return KNN_OK;
   const std::string key = tune_key(metric, d, k, lay.maxleaf);
+  if (!fp32_leaf) {
+    // tensor-core tiles: forced, cached, tuned (eager calls with autotune), or the largest group
+    const std::string gkey = key + ":q" + std::to_string(o.precision);
+    auto gi = C->tuned_group.find(gkey);
+    if (o.tc_group) sh->tc_group = o.tc_group;
+    else if (gi != C->tuned_group.end()) sh->tc_group = gi->second;
+    else if (o.autotune && may_tune && lay.tc_group_max > 1) {
+      int rc = tune_tc_group(C, X, n, d, dpad, k, lay, metric, o.precision, perm, norms, *L, err_flag, st,
+                             &sh->tc_group);
+      if (rc) return rc;
+      C->tuned_group[gkey] = sh->tc_group;
+    } else {
+      sh->tc_group = lay.tc_group_max;
+    }
+    sh->tc_group = std::min(sh->tc_group, lay.tc_group_max);
+  }
+  if (!o.autotune) return KNN_OK;
   auto it = C->tuned.find(key);
   if (it != C->tuned.end()) {
     if (!sh->leaf_tile) sh->leaf_tile = it->second.first;
@@ -748,6 +817,8 @@ int resolve_options(const knn_options* opt, knn_options* o) {
   if (o->tree_offset < 0 || o->tree_stride < 0) return fail(KNN_ERR_ARGS, "negative tree offset or stride");
   if (o->raw_keys < 0 || o->raw_keys > 1) return fail(KNN_ERR_ARGS, "raw_keys must be 0 or 1");
   if (o->split_rule < 0 || o->split_rule > 1) return fail(KNN_ERR_ARGS, "unknown split rule");
+  if (o->tc_group != 0 && o->tc_group != 1 && o->tc_group != 2 && o->tc_group != 4)
+    return fail(KNN_ERR_ARGS, "tc_group must be 0, 1, 2 or 4");
   if (o->split_rule == KNN_SPLIT_REFERENCE && o->learned_splits)
     return fail(KNN_ERR_UNSUPPORTED, "reference-rule splits and learned splits do not combine");
   return KNN_OK;
@@ -850,18 +921,25 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
                            d <= 256 && k <= 32;
   Layout lay = single_layout(n, T.depth);
   lay.maxblock = host_max_block(n, T.depth, k);
+  {
+    knn::SegEntry e{};
+    e.n = n;
+    e.depth = T.depth;
+    lay.tc_group_max = tc_group_max(&e, 1, k, lay.maxleaf);
+  }
   if (ftab_d) {
     lay.ftable = ftab_d;
     lay.foff = foff_h.data();
     lay.fcount = fcount_h.data();
     lay.maxleaf = leaf;
+    lay.tc_group_max = 1;
   }
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   KNN_CK(cudaStreamIsCapturing(st, &cs));
   Shapes sh;
   bool tune_prop = false;
   rc = pick_shapes(C, o, cs == cudaStreamCaptureStatusNone, !tensor_leaf, props, P.X, n, d, P.dpad, k, lay,
-                   metric, T.perm, norms, &L, st, &sh, &tune_prop);
+                   metric, T.perm, norms, &L, st, &sh, &tune_prop, err_flag);
   if (rc) return rc;
   cudaEvent_t* kev = nullptr;  // per-tree tile-kernel events for the statistics
   if (timed && cs == cudaStreamCaptureStatusNone) {
@@ -870,7 +948,7 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
   }
   if (tensor_leaf) {
     rc = run_leaf_umma(C, P.X, n, d, P.dpad, k, trees, lay, metric, o.precision, T.perm, norms, &L, err_flag, st,
-                       log, kev);
+                       log, kev, sh.tc_group);
   } else {
     rc = run_leaf(C, P.X, n, d, P.dpad, k, trees, lay, metric, T.perm, norms, &L, stats ? counters : nullptr, st,
                   log, sh.leaf_tile, kev);
@@ -950,6 +1028,7 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
     stats->props_run = props;
     stats->leaf_tile = tensor_leaf ? 128 : (sh.leaf_tile ? sh.leaf_tile : 64);
     stats->leaf_path = tensor_leaf ? o.precision : 0;
+    stats->tc_group = tensor_leaf ? std::min(std::max(sh.tc_group, 1), lay.tc_group_max) : 0;
     stats->leaf_fallback = (o.precision != KNN_PREC_FP32 && !tensor_leaf) ? 1 : 0;
     stats->prop_warps = sh.prop_warps;
     unsigned long long host[2 + KNN_MAX_PROPS];
@@ -1053,16 +1132,17 @@ int group_compute(knn_context* C, const BatchGroup& g, int k, int trees, int pro
   lay.leaves = g.leaves;
   lay.maxleaf = g.maxleaf;
   for (const auto& e : g.hsegs) lay.maxblock = std::max(lay.maxblock, host_max_block(e.n, e.depth, k));
+  lay.tc_group_max = tc_group_max(g.hsegs.data(), (int)g.hsegs.size(), k, g.maxleaf);
   const bool tensor_leaf = precision != KNN_PREC_FP32 && metric != KNN_METRIC_TAXICAB && g.d <= 256 &&
                            k <= 32;
   Shapes sh;
   bool tune_prop = false;
   rc = pick_shapes(C, o, may_tune, !tensor_leaf, props, X, g.ntot, g.d, g.dpad, k, lay, metric, T.perm, norms, &L,
-                   st, &sh, &tune_prop);
+                   st, &sh, &tune_prop, err_flag);
   if (rc) return rc;
   if (tensor_leaf)
     rc = run_leaf_umma(C, X, g.ntot, g.d, g.dpad, k, trees, lay, metric, precision, T.perm, norms, &L, err_flag,
-                       st, log);
+                       st, log, nullptr, sh.tc_group);
   else
     rc = run_leaf(C, X, g.ntot, g.d, g.dpad, k, trees, lay, metric, T.perm, norms, &L, nullptr, st, log,
                   sh.leaf_tile);

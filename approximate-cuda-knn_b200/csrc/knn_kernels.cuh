@@ -119,6 +119,7 @@ struct UmmaLeafArgs {
   SegView segs;
   int64_t leaves, maxleaf;  // leaf blocks per tree; points in the largest leaf
   int64_t maxblock;         // points in the largest leaf block (median trees)
+  int tc_group;             // sibling leaves per 128-row tile: 1, 2 or 4 (each leaf its own block)
   const int32_t* perm;   // [trees][n]
   const float* norms;    // [n] FP32 norms (COSINE) or null
   bool f16;              // operands FP16 (else BF16)

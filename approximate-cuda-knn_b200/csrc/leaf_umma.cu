@@ -230,7 +230,7 @@ template <int METRIC, bool FIRST>
 __global__ void __launch_bounds__(kUThreads, 2)
     k_leaf_tc(const uint16_t* __restrict__ Xb, uint32_t idesc, int Kp, SegView segs,
               const int64_t* __restrict__ ftab, int k, int kq,
-              int qtiles, const int32_t* __restrict__ perm, const int32_t* __restrict__ inv,
+              int qtiles, int glog, const int32_t* __restrict__ perm, const int32_t* __restrict__ inv,
               const float* __restrict__ norms2, float* __restrict__ akey, uint32_t* __restrict__ aid,
               int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -248,6 +248,9 @@ __global__ void __launch_bounds__(kUThreads, 2)
   float* cmax2 = reinterpret_cast<float*>(msk + kBM * 2);      // [2][4] largest candidate norm per warp
   uint16_t* xp = reinterpret_cast<uint16_t*>(cmax2 + 8);       // [128][kXS] listed columns
   float* tcap = reinterpret_cast<float*>(xp + kBM * kXS);      // [128] first tree: bound on the kq-th key
+  // [128][2] grouped leaves: the row's own columns (in the listed-column area,
+  // unused then: a grouped tile is one column tile, so xcl is off)
+  int16_t* rcol = reinterpret_cast<int16_t*>(xp);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(tcap + kBM);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
   int* status = reinterpret_cast<int*>(tmem_slot + 1);
@@ -262,10 +265,32 @@ __global__ void __launch_bounds__(kUThreads, 2)
     hi = e[1];
     blo = e[2];
     bhi = e[3];
-  } else {
+  } else if (glog == 0) {
     int64_t j;
     const SegEntry seg = segs.leaf(leaf, &j);
     leaf_block(seg, j, k, &lo, &hi, &blo, &bhi);
+  } else {
+    // 2^glog sibling leaves, each its own block (the host checks that every
+    // leaf holds k+1 points), as one tile: a row keeps only its own leaf's
+    // columns (rcol)
+    int64_t j;
+    const SegEntry seg = segs.leaf(leaf << glog, &j);
+    lo = blo = seg.off + node_lo(seg.n, seg.depth, j);
+    hi = bhi = seg.off + node_lo(seg.n, seg.depth, j + (int64_t(1) << glog));
+    if (threadIdx.x < kBM) {
+      const int64_t p = lo + threadIdx.x;
+      int64_t a = lo, b = lo;
+      for (int g = 0; g < (1 << glog); ++g) {
+        const int64_t e = seg.off + node_lo(seg.n, seg.depth, j + g + 1);
+        if (p < e) {
+          b = e;
+          break;
+        }
+        a = e;
+      }
+      rcol[2 * threadIdx.x] = (int16_t)(a - blo);
+      rcol[2 * threadIdx.x + 1] = (int16_t)(b - blo);
+    }
   }
   const int nq = (int)(hi - lo);
   const int q0 = qt * kBM;
@@ -276,7 +301,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
   // Listed ids are located up front only in blocks of several tiles: in a
   // one-tile block the few survivors are cheaper to check by the merge's ballot.
   const bool xcl = !FIRST && inv != nullptr && nb > kBN && nb <= kXMaxBlock;  // block-uniform
-  const bool pre = FIRST && nb >= kPrepassMin;
+  const bool pre = FIRST && nb >= kPrepassMin && glog == 0;
   const int nsteps = pre ? 2 * ntiles : ntiles;
   const float kInf = __int_as_float(0x7F800000);
   const float kMaxF = __int_as_float(0x7F7FFFFF);
@@ -494,6 +519,11 @@ __global__ void __launch_bounds__(kUThreads, 2)
             // the row's own point (its leaf lies inside the block) never survives
             const int64_t selfbit = (lo + q0 + r) - blo - c0 - col0;
             if (selfbit >= 0 && selfbit < 32) mask &= ~(1u << (int)selfbit);
+            if (glog) {  // grouped leaves: the row's own leaf's columns only
+              const int a = min(max((int)rcol[2 * r] - (c0 + col0), 0), 32);
+              const int b = min(max((int)rcol[2 * r + 1] - (c0 + col0), 0), 32);
+              mask &= (uint32_t)(((1ull << b) - 1ull) ^ ((1ull << a) - 1ull));
+            }
             if (xcl) {
               // listed ids among these 32 columns: walk the row's sorted
               // positions (each thread's columns only increase)
@@ -808,11 +838,14 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
   const uint32_t idesc = idesc_for(a.f16);
   const size_t smem = umma_smem_bytes(Kp);
   const int64_t leaves = a.leaves;
-  const int qtiles = (int)((a.maxleaf + kBM - 1) / kBM);
+  // 2^glog sibling leaves per tile (the caller checks it is allowed)
+  const int glog = a.tc_group >= 4 ? 2 : a.tc_group == 2 ? 1 : 0;
+  if (glog && (a.ftable || (a.maxleaf << glog) > kBM)) return KNN_ERR_UNSUPPORTED;
+  const int qtiles = glog ? 1 : (int)((a.maxleaf + kBM - 1) / kBM);
   for (int t = 0; t < a.trees; ++t) {
     const int32_t* perm = a.perm + (size_t)t * a.n;
     const int64_t* ftab = a.ftable ? a.ftable + 4 * a.foff[t] : nullptr;
-    const int64_t tleaves = a.ftable ? a.fcount[t] : leaves;
+    const int64_t tleaves = a.ftable ? a.fcount[t] : (leaves >> glog);
     if (tleaves <= 0) {
       if (a.kev) {
         cudaEventRecord(a.kev[2 * t], st);
@@ -830,7 +863,8 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
 #define KNN_TC_LAUNCH(M, F)                                                                               \
   do {                                                                                                    \
     cudaFuncSetAttribute(k_leaf_tc<M, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);       \
-    k_leaf_tc<M, F><<<grid, kUThreads, smem, st>>>(Xb, idesc, Kp, a.segs, ftab, a.k, a.kq, qtiles, perm, inv, a.norms2, \
+    k_leaf_tc<M, F><<<grid, kUThreads, smem, st>>>(Xb, idesc, Kp, a.segs, ftab, a.k, a.kq, qtiles, glog, perm, inv, \
+                                                   a.norms2,                                                          \
                                                    a.akey, a.aid, a.err);                                \
   } while (0)
     if (a.kev) cudaEventRecord(a.kev[2 * t], st);

@@ -102,7 +102,11 @@ typedef struct knn_options {
   int32_t raw_keys;          /* 1: out_dist receives the ranking keys (squared L2 for
                                 EUCLIDEAN) instead of distances                       */
   int32_t split_rule;        /* KNN_SPLIT_MEDIAN (default) or KNN_SPLIT_REFERENCE     */
-  int32_t reserved[3];
+  int32_t tc_group;          /* tensor-core leaf tiles: sibling leaves per 128-row tile,
+                                1, 2 or 4 (0: tuned with autotune, else the most that
+                                fit); a row keeps its own leaf's columns, so results do
+                                not depend on it; capped at what the leaves allow      */
+  int32_t reserved[2];
 } knn_options;
 
 typedef struct knn_stats {
@@ -126,7 +130,9 @@ typedef struct knn_stats {
   int32_t leaf_path;         /* leaf stage that ran: 0 FP32 CUDA cores, 1 BF16 tensor-core
                                 tiles, 2 FP16 tensor-core tiles                        */
   int32_t leaf_fallback;     /* 1: tensor-core precision was asked for, FP32 ran        */
-  int64_t reserved[5];
+  int32_t tc_group;          /* sibling leaves per tensor-core tile used (0: FP32 path) */
+  int32_t reserved32;
+  int64_t reserved[4];
 } knn_stats;
 
 typedef struct knn_context knn_context;

@@ -94,6 +94,7 @@ def test_cli_matches_library_and_mirror(hello, tmp_path, metric):
 @pytest.mark.gpu
 @pytest.mark.parametrize("env, kw", [
     ({"ACKNN_PRECISION": "bf16", "ACKNN_SEED": "11"}, {"precision": 1, "seed": 11}),
+    ({"ACKNN_PRECISION": "f16", "ACKNN_TIMING": "1"}, {"precision": 2}),
     ({"ACKNN_SPLITS": "reference", "ACKNN_SEED": "3"}, {"split_rule": 1, "seed": 3}),
 ])
 def test_cli_environment_knobs(hello, tmp_path, env, kw):

@@ -122,3 +122,52 @@ def test_precision_stats_report_the_leaf_path(lib):
                                          (lib.PREC_F16_RERANK, 2, 2, 0), (lib.PREC_BF16_RERANK, 1, 0, 1)):
         _, _, st = lib.knn_build(x, 6, 2, 64, 1, metric, precision=prec, stats=True)
         assert (st["leaf_path"], st["leaf_fallback"]) == (path, fallback)
+
+
+@pytest.mark.parametrize("metric", [0, 2])
+@pytest.mark.parametrize("n,d,k,leaf", [(20000, 64, 10, 48), (30000, 96, 10, 64), (9000, 32, 8, 30),
+                                        (5000, 128, 15, 40)])
+def test_grouped_sibling_leaves_equal_single_leaf_tiles(lib, metric, n, d, k, leaf):
+    """Two or four sibling leaves in one 128-row tile (each row masked to its
+    own leaf's columns) give the one-leaf-per-tile graph bit for bit."""
+    x = lib.workloads.gaussian_mixture(n, d, 16, seed=n + leaf)
+    want = None
+    for g in (1, 2, 4):
+        for prec in (lib.PREC_BF16_RERANK, lib.PREC_F16_RERANK):
+            opts = dict(precision=prec, tc_group=g)
+            gi, gd, st = lib.knn_build(x, k, 4, leaf, 1, metric, seed=3, stats=True, **opts)
+            assert st["tc_group"] <= g
+            key = prec
+            if g == 1:
+                want = want or {}
+                want[key] = (gi, gd)
+            else:
+                np.testing.assert_array_equal(gi, want[key][0])
+                np.testing.assert_array_equal(gd.view(np.uint32), want[key][1].view(np.uint32))
+
+
+def test_grouped_tiles_in_batches_and_on_exact_data(lib):
+    """Batches of sets with different depths: each set's graph is its single
+    build's with any group; on exact-integer data every grouping equals the
+    plain FP32 graph."""
+    xs = [_ints(3000 + 1100 * i, 32, 40 + i) for i in range(5)]
+    base = lib.knn_build_batch(xs, 12, 3, 48, 1, 0, seeds=list(range(5)), precision=lib.PREC_BF16_RERANK,
+                               tc_group=1)
+    for g in (2, 4):
+        got = lib.knn_build_batch(xs, 12, 3, 48, 1, 0, seeds=list(range(5)), precision=lib.PREC_BF16_RERANK,
+                                  tc_group=g)
+        for (bi, bd), (gi, gd) in zip(base, got):
+            np.testing.assert_array_equal(bi, gi)
+            np.testing.assert_array_equal(bd.view(np.uint32), gd.view(np.uint32))
+    for i, x in enumerate(xs):
+        pi, pd = lib.knn_build(x, 12, 3, 48, 1, 0, seed=i)
+        np.testing.assert_array_equal(base[i][0], pi)
+        np.testing.assert_array_equal(base[i][1].view(np.uint32), pd.view(np.uint32))
+
+
+def test_grouped_tiles_autotuned(lib):
+    x = lib.workloads.gaussian_mixture(40000, 64, 16, seed=5)
+    a = lib.knn_build(x, 10, 3, 40, 1, 0, precision=lib.PREC_BF16_RERANK, autotune=True)
+    b = lib.knn_build(x, 10, 3, 40, 1, 0, precision=lib.PREC_BF16_RERANK, tc_group=1)
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
