@@ -21,13 +21,14 @@
 //     accumulators so that one tile's MMA overlaps the previous tile's rounds;
 //   * completion: tcgen05.commit -> mbarrier, waited with an iteration limit
 //     (on expiry the block records an error, drains, frees TMEM and returns);
-//   * epilogue: per 64-column round, tcgen05.ld 32x32b.x32 by all 8 warps (warp
-//     w reads lane quarter w%4, 32 columns); three instructions per key filter
-//     it against a slightly widened bound of the row's current last entry into
-//     a survivor bit mask, then the warps of each lane quarter read their
-//     rows' few survivors back from tensor memory, compute their exact keys
-//     and insert them into the query's sorted list (held in shared memory for
-//     the whole block) with one ballot and one lane shift each.
+//   * epilogue: per tile, tcgen05.ld 32x32b.x32 twice by all 8 warps (warp
+//     w reads lane quarter w%4, two 32-column slices); three instructions per
+//     key filter it against a slightly widened bound of the row's last entry
+//     into a survivor bit mask, then (while the next tile's MMA runs) the warps
+//     of each lane quarter read their rows' few survivors back from tensor
+//     memory, compute their exact keys and insert them into the query's sorted
+//     list (held in shared memory for the whole block) with one ballot and one
+//     lane shift each.  Two block barriers per tile.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -45,12 +46,12 @@ constexpr int kKC = 64;               // bf16 per 128-byte swizzled row
 constexpr int kChunkBytes = kBM * 128; // one 128 x 64 bf16 operand chunk
 constexpr uint32_t kTmemCols = 256;  // two 128-column accumulators
 constexpr int kUThreads = 256;
-constexpr int kRound = 64;          // tile columns per epilogue round
-constexpr int kBulkMerge = 12;      // first tree: survivors in a half round from which sort + merge pays
+constexpr int kRound = 64;          // tile columns per epilogue slice pair
+constexpr int kBulkMerge = 12;      // first tree: survivors in a 32-column slice from which sort + merge pays
 constexpr float kSlack = 4.76837158203125e-07f;  // 2^-21: filter widening, eight units of FP32 rounding
 // Listed candidates inside the block, per row: sorted 16-bit column positions
 // ending in kXEnd (blocks of up to kXMaxBlock columns).
-constexpr int kXS = 34;
+constexpr int kXS = 33;
 constexpr uint32_t kXEnd = 0xFFFFu;
 constexpr int kXMaxBlock = 65000;
 // First tree: blocks of at least kPrepassMin columns get a bounding pass; its
@@ -162,20 +163,28 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-// Stage `rows` gathered rows (ids in `ids`, <0: zero row) of the BF16 copy into
-// a K-major 128B-swizzled operand of Kp/64 chunks.
+// Stage 128 gathered rows (ids in `ids`, <0: zero row) of the 16-bit copy
+// into a K-major 128B-swizzled operand of NCH 64-element chunks.  Thread t
+// always stages the same 16-byte unit (t mod 8 NCH) of rows t / (8 NCH) + i *
+// R, R = the rows one pass of the threads covers.
+template <int NCH>
 __device__ __forceinline__ void stage_operand(unsigned char* op, const uint16_t* __restrict__ Xb,
-                                              int Kp, const int32_t* ids) {
-  const int units = kBM * (Kp / 8);  // 16-byte units
+                                              const int32_t* ids) {
+  constexpr int kUnitsPerRow = 8 * NCH;       // 16-byte units per row
+  constexpr int kRowsPerPass = kUThreads / kUnitsPerRow;
+  constexpr int kActive = kRowsPerPass * kUnitsPerRow;  // all 256 threads but for NCH = 3 (240)
   const uint32_t base = smem_u32(op);
-  for (int u = threadIdx.x; u < units; u += kUThreads) {
-    const int r = u / (Kp / 8);
-    const int c16 = u - r * (Kp / 8);  // 16-byte unit along K
+  if (threadIdx.x < kActive) {
+    const int c16 = threadIdx.x % kUnitsPerRow;
     const int chunk = c16 >> 3, w = c16 & 7;
-    const uint32_t dst = base + chunk * kChunkBytes + r * 128 + ((w ^ (r & 7)) << 4);
-    const int32_t id = ids[r];
-    const uint16_t* src = Xb + (size_t)(id < 0 ? 0 : id) * Kp + c16 * 8;
-    cp_async16(dst, src, id < 0 ? 0 : 16);
+    const int r0 = threadIdx.x / kUnitsPerRow;
+#pragma unroll
+    for (int r = r0; r < kBM; r += kRowsPerPass) {
+      const uint32_t dst = base + chunk * kChunkBytes + r * 128 + ((w ^ (r & 7)) << 4);
+      const int32_t id = ids[r];
+      const uint16_t* src = Xb + (size_t)(id < 0 ? 0 : id) * (NCH * kKC) + c16 * 8;
+      cp_async16(dst, src, id < 0 ? 0 : 16);
+    }
   }
   asm volatile("cp.async.commit_group;\n" ::);
 }
@@ -200,22 +209,23 @@ __device__ __forceinline__ uint32_t warp_sort32_u32(uint32_t v) {
 // One block per (leaf, 128-query tile), stepping over the block's 128-column
 // candidate tiles.  The 128 queries' lists stay in shared memory for the whole
 // block (read once, written once).  Each step empties one 128x128 tensor-core
-// tile (tensor memory, two 128-column buffers) in two 64-column rounds:
-//   * epilogue: thread (row, 32-column half) loads its products
-//     (tcgen05.ld 32x32b.x32), filters them against a conservative bound of
-//     the row's list tail into a survivor bit mask (three instructions per
-//     key), drops the row's own column and listed ids;
+// tile (tensor memory, two 128-column buffers):
+//   * epilogue: thread (row, 32-column half) loads the products of its two
+//     32-column slices (tcgen05.ld 32x32b.x32), filters them against a
+//     conservative bound of the row's list tail at the step's start into
+//     survivor bit masks (three instructions per key), drops the row's own
+//     column and listed ids;
 //   * merge: the warps of the rows' lane quarter insert each row's survivors,
 //     reading their products back from tensor memory (tcgen05.ld x1 per
 //     survivor, or x32 and a lane transpose for a bulk batch), computing the
 //     exact keys and applying the exact (key, id) rule.
-// The next step's operand is staged while round 0 runs (its MMA has
+// The next step's operand is staged while the epilogue runs (its MMA has
 // completed), and its MMA runs into the other tensor-memory buffer during
-// round 1.  MMA issue, bounded waits and the tensor-memory loads follow the
+// the merge.  MMA issue, bounded waits and the tensor-memory loads follow the
 // single-tile sequence that was checked on its own against a CPU product.
 // FIRST: the launch of the first tree, whose lists start empty; a point then
 // meets every candidate once, so no survivor can already be listed, and a
-// half round with many survivors is sorted and merged into the list in one go.
+// 32-column slice with many survivors is sorted and merged into the list in one go.
 // Blocks of kPrepassMin columns or more first run all tiles once (pass 0) to
 // record each row's smallest exact key in each of kGroups column groups
 // (32-column slices, wrapping); the kq-th smallest group minimum is the key of
@@ -226,27 +236,27 @@ __device__ __forceinline__ uint32_t warp_sort32_u32(uint32_t v) {
 // id) and masked out of the survivors, so the merge needs no duplicate check;
 // a candidate meets a row once per tree, so ids inserted during the block
 // cannot come back.
-template <int METRIC, bool FIRST>
+template <int METRIC, bool FIRST, int NCH>
 __global__ void __launch_bounds__(kUThreads, 2)
-    k_leaf_tc(const uint16_t* __restrict__ Xb, uint32_t idesc, int Kp, SegView segs,
+    k_leaf_tc(const uint16_t* __restrict__ Xb, uint32_t idesc, SegView segs,
               const int64_t* __restrict__ ftab, int k, int kq,
               int qtiles, int glog, const int32_t* __restrict__ perm, const int32_t* __restrict__ inv,
               const float* __restrict__ norms2, float* __restrict__ akey, uint32_t* __restrict__ aid,
               int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  const int nchunks = Kp / kKC;
+  constexpr int nchunks = NCH;
   unsigned char* opA = smem;
   unsigned char* opB = opA + nchunks * kChunkBytes;
   float* Lk = reinterpret_cast<float*>(opB + nchunks * kChunkBytes);  // [128][kLS] list keys
   uint32_t* Li = reinterpret_cast<uint32_t*>(Lk + kBM * kLS);         // [128][kLS] list ids
   int32_t* qid = reinterpret_cast<int32_t*>(Li + kBM * kLS);
   float* qn = reinterpret_cast<float*>(qid + kBM);
-  int32_t* cid2 = reinterpret_cast<int32_t*>(qn + kBM);  // [2][128] candidate ids per step parity
-  float* cn2 = reinterpret_cast<float*>(cid2 + 2 * kBN);  // [2][128] norms (EUCLIDEAN) or 0; +inf: padding
-  uint32_t* msk = reinterpret_cast<uint32_t*>(cn2 + 2 * kBN);  // [128][2] survivor bits of the round
-  float* cmax2 = reinterpret_cast<float*>(msk + kBM * 2);      // [2][4] largest candidate norm per warp
-  uint16_t* xp = reinterpret_cast<uint16_t*>(cmax2 + 8);       // [128][kXS] listed columns
+  int32_t* cid3 = reinterpret_cast<int32_t*>(qn + kBM);  // [3][128] candidate ids, slot = step mod 3
+  float* cn3 = reinterpret_cast<float*>(cid3 + 3 * kBN);  // [3][128] norms (EUCLIDEAN) or 0; +inf: padding
+  uint32_t* msk = reinterpret_cast<uint32_t*>(cn3 + 3 * kBN);  // [128][4] survivor bits of the step's tile
+  float* cmax3 = reinterpret_cast<float*>(msk + kBM * 4);      // [3][4] largest candidate norm per warp
+  uint16_t* xp = reinterpret_cast<uint16_t*>(cmax3 + 12);      // [128][kXS] listed columns
   float* tcap = reinterpret_cast<float*>(xp + kBM * kXS);      // [128] first tree: bound on the kq-th key
   // [128][2] grouped leaves: the row's own columns (in the listed-column area,
   // unused then: a grouped tile is one column tile, so xcl is off)
@@ -325,7 +335,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
     qn[tid] = (METRIC == KNN_METRIC_EUCLIDEAN && id >= 0) ? norms2[id] : 0.f;
     tcap[tid] = kInf;
   }
-  // candidates of step s (warps 0-3, whole warps) into parity slot s & 1
+  // candidates of step s (warps 0-3, whole warps) into slot s mod 3;
   // fetch_cols loads them into registers (a step ahead), put_cols stores them
   int32_t nid = -1;
   float nnv = 0.f;
@@ -335,11 +345,11 @@ __global__ void __launch_bounds__(kUThreads, 2)
     nnv = (METRIC == KNN_METRIC_EUCLIDEAN && nid >= 0) ? norms2[nid] : 0.f;
   };
   auto put_cols = [&](int s) {
-    cid2[(s & 1) * kBN + tid] = nid;
-    cn2[(s & 1) * kBN + tid] = nid >= 0 ? nnv : kInf;
+    cid3[(s % 3) * kBN + tid] = nid;
+    cn3[(s % 3) * kBN + tid] = nid >= 0 ? nnv : kInf;
     // norms are >= 0, so their bit patterns order as unsigned integers
     const uint32_t wm = __reduce_max_sync(0xFFFFFFFFu, __float_as_uint(nnv));
-    if (lane == 0) cmax2[(s & 1) * 4 + warp] = __uint_as_float(wm);
+    if (lane == 0) cmax3[(s % 3) * 4 + warp] = __uint_as_float(wm);
   };
   if (tid < kBN) {
     fetch_cols(0);
@@ -347,8 +357,8 @@ __global__ void __launch_bounds__(kUThreads, 2)
     if (nsteps > 1) fetch_cols(1);
   }
   __syncthreads();
-  stage_operand(opA, Xb, Kp, qid);
-  stage_operand(opB, Xb, Kp, cid2);
+  stage_operand<NCH>(opA, Xb, qid);
+  stage_operand<NCH>(opB, Xb, cid3);
   if (pre) {
     for (int e = tid; e < kBM * kGS; e += kUThreads) gm[e] = kInf;
   } else {
@@ -425,6 +435,11 @@ __global__ void __launch_bounds__(kUThreads, 2)
   };
   if (tid == 0) issue_mma(0);
 
+  // Per step: [A] MMA(s) done -> stage B(s+1) -> epilogue over the tile's 128
+  // columns (two 32-column slices per thread) -> [B] -> MMA(s+1) issued ->
+  // merge of the step's survivors -> the next step's [A].  Candidate ids and
+  // norms live in three slots (step s in slot s mod 3): the merge of step s
+  // still reads its slot while step s+1 fills slot (s+2) mod 3.
   uint32_t phase = 0;
   for (int s = 0; s < nsteps; ++s) {
     const int pass = pre && s < ntiles ? 0 : 1;
@@ -441,183 +456,177 @@ __global__ void __launch_bounds__(kUThreads, 2)
       mbar_wait_bounded(bar, phase);  // let the MMAs drain before TMEM is freed
     }
     phase ^= 1u;
-    __syncthreads();
+    __syncthreads();  // [A]
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (*status != 0) break;  // uniform: read after the barrier
     // step s's MMA has completed: B is free for step s + 1
-    if (has_next) stage_operand(opB, Xb, Kp, cid2 + ((s + 1) & 1) * kBN);
-    const int32_t* cid = cid2 + (s & 1) * kBN;
-    const float* cn = cn2 + (s & 1) * kBN;
-    const float* cmx = cmax2 + (s & 1) * 4;
+    if (has_next) stage_operand<NCH>(opB, Xb, cid3 + ((s + 1) % 3) * kBN);
+    const int32_t* cid = cid3 + (s % 3) * kBN;
+    const float* cn = cn3 + (s % 3) * kBN;
+    const float* cmx = cmax3 + (s % 3) * 4;
     const float cm = fmaxf(fmaxf(cmx[0], cmx[1]), fmaxf(cmx[2], cmx[3]));
     const uint32_t tbuf = tmem + (uint32_t)((s & 1) * kBN);
     const int quarter = warp & 3, half = warp >> 2;
     const uint32_t tq = tbuf + ((uint32_t)(quarter * 32) << 16);  // this warp's lane quarter
-
-    for (int ri = 0; ri < 2; ++ri) {
-      const int rb = ri * kRound;
-      if (rb < mc) {
-        {
-          const int r = quarter * 32 + lane;
-          const int col0 = rb + half * 32;
-          uint32_t v[32];
-          tmem_ld32(tq + (uint32_t)col0, v);
-          const float4* cn4 = reinterpret_cast<const float4*>(cn + col0);
-          if (FIRST && pass == 0) {
-            // smallest exact key of these 32 columns (the row's own column
-            // left out) into the slice's group
-            const float myn = qn[r];
-            const int64_t sb = (lo + q0 + r) - blo - c0 - col0;
-            float m = kInf;
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              const float4 c = cn4[q];
-              const float cc[4] = {c.x, c.y, c.z, c.w};
-#pragma unroll
-              for (int e = 0; e < 4; ++e) {
-                const float dot = __uint_as_float(v[4 * q + e]);
-                const float key = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cc[e]))
-                                                                 : __fsub_rn(1.f + cc[e], dot);
-                m = (sb == 4 * q + e) ? m : fminf(m, key);
-              }
-            }
-            const int g = ((c0 / kBN) * 4 + ri * 2 + half) & (kGroups - 1);
-            gm[r * kGS + g] = fminf(gm[r * kGS + g], m);
-          } else {
-            // Row filter, a superset of what the exact rule (key <= the row's
-            // list tail tk) can admit: key' = |y|^2 - 2 x.y (EUCLIDEAN) or
-            // -x.y (COSINE) against thr = tk - |x|^2 (or tk - 1) widened by
-            // 2^-21 (|tk| + |x|^2 + max|y|^2), which bounds the rounding of
-            // both the key and the threshold.  Padding columns have key' =
-            // +inf, a row outside the block thr = -inf, a list with free slots
-            // thr = FLT_MAX.
-            const float tk = FIRST ? fminf(Lk[r * kLS + kq - 1], tcap[r]) : Lk[r * kLS + kq - 1];
-            float thr;
-            if (r >= mq) thr = -kInf;
-            else if (tk == kInf) thr = kMaxF;
-            else if (METRIC == KNN_METRIC_EUCLIDEAN) {
-              const float myn = qn[r];
-              thr = fminf((tk - myn) + kSlack * (fabsf(tk) + myn + cm), kMaxF);
-            } else {
-              thr = fminf((tk - 1.f) + kSlack * (fabsf(tk) + 2.f), kMaxF);
-            }
-            // bit j of neg = sign of thr - key'_j, shifted in from column 31 down
-            uint32_t neg = 0;
-#pragma unroll
-            for (int q = 7; q >= 0; --q) {
-              const float4 c = cn4[q];
-              const float cc[4] = {c.x, c.y, c.z, c.w};
-#pragma unroll
-              for (int e = 3; e >= 0; --e) {
-                const float dot = __uint_as_float(v[4 * q + e]);
-                const float kp =
-                    METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, cc[e]) : __fsub_rn(cc[e], dot);
-                neg = __funnelshift_l(__float_as_uint(__fsub_rn(thr, kp)), neg, 1);
-              }
-            }
-            uint32_t mask = ~neg;
-            // the row's own point (its leaf lies inside the block) never survives
-            const int64_t selfbit = (lo + q0 + r) - blo - c0 - col0;
-            if (selfbit >= 0 && selfbit < 32) mask &= ~(1u << (int)selfbit);
-            if (glog) {  // grouped leaves: the row's own leaf's columns only
-              const int a = min(max((int)rcol[2 * r] - (c0 + col0), 0), 32);
-              const int b = min(max((int)rcol[2 * r + 1] - (c0 + col0), 0), 32);
-              mask &= (uint32_t)(((1ull << b) - 1ull) ^ ((1ull << a) - 1ull));
-            }
-            if (xcl) {
-              // listed ids among these 32 columns: walk the row's sorted
-              // positions (each thread's columns only increase)
-              const int lo_c = c0 + col0;
-              uint32_t ex = 0;
-              int p = xp[r * kXS + xptr];
-              while (p < lo_c + 32) {
-                if (p >= lo_c) ex |= 1u << (p - lo_c);
-                p = xp[r * kXS + (++xptr)];
-              }
-              mask &= ~ex;
-            }
-            msk[r * 2 + half] = mask;
-          }
-        }
-        // Round 0 completes step s + 1's operand (staged since the top of the
-        // step) before its last barrier; its MMA is issued after that barrier.
-        const bool stage_here = ri == 0 && has_next;
-        if (stage_here && pass == 0) {
-          asm volatile("cp.async.wait_all;\n" ::: "memory");
-          asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        }
-        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        if (pass == 1) {
-          // The quarter's rows with survivors (one ballot) alternate between
-          // its two warps; survivors' products come from the warp's lane
-          // quarter of tensor memory.
-          const int rowq = quarter * 32 + lane;
-          const bool has = rowq < mq && (msk[rowq * 2] | msk[rowq * 2 + 1]) != 0;
-          const uint32_t all = __ballot_sync(0xFFFFFFFFu, has);
-          const bool mine = has && (__popc(all & ((1u << lane) - 1u)) & 1) == half;
-          uint32_t rows = __ballot_sync(0xFFFFFFFFu, mine);
-          while (rows) {
-            const int ql = __ffs(rows) - 1;  // row within the quarter
-            const int qq = quarter * 32 + ql;
-            rows &= rows - 1;
-            const uint32_t m0 = msk[qq * 2], m1 = msk[qq * 2 + 1];
-            float lk = Lk[qq * kLS + lane];
-            uint32_t li = Li[qq * kLS + lane];
-            const float myn = qn[qq];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              uint32_t bal = h ? m1 : m0;
-              if (bal == 0) continue;
-              const int cb = rb + h * 32;  // the half's first column in the tile
-              if (FIRST && __popc(bal) >= kBulkMerge) {
-                // lane j <- product of column cb + j of row qq
-                uint32_t v[32];
-                tmem_ld32(tq + (uint32_t)cb, v);
-                float dot = 0.f;
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                  const float t = __shfl_sync(0xFFFFFFFFu, __uint_as_float(v[j]), ql);
-                  if (lane == j) dot = t;
-                }
-                float ck = kInf;
-                uint32_t ci = kNoId;
-                if ((bal >> lane) & 1u) {
-                  ck = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[cb + lane]))
-                                                      : __fsub_rn(1.f, dot);
-                  ci = (uint32_t)cid[cb + lane];
-                }
-                warp_bitonic_sort32(ck, ci);
-                warp_merge_lower(lk, li, ck, ci);
-                continue;
-              }
-              while (bal) {
-                const int j = __ffs(bal) - 1;
-                bal &= bal - 1;
-                const float dot = __shfl_sync(0xFFFFFFFFu, __uint_as_float(tmem_ld1(tq + (uint32_t)(cb + j))), ql);
-                const float k1 = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[cb + j]))
-                                                                : __fsub_rn(1.f, dot);
-                const uint32_t i1 = (uint32_t)cid[cb + j];
-                const bool dup = !FIRST && !xcl && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
-                if (!dup) warp_insert1(lk, li, k1, i1);
-              }
-            }
-            Lk[qq * kLS + lane] = lk;
-            Li[qq * kLS + lane] = li;
-          }
-          if (stage_here) {
-            asm volatile("cp.async.wait_all;\n" ::: "memory");
-            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-          }
-          asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-          __syncthreads();
-          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        }
-        // step s + 1's operand has landed: its MMA runs during round 1
-        if (stage_here && tid == 0) issue_mma(s + 1);
+    const int r = quarter * 32 + lane;
+    // the row's filter bound (pass 1), from its list tail at the step's start
+    float thr = 0.f;
+    if (pass == 1) {
+      // Row filter, a superset of what the exact rule (key <= the row's
+      // list tail tk) can admit: key' = |y|^2 - 2 x.y (EUCLIDEAN) or
+      // -x.y (COSINE) against thr = tk - |x|^2 (or tk - 1) widened by
+      // 2^-21 (|tk| + |x|^2 + max|y|^2), which bounds the rounding of
+      // both the key and the threshold.  Padding columns have key' =
+      // +inf, a row outside the block thr = -inf, a list with free slots
+      // thr = FLT_MAX.  A bound from the step's start is looser than the
+      // current tail, never tighter, so the filter stays a superset.
+      const float tk = FIRST ? fminf(Lk[r * kLS + kq - 1], tcap[r]) : Lk[r * kLS + kq - 1];
+      if (r >= mq) thr = -kInf;
+      else if (tk == kInf) thr = kMaxF;
+      else if (METRIC == KNN_METRIC_EUCLIDEAN) {
+        const float myn = qn[r];
+        thr = fminf((tk - myn) + kSlack * (fabsf(tk) + myn + cm), kMaxF);
+      } else {
+        thr = fminf((tk - 1.f) + kSlack * (fabsf(tk) + 2.f), kMaxF);
       }
     }
+#pragma unroll 1
+    for (int ri = 0; ri < 2; ++ri) {
+      const int col0 = ri * kRound + half * 32;  // this thread's 32 columns
+      if (ri * kRound >= mc) {                   // warp-uniform: no candidates in this round
+        if (pass == 1) msk[r * 4 + ri * 2 + half] = 0u;
+        continue;
+      }
+      uint32_t v[32];
+      tmem_ld32(tq + (uint32_t)col0, v);
+      const float4* cn4 = reinterpret_cast<const float4*>(cn + col0);
+      if (FIRST && pass == 0) {
+        // smallest exact key of these 32 columns (the row's own column
+        // left out) into the slice's group
+        const float myn = qn[r];
+        const int64_t sb = (lo + q0 + r) - blo - c0 - col0;
+        float m = kInf;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float4 c = cn4[q];
+          const float cc[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const float dot = __uint_as_float(v[4 * q + e]);
+            const float key = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cc[e]))
+                                                             : __fsub_rn(1.f + cc[e], dot);
+            m = (sb == 4 * q + e) ? m : fminf(m, key);
+          }
+        }
+        const int g = ((c0 / kBN) * 4 + ri * 2 + half) & (kGroups - 1);
+        gm[r * kGS + g] = fminf(gm[r * kGS + g], m);
+      } else {
+        // bit j of neg = sign of thr - key'_j, shifted in from column 31 down
+        uint32_t neg = 0;
+#pragma unroll
+        for (int q = 7; q >= 0; --q) {
+          const float4 c = cn4[q];
+          const float cc[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+          for (int e = 3; e >= 0; --e) {
+            const float dot = __uint_as_float(v[4 * q + e]);
+            const float kp =
+                METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, cc[e]) : __fsub_rn(cc[e], dot);
+            neg = __funnelshift_l(__float_as_uint(__fsub_rn(thr, kp)), neg, 1);
+          }
+        }
+        uint32_t mask = ~neg;
+        // the row's own point (its leaf lies inside the block) never survives
+        const int64_t selfbit = (lo + q0 + r) - blo - c0 - col0;
+        if (selfbit >= 0 && selfbit < 32) mask &= ~(1u << (int)selfbit);
+        if (glog) {  // grouped leaves: the row's own leaf's columns only
+          const int a = min(max((int)rcol[2 * r] - (c0 + col0), 0), 32);
+          const int b = min(max((int)rcol[2 * r + 1] - (c0 + col0), 0), 32);
+          mask &= (uint32_t)(((1ull << b) - 1ull) ^ ((1ull << a) - 1ull));
+        }
+        if (xcl) {
+          // listed ids among these 32 columns: walk the row's sorted
+          // positions (each thread's columns only increase)
+          const int lo_c = c0 + col0;
+          uint32_t ex = 0;
+          int p = xp[r * kXS + xptr];
+          while (p < lo_c + 32) {
+            if (p >= lo_c) ex |= 1u << (p - lo_c);
+            p = xp[r * kXS + (++xptr)];
+          }
+          mask &= ~ex;
+        }
+        msk[r * 4 + ri * 2 + half] = mask;
+      }
+    }
+    // step s + 1's operand (staged since [A]) lands before [B]; its MMA is
+    // issued after [B] and runs while this step's survivors are merged
+    if (has_next) {
+      asm volatile("cp.async.wait_all;\n" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();  // [B]
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (has_next && tid == 0) issue_mma(s + 1);
+    if (pass == 1) {
+      // The quarter's rows with survivors (one ballot) alternate between
+      // its two warps; survivors' products come from the warp's lane
+      // quarter of tensor memory.
+      const int rowq = quarter * 32 + lane;
+      const bool has = rowq < mq && (msk[rowq * 4] | msk[rowq * 4 + 1] | msk[rowq * 4 + 2] | msk[rowq * 4 + 3]) != 0;
+      const uint32_t all = __ballot_sync(0xFFFFFFFFu, has);
+      const bool mine = has && (__popc(all & ((1u << lane) - 1u)) & 1) == half;
+      uint32_t rows = __ballot_sync(0xFFFFFFFFu, mine);
+      while (rows) {
+        const int ql = __ffs(rows) - 1;  // row within the quarter
+        const int qq = quarter * 32 + ql;
+        rows &= rows - 1;
+        float lk = Lk[qq * kLS + lane];
+        uint32_t li = Li[qq * kLS + lane];
+        const float myn = qn[qq];
+#pragma unroll 1
+        for (int h = 0; h < 4; ++h) {
+          uint32_t bal = msk[qq * 4 + h];
+          if (bal == 0) continue;
+          const int cb = h * 32;  // the slice's first column in the tile
+          if (FIRST && __popc(bal) >= kBulkMerge) {
+            // lane j <- product of column cb + j of row qq
+            uint32_t v[32];
+            tmem_ld32(tq + (uint32_t)cb, v);
+            float dot = 0.f;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const float t = __shfl_sync(0xFFFFFFFFu, __uint_as_float(v[j]), ql);
+              if (lane == j) dot = t;
+            }
+            float ck = kInf;
+            uint32_t ci = kNoId;
+            if ((bal >> lane) & 1u) {
+              ck = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[cb + lane]))
+                                                  : __fsub_rn(1.f, dot);
+              ci = (uint32_t)cid[cb + lane];
+            }
+            warp_bitonic_sort32(ck, ci);
+            warp_merge_lower(lk, li, ck, ci);
+            continue;
+          }
+          while (bal) {
+            const int j = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const float dot = __shfl_sync(0xFFFFFFFFu, __uint_as_float(tmem_ld1(tq + (uint32_t)(cb + j))), ql);
+            const float k1 = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[cb + j]))
+                                                            : __fsub_rn(1.f, dot);
+            const uint32_t i1 = (uint32_t)cid[cb + j];
+            const bool dup = !FIRST && !xcl && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
+            if (!dup) warp_insert1(lk, li, k1, i1);
+          }
+        }
+        Lk[qq * kLS + lane] = lk;
+        Li[qq * kLS + lane] = li;
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     if (FIRST && pass == 0 && s == ntiles - 1) {
       // bound per row: the kq-th smallest of its group minima (warp w: rows
       // w + 8 i, four rows' networks interleaved).  Each row's 64 minima:
@@ -817,7 +826,7 @@ size_t umma_smem_bytes(int Kp) {
   // alignment slack + A + B + lists + (qid, qn) + two steps' (cid, cn) + survivor masks + two
   // steps' norm maxima + listed columns + first-tree bounds + barrier words
   return 1024 + 2 * (size_t)(Kp / kKC) * kChunkBytes + (size_t)kBM * kLS * 8 + (size_t)kBM * 8 +
-         (size_t)kBN * 16 + (size_t)kBM * 2 * 4 + 32 + (size_t)kBM * kXS * 2 + (size_t)kBM * 4 + 64;
+         (size_t)kBN * 3 * 8 + (size_t)kBM * 4 * 4 + 48 + (size_t)kBM * kXS * 2 + (size_t)kBM * 4 + 64;
 }
 
 int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
@@ -860,12 +869,18 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
       log.add();
       inv = a.inv;
     }
-#define KNN_TC_LAUNCH(M, F)                                                                               \
+#define KNN_TC_LAUNCH_N(M, F, N)                                                                          \
   do {                                                                                                    \
-    cudaFuncSetAttribute(k_leaf_tc<M, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);       \
-    k_leaf_tc<M, F><<<grid, kUThreads, smem, st>>>(Xb, idesc, Kp, a.segs, ftab, a.k, a.kq, qtiles, glog, perm, inv, \
-                                                   a.norms2,                                                          \
-                                                   a.akey, a.aid, a.err);                                \
+    cudaFuncSetAttribute(k_leaf_tc<M, F, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);    \
+    k_leaf_tc<M, F, N><<<grid, kUThreads, smem, st>>>(Xb, idesc, a.segs, ftab, a.k, a.kq, qtiles, glog, perm, \
+                                                      inv, a.norms2, a.akey, a.aid, a.err);             \
+  } while (0)
+#define KNN_TC_LAUNCH(M, F)                    \
+  do {                                         \
+    if (Kp == 64) KNN_TC_LAUNCH_N(M, F, 1);    \
+    else if (Kp == 128) KNN_TC_LAUNCH_N(M, F, 2); \
+    else if (Kp == 192) KNN_TC_LAUNCH_N(M, F, 3); \
+    else KNN_TC_LAUNCH_N(M, F, 4);             \
   } while (0)
     if (a.kev) cudaEventRecord(a.kev[2 * t], st);
     if (a.metric == KNN_METRIC_EUCLIDEAN) {
@@ -877,6 +892,7 @@ int leaf_stage_umma(const UmmaLeafArgs& a, LaunchLog& log) {
     }
     if (a.kev) cudaEventRecord(a.kev[2 * t + 1], st);
 #undef KNN_TC_LAUNCH
+#undef KNN_TC_LAUNCH_N
     log.add();
   }
   const size_t rsm = (size_t)8 * (a.dpad + 32 * 64 + 32) * sizeof(float);

@@ -80,6 +80,28 @@ def measured_peaks() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
+def profiled_traffic(summary: str, config: dict, n: int):
+    """DRAM bytes per launch from a committed ncu summary under profiles/: the
+    line `traffic_bytes_per_launch: B n=N d=.. k=.. trees=.. leaf=..` gives the
+    mean per launch on N points; it is scaled to n (a launch's traffic grows
+    with the points it processes).  (None, reason) when the summary is absent
+    or was taken on another configuration."""
+    import re
+
+    path = ROOT / "profiles" / summary
+    if not path.exists():
+        return None, f"profiles/{summary} absent"
+    m = re.search(r"^traffic_bytes_per_launch: (\d+) n=(\d+) (.*)$", path.read_text(), flags=re.M)
+    if not m:
+        return None, f"no traffic line in profiles/{summary}"
+    fields = dict(kv.split("=") for kv in m.group(3).split())
+    if any(str(config[key]) != fields.get(key) for key in config):
+        return None, f"profiles/{summary} was taken on another configuration ({m.group(3)})"
+    b, pn = int(m.group(1)), int(m.group(2))
+    return b * n / pn, (f"ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, mean over a build's "
+                        f"launches at {pn:,} points (profiles/{summary}), scaled to {n:,} points")
+
+
 def measured_tensor_peak() -> tuple[float, str]:
     """Dense bf16 TFLOP/s: the burst figure (the leaf kernel runs at full clock in the bench)."""
     p = ROOT / "MEASURED_PEAKS.json"
@@ -394,16 +416,16 @@ def run_ours(args, w):
     dom = max(cand, key=lambda kname: cand[kname][0])
     dms, dbytes, dlaunch = cand[dom]
     achieved = dbytes / (dms / 1e3) / 1e9
-    # DRAM bytes (read + write) per k_leaf_tc launch measured by ncu on 500,000
-    # points of this workload and configuration (mean of the 8 launches of a
-    # build: 342 MB), scaled by n
-    traffic = None
-    if dom == "leaf_tc" and (d, k, T, head["leaf"]) == (128, 16, 8, 2048):
-        traffic = 342e6 * n / 500_000
+    # DRAM bytes (read + write) per k_leaf_tc launch from the committed ncu
+    # summary of this kernel on a smaller case of the same configuration,
+    # scaled by the points a launch processes
+    traffic, traffic_src = None, None
+    if dom == "leaf_tc":
+        traffic, traffic_src = profiled_traffic("k_leaf_tc_integer_mixture_500k.md",
+                                                dict(d=d, k=k, trees=T, leaf=head["leaf"]), n)
     hbm_view = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per k_leaf_tc launch "
-                                  "(mean of a build's 8) at 500,000 points, scaled by n" if traffic else None,
+                "traffic_source": traffic_src,
                 "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": dbytes / dlaunch,
                 "mean_launch_ms": dms / dlaunch,
