@@ -142,13 +142,6 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
                : "memory");
 }
 
-__device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
-  uint32_t v;
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(v) : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-  return v;
-}
-
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -578,22 +571,35 @@ __global__ void __launch_bounds__(kUThreads, 2)
       const uint32_t all = __ballot_sync(0xFFFFFFFFu, has);
       const bool mine = has && (__popc(all & ((1u << lane) - 1u)) & 1) == half;
       uint32_t rows = __ballot_sync(0xFFFFFFFFu, mine);
+      // Two rows at a time: their survivor chains (tensor-memory read, key,
+      // insertion) are independent, so both reads are issued before one
+      // wait and the two insertions interleave.  A row without a survivor
+      // left inserts (+inf, no id), which changes nothing.
       while (rows) {
-        const int ql = __ffs(rows) - 1;  // row within the quarter
-        const int qq = quarter * 32 + ql;
+        const int qa = __ffs(rows) - 1;  // rows within the quarter
         rows &= rows - 1;
-        float lk = Lk[qq * kLS + lane];
-        uint32_t li = Li[qq * kLS + lane];
-        const float myn = qn[qq];
-#pragma unroll 1
-        for (int h = 0; h < 4; ++h) {
-          uint32_t bal = msk[qq * 4 + h];
-          if (bal == 0) continue;
-          const int cb = h * 32;  // the slice's first column in the tile
-          if (FIRST && __popc(bal) >= kBulkMerge) {
-            // lane j <- product of column cb + j of row qq
+        const int qb = rows ? __ffs(rows) - 1 : qa;
+        const bool two = rows != 0;
+        if (two) rows &= rows - 1;
+        const int ra = quarter * 32 + qa, rbw = quarter * 32 + qb;
+        float lka = Lk[ra * kLS + lane], lkb = two ? Lk[rbw * kLS + lane] : kInf;
+        uint32_t lia = Li[ra * kLS + lane], lib = two ? Li[rbw * kLS + lane] : kNoId;
+        const float myna = qn[ra], mynb = qn[rbw];
+        // the rows' survivor bits over the tile's 128 columns, in two 64-bit words each
+        uint64_t a0 = msk[ra * 4] | ((uint64_t)msk[ra * 4 + 1] << 32);
+        uint64_t a1 = msk[ra * 4 + 2] | ((uint64_t)msk[ra * 4 + 3] << 32);
+        uint64_t b0 = two ? (msk[rbw * 4] | ((uint64_t)msk[rbw * 4 + 1] << 32)) : 0ull;
+        uint64_t b1 = two ? (msk[rbw * 4 + 2] | ((uint64_t)msk[rbw * 4 + 3] << 32)) : 0ull;
+        if (FIRST) {
+          // 32-column slices with many survivors: sorted and merged in one go
+          auto bulk = [&](int ql, float myn, uint64_t& w0, uint64_t& w1, int h, float& lk, uint32_t& li) {
+            uint64_t& w = h < 2 ? w0 : w1;
+            const int sh = (h & 1) * 32;
+            const uint32_t m = (uint32_t)(w >> sh);
+            if (__popc(m) < kBulkMerge) return;
+            const int cb = h * 32;
             uint32_t v[32];
-            tmem_ld32(tq + (uint32_t)cb, v);
+            tmem_ld32(tq + (uint32_t)cb, v);  // lane j <- product of column cb + j of row ql
             float dot = 0.f;
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
@@ -602,28 +608,64 @@ __global__ void __launch_bounds__(kUThreads, 2)
             }
             float ck = kInf;
             uint32_t ci = kNoId;
-            if ((bal >> lane) & 1u) {
+            if ((m >> lane) & 1u) {
               ck = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[cb + lane]))
                                                   : __fsub_rn(1.f, dot);
               ci = (uint32_t)cid[cb + lane];
             }
             warp_bitonic_sort32(ck, ci);
             warp_merge_lower(lk, li, ck, ci);
-            continue;
-          }
-          while (bal) {
-            const int j = __ffs(bal) - 1;
-            bal &= bal - 1;
-            const float dot = __shfl_sync(0xFFFFFFFFu, __uint_as_float(tmem_ld1(tq + (uint32_t)(cb + j))), ql);
-            const float k1 = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[cb + j]))
-                                                            : __fsub_rn(1.f, dot);
-            const uint32_t i1 = (uint32_t)cid[cb + j];
-            const bool dup = !FIRST && !xcl && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
-            if (!dup) warp_insert1(lk, li, k1, i1);
+            w &= ~(0xFFFFFFFFull << sh);
+          };
+#pragma unroll 1
+          for (int h = 0; h < 4; ++h) {
+            bulk(qa, myna, a0, a1, h, lka, lia);
+            bulk(qb, mynb, b0, b1, h, lkb, lib);
           }
         }
-        Lk[qq * kLS + lane] = lk;
-        Li[qq * kLS + lane] = li;
+        while (a0 | a1 | b0 | b1) {  // warp-uniform
+          const bool va = (a0 | a1) != 0ull, vb = (b0 | b1) != 0ull;
+          int ca = 0, cbc = 0;
+          if (a0) {
+            ca = __ffsll((long long)a0) - 1;
+            a0 &= a0 - 1ull;
+          } else if (a1) {
+            ca = 64 + __ffsll((long long)a1) - 1;
+            a1 &= a1 - 1ull;
+          }
+          if (b0) {
+            cbc = __ffsll((long long)b0) - 1;
+            b0 &= b0 - 1ull;
+          } else if (b1) {
+            cbc = 64 + __ffsll((long long)b1) - 1;
+            b1 &= b1 - 1ull;
+          }
+          uint32_t ua = 0u, ub = 0u;
+          if (va) asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(ua) : "r"(tq + (uint32_t)ca));
+          if (vb) asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(ub) : "r"(tq + (uint32_t)cbc));
+          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+          const float da = __shfl_sync(0xFFFFFFFFu, __uint_as_float(ua), qa);
+          const float db = __shfl_sync(0xFFFFFFFFu, __uint_as_float(ub), qb);
+          float ka = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, da, __fadd_rn(myna, cn[ca])) : __fsub_rn(1.f, da);
+          float kb = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, db, __fadd_rn(mynb, cn[cbc])) : __fsub_rn(1.f, db);
+          uint32_t ia = (uint32_t)cid[ca], ib = (uint32_t)cid[cbc];
+          if (!FIRST && !xcl) {  // block-uniform: duplicates checked here when not masked up front
+            if (__ballot_sync(0xFFFFFFFFu, lane < kq && lia == ia) != 0u) ka = kInf;
+            if (__ballot_sync(0xFFFFFFFFu, lane < kq && lib == ib) != 0u) kb = kInf;
+          }
+          if (!va) ka = kInf;
+          if (!vb) kb = kInf;
+          ia = ka == kInf ? kNoId : ia;
+          ib = kb == kInf ? kNoId : ib;
+          warp_insert1(lka, lia, ka, ia);
+          warp_insert1(lkb, lib, kb, ib);
+        }
+        Lk[ra * kLS + lane] = lka;
+        Li[ra * kLS + lane] = lia;
+        if (two) {
+          Lk[rbw * kLS + lane] = lkb;
+          Li[rbw * kLS + lane] = lib;
+        }
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
