@@ -59,6 +59,36 @@ def run_tree(L, cands, kq, first, exclude, widen, rng):
     return L
 
 
+def run_tree_tile(L, cands, kq, first, exclude, widen, rng):
+    """The per-tile schedule: the filter bound is the tail at the tile's start
+    for all 128 columns; then, first tree only, every 32-column slice with
+    many survivors is sorted and merged before the remaining single survivors
+    are inserted in column order."""
+    listed = {e[1] for e in L[:kq] if e[1] != NOID}
+    for t0 in range(0, len(cands), 128):
+        tail = L[kq - 1][0]
+        slices = []
+        for h0 in range(t0, min(t0 + 128, len(cands)), 32):
+            surv = []
+            for c in cands[h0:h0 + 32]:
+                if exclude and c[1] in listed:
+                    continue
+                if c[0] <= tail or (widen and c[0] <= tail * 1.0001 + 1e-6):
+                    surv.append(c)
+            slices.append(surv)
+        singles = []
+        for surv in slices:
+            if first and len(surv) >= 12:
+                L = merge_batch(L, surv)
+            else:
+                singles += surv
+        for c in singles:
+            if not first and not exclude and any(e[1] == c[1] for e in L[:kq]):
+                continue
+            insert1(L, c)
+    return L
+
+
 def expected(initial, trees, kq):
     best = {}
     for e in initial:
@@ -89,5 +119,30 @@ def test_every_merge_path_keeps_the_kq_best():
                 for t, cands in enumerate(trees):
                     L = run_tree(L, cands, kq, t == 0, exclude and t > 0, widen, rng)
                     L = L[:kq] + [(float(INF), NOID)] * (32 - kq)  # only kq entries are kept
+                got = [e for e in L[:kq] if e[1] != NOID]
+                assert got == want[:len(got)] and len(got) == min(kq, len(want)), (trial, exclude, widen)
+
+
+def test_tile_schedule_keeps_the_kq_best():
+    """One filter bound per 128-column tile and bulk slices merged before the
+    single survivors of earlier slices: the kq best are still kept, as the
+    result of every path is the kq smallest of the union."""
+    rng = np.random.Generator(np.random.PCG64(9))
+    for trial in range(300):
+        kq = int(rng.choice([8, 16, 20, 32]))
+        npts = 600
+        key_of = np.round(rng.random(npts) * 60).astype(np.float32)  # ties on purpose
+        trees = []
+        for _ in range(4):
+            nb = int(rng.integers(40, 500))
+            ids = rng.choice(npts, size=nb, replace=False)
+            trees.append([(float(key_of[i]), int(i)) for i in ids])
+        want = expected([], trees, kq)
+        for exclude in (False, True):
+            for widen in (False, True):
+                L = [(float(INF), NOID)] * 32
+                for t, cands in enumerate(trees):
+                    L = run_tree_tile(L, cands, kq, t == 0, exclude and t > 0, widen, rng)
+                    L = L[:kq] + [(float(INF), NOID)] * (32 - kq)
                 got = [e for e in L[:kq] if e[1] != NOID]
                 assert got == want[:len(got)] and len(got) == min(kq, len(want)), (trial, exclude, widen)
