@@ -82,3 +82,30 @@ def test_reference_recall_small_gaussians(tmp_path, oracle, capsys):
               f"({ref_ms} ms on the GPU), median-split restatement {r_ora:.4f}, "
               f"reference-rule splits {r_fai:.4f}")
     assert r_ref > 0.3 and r_ora > 0.9 and r_fai > 0.3
+
+
+@pytest.mark.parametrize("trees,leaf,props", [(10, 32, 3), (3, 16, 0), (4, 64, 1)])
+def test_reference_recall_distribution_matches_reference_rule_mode(tmp_path, oracle, capsys, trees, leaf, props):
+    """Beyond the one-leaf cases: the reference's own build (several runs; its
+    output varies with atomic order) against the reference-rule split mode
+    over several seeds, on the same normalised 10-cluster data.  The mean
+    recalls must agree within 0.02 plus three standard deviations of the
+    seeds' spread, in a high-recall and two low-recall regimes."""
+    acknn = load_package()
+    x = acknn.workloads.small_gaussians(0)
+    xn = acknn.normalize_reference(x)
+    exn, _ = oracle.exact(xn, 10)
+    ref = []
+    for _ in range(3):
+        ids, _ = run_reference(tmp_path, x, 10, trees=trees, leaf=leaf, props=props)
+        ref.append(recall_at_k(ids, exn))
+    fai = []
+    for seed in range(6):
+        ids, _ = acknn.knn_build(xn, 10, trees, leaf, props, 0, seed=seed, split_rule=1)
+        fai.append(recall_at_k(ids, exn))
+    mr, mf, sf = float(np.mean(ref)), float(np.mean(fai)), float(np.std(fai))
+    with capsys.disabled():
+        print(f"\nsmall_gaussians k=10 T={trees} leaf={leaf} P={props}: reference recall "
+              f"{mr:.4f} (runs {', '.join(f'{r:.4f}' for r in ref)}), reference-rule mode {mf:.4f} +- {sf:.4f} "
+              f"over 6 seeds")
+    assert abs(mr - mf) <= 0.02 + 3 * sf, (mr, mf, sf)
