@@ -454,6 +454,19 @@ def run_ours(args, w):
         r = cpu_rendition(w, head, args.cpu_sample)
         cpu = {kk: r[kk] for kk in ("value", "unit", "cores", "kind", "sample")}
 
+    # the reference's own CUDA build on the same points (its CLI, its own timer),
+    # after every timed region of this process
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        settings = {"literal": CONFIG_PARAMS}
+        if args.reference_gpu_headline:
+            settings["headline"] = head
+        ref_gpu = reference_gpu_runs(acknn, x, k, q, exact[0], settings, args.ref_limit)
+        for name, rr in ref_gpu.items():
+            if isinstance(rr, dict) and rr.get("ms_calculate"):
+                ours = value if rr["params"] == head else lit.get("mixed", {}).get("points_per_s")
+                rr["ours_points_per_s_same_setting"] = ours
+
     if rank == 0:
         line = {
             "metric": METRIC_NAME, "value": value, "unit": "points/s", "n_gpus": world,
@@ -481,7 +494,7 @@ def run_ours(args, w):
                     "d2h_bytes_per_step": int(n * k * 8), "matches_device_run": same_dev_host},
             "gpu_launches": int(stages["launches"]) * args.steps * 2,
             "gpu_launches_note": "kernels of the timed device-resident and end-to-end mixed builds",
-            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+            "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "clocks": clk,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -1248,6 +1261,10 @@ def main():
     ap.add_argument("--reference-gpu", action="store_true",
                     help="time the reference's own sm_100a build (oracle/_ref/hello) on the workload")
     ap.add_argument("--ref-limit", type=float, default=300.0, help="seconds per reference run")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference's own build in the default run")
+    ap.add_argument("--reference-gpu-headline", action="store_true",
+                    help="also run the reference's own build at the headline setting")
     ap.add_argument("--sharded", action="store_true",
                     help="one dataset built by all ranks together (strong scaling; launch with torchrun for N > 1)")
     ap.add_argument("--cli", action="store_true",
