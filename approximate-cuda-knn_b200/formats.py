@@ -124,16 +124,16 @@ def write_csv_integers(path: str, x: np.ndarray) -> None:
 
 
 def write_csv_fixed(path: str, x: np.ndarray, decimals: int = 9) -> np.ndarray:
-    """CSV in the reference's input format for values in [0, 10): exact zeros
-    as "0", every other value in fixed point with ``decimals`` digits (no
-    per-value formatting, so a multi-GB file takes seconds).  Returns the
-    float32 values a reader parses back (the written decimals, rounded)."""
+    """CSV in the reference's input format for values in (-1000, 1000): exact
+    zeros as "0", every other value in fixed point, with a sign when negative
+    and ``decimals`` digits after the point (no per-value formatting, so a
+    multi-GB file takes seconds).  Returns the float32 values a reader parses
+    back (the written decimals, rounded)."""
     x = np.asarray(x, dtype=np.float32)
     n, d = x.shape
-    if x.size and (x.min() < 0 or x.max() >= 10):
-        raise ValueError("write_csv_fixed takes values in [0, 10)")
+    if x.size and (x.min() <= -1000 or x.max() >= 1000):
+        raise ValueError("write_csv_fixed takes values in (-1000, 1000)")
     scale = 10 ** decimals
-    width = decimals + 2  # "d." + decimals
     parsed = np.empty_like(x)
     with open(path, "wb") as f:
         f.write(f"{n}\n{d}\n".encode())
@@ -143,27 +143,35 @@ def write_csv_fixed(path: str, x: np.ndarray, decimals: int = 9) -> np.ndarray:
             m = np.rint(blk * scale).astype(np.int64)
             zero = m == 0
             parsed[s:s + step] = (m / scale).astype(np.float32)
-            w = np.where(zero, 1, width) + 1  # token + separator
+            neg = m < 0
+            am = np.abs(m)
+            ip = am // scale
+            ndig = 1 + (ip >= 10) + (ip >= 100)
+            w = np.where(zero, 1, neg + ndig + 1 + decimals) + 1  # token + separator
             ends = np.cumsum(w, axis=1)
             starts = ends - w
-            rows = blk.shape[0]
             row_len = ends[:, -1]
             row_off = np.concatenate(([0], np.cumsum(row_len)[:-1]))
             buf = np.empty(int(row_len.sum()), dtype=np.uint8)
             pos = row_off[:, None] + starts
             buf[pos[zero]] = ord("0")
             nz = ~zero
-            pz, mz = pos[nz], m[nz]
-            buf[pz] = (mz // scale + ord("0")).astype(np.uint8)
-            buf[pz + 1] = ord(".")
-            frac = mz % scale
+            pz, iz, dz, gz = pos[nz], ip[nz], ndig[nz], neg[nz]
+            buf[pz[gz]] = ord("-")
+            p0 = pz + gz  # first digit
+            for j in range(3):  # integer digits, most significant first
+                has = dz > j
+                digit = (iz // (10 ** (dz - 1 - j).clip(0))) % 10
+                buf[(p0 + j)[has]] = (digit[has] + ord("0")).astype(np.uint8)
+            pdot = p0 + dz
+            buf[pdot] = ord(".")
+            frac = am[nz] % scale
             for j in range(decimals):
-                buf[pz + 1 + decimals - j] = (frac % 10 + ord("0")).astype(np.uint8)
+                buf[pdot + decimals - j] = (frac % 10 + ord("0")).astype(np.uint8)
                 frac //= 10
             sep = row_off[:, None] + ends - 1
             buf[sep] = ord(",")
             buf[sep[:, -1]] = ord("\n")
-            assert rows == sep.shape[0]
             f.write(buf.tobytes())
     return parsed
 

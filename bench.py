@@ -861,11 +861,113 @@ def reference_gpu_runs(acknn, x, k, q, exact_ids, settings, limit_s: float) -> d
     return out
 
 
-def run_reference_gpu(args, w):
-    """The reference's own build on the integer mixture at the configuration's
-    literal parameters and at the headline setting (one run each)."""
+def run_reference_gpu_batch(args):
+    """The 256-dataset batch through the reference's own build: one process
+    per set (the reference builds one set per process), at the batch's
+    literal parameters; its self-reported device time summed over the sets,
+    the wall time of all processes, and recall@k by id per set against the
+    FP64 exact graph (up to 500 seeded queries per set).  Our batched build of
+    the same sets at the same parameters (plain FP32 and BF16 tiles) is timed
+    beside it.  Sets are stopped once `--ref-limit` seconds of wall time have
+    gone by."""
+    import re
+    import shutil
+    import tempfile
+
     import torch
 
+    torch.cuda.set_device(0)
+    acknn = load_package()
+    lib = acknn.load_library()
+    cfg = acknn.workloads.CONFIGS["dataset_batch"]
+    count = args.count or cfg["count"]
+    k, T, L, P = cfg["k"], cfg["trees"], cfg["leaf"], cfg["props"]
+    xs = [acknn.workloads.batch_dataset(s) for s in range(count)]
+    tmp = Path(tempfile.mkdtemp(prefix="acknn_refb_"))
+    ref_ms, ref_wall, ref_rec, done = 0.0, 0.0, [], 0
+    ours_rec = {"plain_fp32": [], "mixed": []}
+    rng = np.random.Generator(np.random.PCG64(7))
+    t_all = time.perf_counter()
+    try:
+        for i, x in enumerate(xs):
+            if time.perf_counter() - t_all > args.ref_limit:
+                break
+            q = np.sort(rng.choice(x.shape[0], size=min(500, x.shape[0]), replace=False)).astype(np.int64)
+            csv = tmp / "set.csv"
+            parsed = acknn.formats.write_csv_fixed(str(csv), x)
+            xn = acknn.normalize_reference(parsed)
+            ei, _ = acknn.exact_fp64(xn, k, q, 0)
+            out = tmp / "set.bin"
+            t = time.perf_counter()
+            r = subprocess.run([str(REF_BIN), str(csv), str(out), str(k), str(T), str(L), str(P), "EUCLIDEAN", "0", "F"],
+                               capture_output=True, text=True, timeout=max(30.0, args.ref_limit))
+            ref_wall += time.perf_counter() - t
+            m = re.search(r"has done task in: ([0-9.eE+-]+) ms", r.stdout)
+            if r.returncode != 0 or not m:
+                break
+            ref_ms += float(m.group(1))
+            _, _, ids, _ = acknn.formats.read_result(str(out))
+            ref_rec.append(sum(len(np.intersect1d(a, b)) for a, b in zip(ids[q], ei)) / (k * len(q)))
+            for name, prec in (("plain_fp32", acknn.PREC_FP32), ("mixed", acknn.PREC_BF16_RERANK)):
+                oi, _ = acknn.knn_build(xn, k, T, L, P, 0, seed=i, precision=prec)
+                ours_rec[name].append(sum(len(np.intersect1d(a, b)) for a, b in zip(oi[q], ei)) / (k * len(q)))
+            done += 1
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    pts = sum(x.shape[0] for x in xs[:done])
+    # our batched build of the same sets (device-resident, captured graphs replayed)
+    stream = torch.cuda.current_stream()
+    ctx = acknn.Context(0)
+    sub = xs[:done]
+    xd = [torch.from_numpy(acknn.normalize_reference(x)).cuda() for x in sub]
+    oi = [torch.empty((x.shape[0], k), dtype=torch.int32, device="cuda") for x in sub]
+    od = [torch.empty((x.shape[0], k), dtype=torch.float32, device="cuda") for x in sub]
+    arr = (acknn.KnnDataset * max(1, done))()
+    for i, x in enumerate(sub):
+        arr[i].points = xd[i].data_ptr()
+        arr[i].n, arr[i].d, arr[i].seed = x.shape[0], x.shape[1], i
+        arr[i].out_idx, arr[i].out_dist = oi[i].data_ptr(), od[i].data_ptr()
+    ours = {}
+    for name, prec in (("plain_fp32", acknn.PREC_FP32), ("mixed", acknn.PREC_BF16_RERANK)):
+        def b(prec=prec):
+            opt = acknn.default_options(points_on_device=1, outputs_on_device=1, stream=stream.cuda_stream,
+                                        precision=prec, autotune=1)
+            rc = lib.knn_build_batch(ctx.handle, arr, done, k, T, L, P, 0, ctypes.byref(opt), None)
+            if rc:
+                raise acknn.KnnError(rc, lib.knn_last_error().decode())
+        for _ in range(3):
+            b()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            b()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        ours[name] = {"ms": ms, "points_per_s": pts / (ms / 1e3),
+                      "recall_mean_of_sets": float(np.mean(ours_rec[name])) if ours_rec[name] else None}
+    ctx.close()
+    print(json.dumps({"reference_gpu_batch": {
+        "sets_run": done, "sets": count, "points": pts, "params": {"k": k, "trees": T, "leaf": L, "props": P},
+        "ms_calculate_sum": ref_ms, "process_wall_s": ref_wall,
+        "points_per_s_calculate": pts / (ref_ms / 1e3) if ref_ms else None,
+        "recall_mean_of_sets": float(np.mean(ref_rec)) if ref_rec else None,
+        "recall_min": float(np.min(ref_rec)) if ref_rec else None},
+        "ours_batched_same_sets": ours,
+        "note": "the sets as CSV in fixed point with 9 decimals, normalised by the reference's rule on both sides"}),
+        flush=True)
+    return 0
+
+
+def run_reference_gpu(args, w):
+    """The reference's own build on the integer mixture at the configuration's
+    literal parameters and at the headline setting (one run each); with
+    --workload dataset_batch, the 256-set batch (run_reference_gpu_batch)."""
+    import torch
+
+    if args.workload == "dataset_batch":
+        return run_reference_gpu_batch(args)
     torch.cuda.set_device(0)
     acknn = load_package()
     acknn.load_library()
