@@ -853,7 +853,8 @@ int check_error_words(knn_context* C) {
   int host[2] = {0, 0};
   KNN_CK(cudaMemcpy(host, C->err_words, sizeof(host), cudaMemcpyDeviceToHost));
   if (host[0] == 0 && host[1] == 0) return KNN_OK;
-  KNN_CK(cudaMemset(C->err_words + 1, 0, sizeof(int)));
+  // reported: clear both (the stream has finished, so no kernel of the build reads them)
+  KNN_CK(cudaMemset(C->err_words, 0, 2 * sizeof(int)));
   return fail(KNN_ERR_TIMEOUT, "a tensor-core tile wait exceeded its time limit");
 }
 

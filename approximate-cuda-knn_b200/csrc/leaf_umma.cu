@@ -721,6 +721,8 @@ __global__ void __launch_bounds__(kUThreads, 2)
       }
     }
   }
+  // the last step's merge is ordered before the write-back only by this barrier
+  __syncthreads();
   if (*status == 0) {
     for (int e = tid; e < kBM * 32; e += kUThreads) {
       const int r = e >> 5, s = e & 31;
