@@ -7,11 +7,10 @@
 //   * the k x k neighbour-of-neighbour ids are read all at once (four loads in
 //     flight per lane), deduplicated in a per-warp shared-memory hash set
 //     seeded with i and N(i), and compacted into a candidate array;
-//   * the candidates' rows stream through a two-slot cp.async pipeline in
-//     256-byte row slices (32 rows per stage, xor-swizzled so the per-lane
-//     row reads are conflict-free): stage t+1 is in flight while stage t is
-//     summed, across batch boundaries too; FP16 inputs are gathered as FP16
-//     (the conversion to FP32 is exact, so the keys are unchanged);
+//   * the candidates' rows are staged by cp.async in 256-byte row slices (32
+//     rows per stage, padded pitch so the per-lane row reads are conflict-free
+//     at compile-time offsets); FP16 inputs are gathered as FP16 (the
+//     conversion to FP32 is exact, so the keys are unchanged);
 //   * each lane computes one key in the reference's order and the batch's
 //     survivors are merged into the warp-held sorted list (bitonic via shuffles).
 // "New" flags: a pair (a, j) is skipped when a was already in N(i) and j already
@@ -32,7 +31,8 @@ namespace knn {
 namespace {
 constexpr int kPropMaxWarps = 8;
 constexpr size_t kPropSmemBudget = 200 * 1024;
-constexpr int kSliceBytes = 256;  // bytes of one candidate row per pipeline stage (16 x 16 B)
+constexpr int kSliceBytes = 256;  // bytes of one candidate row per stage (16 x 16 B)
+constexpr int kRowStride = kSliceBytes + 16;  // padded row pitch of the staging buffer
 constexpr int kGatherUnroll = 4;  // neighbour-list entries in flight per lane
 
 __device__ __forceinline__ bool hash_insert(int32_t* H, int hbits, int32_t id) {
@@ -69,10 +69,10 @@ int prop_hash_bits(int k) {
 }
 
 // hash set | candidates [k*k] | N(i) ids and flags | query row (float, d
-// rounded to 8) | two row-slice buffers
+// rounded to 8) | the row-slice buffer (32 rows, padded pitch)
 size_t prop_warp_bytes(int k, int d) {
   size_t b = ((size_t)4 << prop_hash_bits(k)) + (size_t)4 * round_up(k * k, 32) + (size_t)8 * round_up(k, 32) +
-             (size_t)4 * round_up(d, 8) + (size_t)2 * 32 * kSliceBytes;
+             (size_t)4 * round_up(d, 8) + (size_t)32 * kRowStride;
   return (b + 15) & ~(size_t)15;
 }
 
@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
   uint32_t* nbid = Q + ((kk + 31) & ~31);
   uint32_t* nbfl = nbid + kr;
   float* xq = reinterpret_cast<float*>(nbfl + kr);
-  unsigned char* rows = reinterpret_cast<unsigned char*>(xq + dq);  // [2][32][kSliceBytes]
+  unsigned char* rows = reinterpret_cast<unsigned char*>(xq + dq);  // [32][kRowStride]
   const float kInf = __int_as_float(0x7F800000);
   const uint32_t lt_mask = (1u << lane) - 1u;
   const int nch = (d + kCH - 1) / kCH;
@@ -180,55 +180,52 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
     }
     __syncwarp();
 
-    // keys of the candidates, 32 per batch, row slices through two buffers
+    // keys of the candidates, 32 per batch, one row slice of kSliceBytes per
+    // stage; rows are kRowStride apart, so lane r's 16-byte loads of unit q
+    // (address r * 272 + 16 q) fall in distinct bank groups within each
+    // 8-lane phase and the unit offsets are compile-time constants
     const int stages = ((qn + 31) >> 5) * nch;
-    auto issue = [&](int t) {
-      const int b = t / nch, c = t - b * nch;
-      const int m = min(32, qn - 32 * b);
-      const int half = lane >> 4, c16 = lane & 15;
-      const int dim = c * kCH + kEPU * c16;
-      unsigned char* buf = rows + (size_t)(t & 1) * 32 * kSliceBytes;
-      for (int r = half; r < m; r += 2) {
-        const uint32_t jid = Q[32 * b + r];
-        const Elem* src = X + (size_t)jid * ldr + (dim < ldr ? dim : 0);
-        cp_async16(buf + r * kSliceBytes + ((c16 ^ (r & 7)) << 4), src, dim < ldr ? 16 : 0);
-      }
-      cp_async_commit();
-    };
-    if (stages > 0) issue(0);
+    const int half = lane >> 4, c16 = lane & 15;
     float total = 0.f, part = 0.f;
     for (int t = 0; t < stages; ++t) {
-      if (t + 1 < stages) {
-        issue(t + 1);
-        cp_async_wait<1>();
-      } else {
-        cp_async_wait<0>();
-      }
-      __syncwarp();
       const int b = t / nch, c = t - b * nch;
       const int m = min(32, qn - 32 * b);
       const int cd = c * kCH;
+      {
+        const int dim = cd + kEPU * c16;
+        const bool ok = dim < ldr;
+        for (int r = half; r < m; r += 2) {
+          const uint32_t jid = Q[32 * b + r];
+          cp_async16(rows + r * kRowStride + c16 * 16, X + (size_t)jid * ldr + (ok ? dim : 0), ok ? 16 : 0);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+      }
+      __syncwarp();
       if (lane < m) {
-        const unsigned char* myrow = rows + (size_t)(t & 1) * 32 * kSliceBytes + lane * kSliceBytes;
-        const int lim = min(kCH, d - cd);
-        for (int q = 0; q < (lim + kEPU - 1) / kEPU; ++q) {
-          const uint4 raw = *reinterpret_cast<const uint4*>(myrow + ((q ^ (lane & 7)) << 4));
-          const float* qx = xq + cd + kEPU * q;
-          if (HALF) {
-            const __half2* h2 = reinterpret_cast<const __half2*>(&raw);
+        const unsigned char* myrow = rows + lane * kRowStride;
+        const int nu = (min(kCH, d - cd) + kEPU - 1) / kEPU;  // 16-byte units holding dims
+        const float* qx = xq + cd;
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const float2 cv = __half22float2(h2[e]);
-              part = acc_step<METRIC>(qx[2 * e], cv.x, part);
-              part = acc_step<METRIC>(qx[2 * e + 1], cv.y, part);
+        for (int q = 0; q < kCH / kEPU; ++q) {
+          if (q < nu) {
+            const uint4 raw = *reinterpret_cast<const uint4*>(myrow + q * 16);
+            if (HALF) {
+              const __half2* h2 = reinterpret_cast<const __half2*>(&raw);
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                const float2 cv = __half22float2(h2[e]);
+                part = acc_step<METRIC>(qx[kEPU * q + 2 * e], cv.x, part);
+                part = acc_step<METRIC>(qx[kEPU * q + 2 * e + 1], cv.y, part);
+              }
+            } else {
+              const float4 cv = *reinterpret_cast<const float4*>(&raw);
+              const float4 qv = *reinterpret_cast<const float4*>(qx + kEPU * q);
+              part = acc_step<METRIC>(qv.x, cv.x, part);
+              part = acc_step<METRIC>(qv.y, cv.y, part);
+              part = acc_step<METRIC>(qv.z, cv.z, part);
+              part = acc_step<METRIC>(qv.w, cv.w, part);
             }
-          } else {
-            const float4 cv = *reinterpret_cast<const float4*>(&raw);
-            const float4 qv = *reinterpret_cast<const float4*>(qx);
-            part = acc_step<METRIC>(qv.x, cv.x, part);
-            part = acc_step<METRIC>(qv.y, cv.y, part);
-            part = acc_step<METRIC>(qv.z, cv.z, part);
-            part = acc_step<METRIC>(qv.w, cv.w, part);
           }
         }
         if (((cd + kCH) & 255) == 0 || cd + kCH >= d) {
@@ -236,7 +233,7 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
           part = 0.f;
         }
       }
-      __syncwarp();  // the slot is refilled by stage t + 2
+      __syncwarp();  // the buffer is refilled by the next stage
       if (c == nch - 1) {
         const int32_t cj = lane < m ? (int32_t)Q[32 * b + lane] : 0;
         float key = total;
