@@ -623,43 +623,62 @@ __global__ void __launch_bounds__(kUThreads, 2)
             bulk(qb, mynb, b0, b1, h, lkb, lib);
           }
         }
-        while (a0 | a1 | b0 | b1) {  // warp-uniform
-          const bool va = (a0 | a1) != 0ull, vb = (b0 | b1) != 0ull;
-          int ca = 0, cbc = 0;
-          if (a0) {
-            ca = __ffsll((long long)a0) - 1;
-            a0 &= a0 - 1ull;
-          } else if (a1) {
-            ca = 64 + __ffsll((long long)a1) - 1;
-            a1 &= a1 - 1ull;
+        // next survivor column of a row's 128-bit set (warp-uniform), -1 when empty
+        auto next_col = [](uint64_t& w0, uint64_t& w1) -> int {
+          if (w0) {
+            const int c = __ffsll((long long)w0) - 1;
+            w0 &= w0 - 1ull;
+            return c;
           }
-          if (b0) {
-            cbc = __ffsll((long long)b0) - 1;
-            b0 &= b0 - 1ull;
-          } else if (b1) {
-            cbc = 64 + __ffsll((long long)b1) - 1;
-            b1 &= b1 - 1ull;
+          if (w1) {
+            const int c = 64 + __ffsll((long long)w1) - 1;
+            w1 &= w1 - 1ull;
+            return c;
           }
-          uint32_t ua = 0u, ub = 0u;
-          if (va) asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(ua) : "r"(tq + (uint32_t)ca));
-          if (vb) asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(ub) : "r"(tq + (uint32_t)cbc));
+          return -1;
+        };
+        auto key_of = [&](float dot, float myn, int c) {
+          return METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[c])) : __fsub_rn(1.f, dot);
+        };
+        // both rows while both have survivors: two reads before one wait, two
+        // independent insertions
+        while ((a0 | a1) != 0ull && (b0 | b1) != 0ull) {
+          const int ca = next_col(a0, a1), cbc = next_col(b0, b1);
+          uint32_t ua, ub;
+          asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(ua) : "r"(tq + (uint32_t)ca));
+          asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(ub) : "r"(tq + (uint32_t)cbc));
           asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-          const float da = __shfl_sync(0xFFFFFFFFu, __uint_as_float(ua), qa);
-          const float db = __shfl_sync(0xFFFFFFFFu, __uint_as_float(ub), qb);
-          float ka = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, da, __fadd_rn(myna, cn[ca])) : __fsub_rn(1.f, da);
-          float kb = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, db, __fadd_rn(mynb, cn[cbc])) : __fsub_rn(1.f, db);
+          float ka = key_of(__shfl_sync(0xFFFFFFFFu, __uint_as_float(ua), qa), myna, ca);
+          float kb = key_of(__shfl_sync(0xFFFFFFFFu, __uint_as_float(ub), qb), mynb, cbc);
           uint32_t ia = (uint32_t)cid[ca], ib = (uint32_t)cid[cbc];
           if (!FIRST && !xcl) {  // block-uniform: duplicates checked here when not masked up front
-            if (__ballot_sync(0xFFFFFFFFu, lane < kq && lia == ia) != 0u) ka = kInf;
-            if (__ballot_sync(0xFFFFFFFFu, lane < kq && lib == ib) != 0u) kb = kInf;
+            if (__ballot_sync(0xFFFFFFFFu, lane < kq && lia == ia) != 0u) {
+              ka = kInf;
+              ia = kNoId;
+            }
+            if (__ballot_sync(0xFFFFFFFFu, lane < kq && lib == ib) != 0u) {
+              kb = kInf;
+              ib = kNoId;
+            }
           }
-          if (!va) ka = kInf;
-          if (!vb) kb = kInf;
-          ia = ka == kInf ? kNoId : ia;
-          ib = kb == kInf ? kNoId : ib;
           warp_insert1(lka, lia, ka, ia);
           warp_insert1(lkb, lib, kb, ib);
         }
+        // then the row that still has survivors, one at a time
+        auto rest = [&](uint64_t& w0, uint64_t& w1, int ql, float myn, float& lk, uint32_t& li) {
+          while ((w0 | w1) != 0ull) {
+            const int c = next_col(w0, w1);
+            uint32_t u;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(u) : "r"(tq + (uint32_t)c));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            const float k1 = key_of(__shfl_sync(0xFFFFFFFFu, __uint_as_float(u), ql), myn, c);
+            const uint32_t i1 = (uint32_t)cid[c];
+            const bool dup = !FIRST && !xcl && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0u;
+            if (!dup) warp_insert1(lk, li, k1, i1);
+          }
+        };
+        rest(a0, a1, qa, myna, lka, lia);
+        rest(b0, b1, qb, mynb, lkb, lib);
         Lk[ra * kLS + lane] = lka;
         Li[ra * kLS + lane] = lia;
         if (two) {
