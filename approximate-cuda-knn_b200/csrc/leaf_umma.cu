@@ -142,6 +142,13 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
                : "memory");
 }
 
+__device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
+  uint32_t v;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(v) : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+  return v;
+}
+
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -576,30 +583,21 @@ __global__ void __launch_bounds__(kUThreads, 2)
       // wait and the two insertions interleave.  A row without a survivor
       // left inserts (+inf, no id), which changes nothing.
       while (rows) {
-        const int qa = __ffs(rows) - 1;  // rows within the quarter
+        const int ql = __ffs(rows) - 1;  // row within the quarter
+        const int qq = quarter * 32 + ql;
         rows &= rows - 1;
-        const int qb = rows ? __ffs(rows) - 1 : qa;
-        const bool two = rows != 0;
-        if (two) rows &= rows - 1;
-        const int ra = quarter * 32 + qa, rbw = quarter * 32 + qb;
-        float lka = Lk[ra * kLS + lane], lkb = two ? Lk[rbw * kLS + lane] : kInf;
-        uint32_t lia = Li[ra * kLS + lane], lib = two ? Li[rbw * kLS + lane] : kNoId;
-        const float myna = qn[ra], mynb = qn[rbw];
-        // the rows' survivor bits over the tile's 128 columns, in two 64-bit words each
-        uint64_t a0 = msk[ra * 4] | ((uint64_t)msk[ra * 4 + 1] << 32);
-        uint64_t a1 = msk[ra * 4 + 2] | ((uint64_t)msk[ra * 4 + 3] << 32);
-        uint64_t b0 = two ? (msk[rbw * 4] | ((uint64_t)msk[rbw * 4 + 1] << 32)) : 0ull;
-        uint64_t b1 = two ? (msk[rbw * 4 + 2] | ((uint64_t)msk[rbw * 4 + 3] << 32)) : 0ull;
-        if (FIRST) {
-          // 32-column slices with many survivors: sorted and merged in one go
-          auto bulk = [&](int ql, float myn, uint64_t& w0, uint64_t& w1, int h, float& lk, uint32_t& li) {
-            uint64_t& w = h < 2 ? w0 : w1;
-            const int sh = (h & 1) * 32;
-            const uint32_t m = (uint32_t)(w >> sh);
-            if (__popc(m) < kBulkMerge) return;
-            const int cb = h * 32;
+        float lk = Lk[qq * kLS + lane];
+        uint32_t li = Li[qq * kLS + lane];
+        const float myn = qn[qq];
+#pragma unroll 1
+        for (int h = 0; h < 4; ++h) {
+          uint32_t bal = msk[qq * 4 + h];
+          if (bal == 0) continue;
+          const int cb = h * 32;  // the slice's first column in the tile
+          if (FIRST && __popc(bal) >= kBulkMerge) {
+            // lane j <- product of column cb + j of row qq
             uint32_t v[32];
-            tmem_ld32(tq + (uint32_t)cb, v);  // lane j <- product of column cb + j of row ql
+            tmem_ld32(tq + (uint32_t)cb, v);
             float dot = 0.f;
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
@@ -608,83 +606,28 @@ __global__ void __launch_bounds__(kUThreads, 2)
             }
             float ck = kInf;
             uint32_t ci = kNoId;
-            if ((m >> lane) & 1u) {
+            if ((bal >> lane) & 1u) {
               ck = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[cb + lane]))
                                                   : __fsub_rn(1.f, dot);
               ci = (uint32_t)cid[cb + lane];
             }
             warp_bitonic_sort32(ck, ci);
             warp_merge_lower(lk, li, ck, ci);
-            w &= ~(0xFFFFFFFFull << sh);
-          };
-#pragma unroll 1
-          for (int h = 0; h < 4; ++h) {
-            bulk(qa, myna, a0, a1, h, lka, lia);
-            bulk(qb, mynb, b0, b1, h, lkb, lib);
+            continue;
           }
-        }
-        // next survivor column of a row's 128-bit set (warp-uniform), -1 when empty
-        auto next_col = [](uint64_t& w0, uint64_t& w1) -> int {
-          if (w0) {
-            const int c = __ffsll((long long)w0) - 1;
-            w0 &= w0 - 1ull;
-            return c;
-          }
-          if (w1) {
-            const int c = 64 + __ffsll((long long)w1) - 1;
-            w1 &= w1 - 1ull;
-            return c;
-          }
-          return -1;
-        };
-        auto key_of = [&](float dot, float myn, int c) {
-          return METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[c])) : __fsub_rn(1.f, dot);
-        };
-        // both rows while both have survivors: two reads before one wait, two
-        // independent insertions
-        while ((a0 | a1) != 0ull && (b0 | b1) != 0ull) {
-          const int ca = next_col(a0, a1), cbc = next_col(b0, b1);
-          uint32_t ua, ub;
-          asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(ua) : "r"(tq + (uint32_t)ca));
-          asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(ub) : "r"(tq + (uint32_t)cbc));
-          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-          float ka = key_of(__shfl_sync(0xFFFFFFFFu, __uint_as_float(ua), qa), myna, ca);
-          float kb = key_of(__shfl_sync(0xFFFFFFFFu, __uint_as_float(ub), qb), mynb, cbc);
-          uint32_t ia = (uint32_t)cid[ca], ib = (uint32_t)cid[cbc];
-          if (!FIRST && !xcl) {  // block-uniform: duplicates checked here when not masked up front
-            if (__ballot_sync(0xFFFFFFFFu, lane < kq && lia == ia) != 0u) {
-              ka = kInf;
-              ia = kNoId;
-            }
-            if (__ballot_sync(0xFFFFFFFFu, lane < kq && lib == ib) != 0u) {
-              kb = kInf;
-              ib = kNoId;
-            }
-          }
-          warp_insert1(lka, lia, ka, ia);
-          warp_insert1(lkb, lib, kb, ib);
-        }
-        // then the row that still has survivors, one at a time
-        auto rest = [&](uint64_t& w0, uint64_t& w1, int ql, float myn, float& lk, uint32_t& li) {
-          while ((w0 | w1) != 0ull) {
-            const int c = next_col(w0, w1);
-            uint32_t u;
-            asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(u) : "r"(tq + (uint32_t)c));
-            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-            const float k1 = key_of(__shfl_sync(0xFFFFFFFFu, __uint_as_float(u), ql), myn, c);
-            const uint32_t i1 = (uint32_t)cid[c];
-            const bool dup = !FIRST && !xcl && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0u;
+          while (bal) {
+            const int j = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const float dot = __shfl_sync(0xFFFFFFFFu, __uint_as_float(tmem_ld1(tq + (uint32_t)(cb + j))), ql);
+            const float k1 = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[cb + j]))
+                                                            : __fsub_rn(1.f, dot);
+            const uint32_t i1 = (uint32_t)cid[cb + j];
+            const bool dup = !FIRST && !xcl && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
             if (!dup) warp_insert1(lk, li, k1, i1);
           }
-        };
-        rest(a0, a1, qa, myna, lka, lia);
-        rest(b0, b1, qb, mynb, lkb, lib);
-        Lk[ra * kLS + lane] = lka;
-        Li[ra * kLS + lane] = lia;
-        if (two) {
-          Lk[rbw * kLS + lane] = lkb;
-          Li[rbw * kLS + lane] = lib;
         }
+        Lk[qq * kLS + lane] = lk;
+        Li[qq * kLS + lane] = li;
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
