@@ -578,10 +578,6 @@ __global__ void __launch_bounds__(kUThreads, 2)
       const uint32_t all = __ballot_sync(0xFFFFFFFFu, has);
       const bool mine = has && (__popc(all & ((1u << lane) - 1u)) & 1) == half;
       uint32_t rows = __ballot_sync(0xFFFFFFFFu, mine);
-      // Two rows at a time: their survivor chains (tensor-memory read, key,
-      // insertion) are independent, so both reads are issued before one
-      // wait and the two insertions interleave.  A row without a survivor
-      // left inserts (+inf, no id), which changes nothing.
       while (rows) {
         const int ql = __ffs(rows) - 1;  // row within the quarter
         const int qq = quarter * 32 + ql;
