@@ -61,9 +61,9 @@ def run_tree(L, cands, kq, first, exclude, widen, rng):
 
 def run_tree_tile(L, cands, kq, first, exclude, widen, rng):
     """The per-tile schedule: the filter bound is the tail at the tile's start
-    for all 128 columns; then, first tree only, every 32-column slice with
-    many survivors is sorted and merged before the remaining single survivors
-    are inserted in column order."""
+    for all 128 columns; then the tile's 32-column slices are merged in column
+    order, a slice with many survivors sorted and merged in one go (first tree
+    only), the others one survivor at a time."""
     listed = {e[1] for e in L[:kq] if e[1] != NOID}
     for t0 in range(0, len(cands), 128):
         tail = L[kq - 1][0]
@@ -76,16 +76,14 @@ def run_tree_tile(L, cands, kq, first, exclude, widen, rng):
                 if c[0] <= tail or (widen and c[0] <= tail * 1.0001 + 1e-6):
                     surv.append(c)
             slices.append(surv)
-        singles = []
         for surv in slices:
             if first and len(surv) >= 12:
                 L = merge_batch(L, surv)
-            else:
-                singles += surv
-        for c in singles:
-            if not first and not exclude and any(e[1] == c[1] for e in L[:kq]):
                 continue
-            insert1(L, c)
+            for c in surv:
+                if not first and not exclude and any(e[1] == c[1] for e in L[:kq]):
+                    continue
+                insert1(L, c)
     return L
 
 
@@ -124,9 +122,9 @@ def test_every_merge_path_keeps_the_kq_best():
 
 
 def test_tile_schedule_keeps_the_kq_best():
-    """One filter bound per 128-column tile and bulk slices merged before the
-    single survivors of earlier slices: the kq best are still kept, as the
-    result of every path is the kq smallest of the union."""
+    """One filter bound per 128-column tile (looser than a bound refreshed
+    after every 64 columns): the kq best are still kept, as the result of
+    every path is the kq smallest of the union."""
     rng = np.random.Generator(np.random.PCG64(9))
     for trial in range(300):
         kq = int(rng.choice([8, 16, 20, 32]))
