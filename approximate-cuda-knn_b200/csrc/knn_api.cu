@@ -442,6 +442,7 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
   a.trees = trees;
   a.segs = lay.segs;
   a.leaves = lay.leaves;
+  a.maxleaf = lay.maxleaf;
   a.metric = metric;
   a.perm = perm;
   a.norms = norms;

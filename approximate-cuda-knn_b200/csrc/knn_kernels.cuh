@@ -96,6 +96,7 @@ struct LeafArgs {
   int d, dpad, k, trees, metric;
   SegView segs;
   int64_t leaves;
+  int64_t maxleaf;       // points in the largest leaf (query tiles per leaf)
   const int32_t* perm;   // [trees][n]
   const float* norms;    // [n] (COSINE) or null
   float* rkey;           // [n][k] in/out, sorted

@@ -4,7 +4,8 @@
 // Taxicab,Cosine}KNN (euclideandistancematrixgpu.cu:87-105, :107-1031).  The
 // reference unions every tree's block of a point in an N-byte bitmap, scans the
 // bitmap per point and selects k with a histogram; here each (tree, leaf) block
-// is one tile job: the block's rows are staged in shared memory 32 dims at a
+// is split into tile jobs of 64 query rows against all the block's candidates:
+// the rows are staged in shared memory 32 dims at a
 // time, every (query, candidate) key of the block is computed by a 4x4 register
 // tile per thread in the reference's summation order, and each query's k best
 // are merged into its running sorted list by one warp (bitonic sort + merge via
@@ -40,7 +41,7 @@ __device__ __forceinline__ void load_r(const float* p, float (&v)[R]) {
 // union under (key, id), so all TILE variants give identical lists.
 template <int METRIC, int KPL, int TILE>
 __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d, int dpad,
-                                              SegView segs, const int64_t* __restrict__ ftab, int k,
+                                              SegView segs, const int64_t* __restrict__ ftab, int qtiles, int k,
                                               const int32_t* __restrict__ perm,
                                               const float* __restrict__ norms,
                                               float* __restrict__ rkey, uint32_t* __restrict__ rid,
@@ -55,29 +56,36 @@ __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d
   __shared__ int32_t qid[kTile], cid[kTile];
   __shared__ float qnorm[kTile], cnorm[kTile];
 
+  // block = (leaf, query tile): the tiles of a large leaf spread over the grid,
+  // and each query row's list is read and written by one block only
+  const int64_t leaf = blockIdx.x / qtiles;
+  const int qt = (int)(blockIdx.x - leaf * qtiles);
   int64_t lo, hi, blo, bhi;
   if (ftab) {  // explicit leaf table (reference-rule trees)
-    const int64_t* e = ftab + 4 * (int64_t)blockIdx.x;
+    const int64_t* e = ftab + 4 * leaf;
     lo = e[0];
     hi = e[1];
     blo = e[2];
     bhi = e[3];
   } else {
     int64_t j;
-    const SegEntry seg = segs.leaf(blockIdx.x, &j);
+    const SegEntry seg = segs.leaf(leaf, &j);
     leaf_block(seg, j, k, &lo, &hi, &blo, &bhi);
   }
   const int nq = (int)(hi - lo);
   const int nb = (int)(bhi - blo);
+  const int q0 = qt * kTile;
+  if (q0 >= nq) return;
 
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   const int warp = tid >> 5, lane = tid & 31;
   const float kInf = __int_as_float(0x7F800000);
   const int nchunks = (d + kDC - 1) / kDC;
 
-  if (pair_counter && tid == 0) atomicAdd(pair_counter, (unsigned long long)nq * (unsigned long long)(nb - 1));
+  if (pair_counter && tid == 0)
+    atomicAdd(pair_counter, (unsigned long long)min(kTile, nq - q0) * (unsigned long long)(nb - 1));
 
-  for (int q0 = 0; q0 < nq; q0 += kTile) {
+  {
     const int mq = min(kTile, nq - q0);
     if (tid < kTile) {
       const int32_t id = tid < mq ? perm[lo + q0 + tid] : -1;
@@ -200,13 +208,14 @@ __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d
 template <int METRIC, int TILE>
 static void launch_leaf_tile(const LeafArgs& a, const int32_t* perm, const int64_t* ftab, int64_t leaves, int kpl) {
   if (leaves <= 0) return;
-  dim3 grid((unsigned)leaves);
+  const int qtiles = (int)((a.maxleaf + TILE - 1) / TILE);
+  dim3 grid((unsigned)(leaves * qtiles));
   if (kpl == 1)
-    k_leaf<METRIC, 1, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 1, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, qtiles, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
   else if (kpl == 2)
-    k_leaf<METRIC, 2, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 2, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, qtiles, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
   else
-    k_leaf<METRIC, 4, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 4, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, qtiles, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
 }
 
 template <int METRIC>
