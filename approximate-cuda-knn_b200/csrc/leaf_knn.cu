@@ -40,8 +40,8 @@ __device__ __forceinline__ void load_r(const float* p, float (&v)[R]) {
 // same order whatever the tile, and each row's list is the k best of the
 // union under (key, id), so all TILE variants give identical lists.
 template <int METRIC, int KPL, int TILE>
-__global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d, int dpad,
-                                              SegView segs, const int64_t* __restrict__ ftab, int qtiles, int k,
+__global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* __restrict__ X, int d, int dpad,
+                                              SegView segs, const int64_t* __restrict__ ftab, int k,
                                               const int32_t* __restrict__ perm,
                                               const float* __restrict__ norms,
                                               float* __restrict__ rkey, uint32_t* __restrict__ rid,
@@ -56,10 +56,10 @@ __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d
   __shared__ int32_t qid[kTile], cid[kTile];
   __shared__ float qnorm[kTile], cnorm[kTile];
 
-  // block = (leaf, query tile): the tiles of a large leaf spread over the grid,
-  // and each query row's list is read and written by one block only
-  const int64_t leaf = blockIdx.x / qtiles;
-  const int qt = (int)(blockIdx.x - leaf * qtiles);
+  // block = (leaf, query tile): the 64-row (or 32-row) query tiles of a large
+  // leaf spread over gridDim.y, and each query row's list is read and written
+  // by one block only
+  const int64_t leaf = blockIdx.x;
   int64_t lo, hi, blo, bhi;
   if (ftab) {  // explicit leaf table (reference-rule trees)
     const int64_t* e = ftab + 4 * leaf;
@@ -74,18 +74,15 @@ __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d
   }
   const int nq = (int)(hi - lo);
   const int nb = (int)(bhi - blo);
-  const int q0 = qt * kTile;
-  if (q0 >= nq) return;
 
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   const int warp = tid >> 5, lane = tid & 31;
   const float kInf = __int_as_float(0x7F800000);
   const int nchunks = (d + kDC - 1) / kDC;
 
-  if (pair_counter && tid == 0)
-    atomicAdd(pair_counter, (unsigned long long)min(kTile, nq - q0) * (unsigned long long)(nb - 1));
-
-  {
+  for (int q0 = (int)blockIdx.y * kTile; q0 < nq; q0 += (int)gridDim.y * kTile) {
+    if (pair_counter && tid == 0)
+      atomicAdd(pair_counter, (unsigned long long)min(kTile, nq - q0) * (unsigned long long)(nb - 1));
     const int mq = min(kTile, nq - q0);
     if (tid < kTile) {
       const int32_t id = tid < mq ? perm[lo + q0 + tid] : -1;
@@ -208,14 +205,14 @@ __global__ void __launch_bounds__(256) k_leaf(const float* __restrict__ X, int d
 template <int METRIC, int TILE>
 static void launch_leaf_tile(const LeafArgs& a, const int32_t* perm, const int64_t* ftab, int64_t leaves, int kpl) {
   if (leaves <= 0) return;
-  const int qtiles = (int)((a.maxleaf + TILE - 1) / TILE);
-  dim3 grid((unsigned)(leaves * qtiles));
+  const int64_t qtiles = (a.maxleaf + TILE - 1) / TILE;
+  dim3 grid((unsigned)leaves, (unsigned)std::min<int64_t>(qtiles, 65535));
   if (kpl == 1)
-    k_leaf<METRIC, 1, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, qtiles, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 1, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
   else if (kpl == 2)
-    k_leaf<METRIC, 2, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, qtiles, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 2, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
   else
-    k_leaf<METRIC, 4, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, qtiles, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 4, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
 }
 
 template <int METRIC>
