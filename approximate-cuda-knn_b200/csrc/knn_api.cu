@@ -429,7 +429,7 @@ Layout single_layout(int64_t n, int depth) {
 int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, int trees,
              const Layout& lay, int metric, const int32_t* perm, const float* norms, Lists* L,
              unsigned long long* counter, cudaStream_t st, knn::LaunchLog& log, int tile = 0,
-             cudaEvent_t* kev = nullptr) {
+             cudaEvent_t* kev = nullptr, bool sparse = false) {
   const int kw = (k + 31) / 32;
   knn::launch_init_lists(L->key[L->cur], L->id[L->cur], L->flags[L->cur], n, k, kw, st);
   log.add(2);
@@ -443,6 +443,7 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
   a.segs = lay.segs;
   a.leaves = lay.leaves;
   a.maxleaf = lay.maxleaf;
+  a.maxblock = lay.maxblock;
   a.metric = metric;
   a.perm = perm;
   a.norms = norms;
@@ -455,10 +456,24 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
   a.foff = lay.foff;
   a.fcount = lay.fcount;
   a.stream = st;
+  if (sparse && metric != KNN_METRIC_COSINE && !lay.ftable) {
+    a.lmax = 256 * ((dpad + 255) / 256);
+    int rc = C->get("dmask", (size_t)lay.leaves * (dpad / 32 + 1), &a.dmask);
+    if (!rc) rc = C->get("dlist", (size_t)lay.leaves * a.lmax, &a.dlist);
+    if (!rc) rc = C->get("dnch", (size_t)lay.leaves, &a.dnch);
+    if (rc) return rc;
+  }
   int rc = knn::leaf_stage(a, log);
   if (rc) return fail_cuda(cudaGetLastError(), "leaf stage launch");
-  (void)C;
   return KNN_OK;
+}
+
+// Sparse-row leaf tiles (same keys, fewer dims read): forced on or off by the
+// option, else on when leaves hold at least 1024 points, where the per-tree
+// mask pass (one read of the points) is small beside the tiles.
+bool use_sparse_dims(const knn_options& o, int metric, const Layout& lay) {
+  if (metric == KNN_METRIC_COSINE || lay.ftable || o.sparse_dims < 0) return false;
+  return o.sparse_dims > 0 || lay.maxleaf >= 1024;
 }
 
 // Mixed precision: BF16 or FP16 tensor-core tiles select each point's best min(2k, 32)
@@ -563,7 +578,7 @@ int time_since(knn_context* C, cudaStream_t st, float* ms) {
 
 int tune_leaf_tile(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, const Layout& lay,
                    int metric, const int32_t* perm, const float* norms, const Lists& L, cudaStream_t st,
-                   int* best) {
+                   bool sparse, int* best) {
   Lists S = L;
   S.cur = 1 - L.cur;  // scratch lists
   float best_ms = 3.4e38f;
@@ -573,7 +588,7 @@ int tune_leaf_tile(knn_context* C, const float* X, int64_t n, int d, int dpad, i
     for (int rep = 0; rep < 2; ++rep) {
       knn::LaunchLog tl;
       KNN_CK(cudaEventRecord(C->tev[0], st));
-      int rc = run_leaf(C, X, n, d, dpad, k, 1, lay, metric, perm, norms, &S, nullptr, st, tl, tile);
+      int rc = run_leaf(C, X, n, d, dpad, k, 1, lay, metric, perm, norms, &S, nullptr, st, tl, tile, nullptr, sparse);
       if (!rc) rc = time_since(C, st, &ms);
       if (rc) return rc;
     }
@@ -612,6 +627,7 @@ int tune_prop_warps(knn_context* C, const float* X, int64_t n, int d, int dpad, 
 // cached, or tuned now (when allowed).
 struct Shapes {
   int leaf_tile = 0, prop_warps = 0;
+  bool sparse = false;  // FP32 leaf tiles read each block's non-zero dims only
   int tc_group = 0;  // tensor-core tiles: sibling leaves per tile
 };
 
@@ -649,6 +665,7 @@ int pick_shapes(knn_context* C, const knn_options& o, bool may_tune, bool fp32_l
                 int* err_flag) {
   sh->leaf_tile = o.leaf_tile;
   sh->prop_warps = o.prop_warps;
+  sh->sparse = fp32_leaf && use_sparse_dims(o, metric, lay);
   *tune_prop_after = false;
   const std::string key = tune_key(metric, d, k, lay.maxleaf);
   if (!fp32_leaf) {
@@ -676,7 +693,7 @@ int pick_shapes(knn_context* C, const knn_options& o, bool may_tune, bool fp32_l
   }
   if (!may_tune) return KNN_OK;
   if (fp32_leaf && !sh->leaf_tile) {
-    int rc = tune_leaf_tile(C, X, n, d, dpad, k, lay, metric, perm, norms, *L, st, &sh->leaf_tile);
+    int rc = tune_leaf_tile(C, X, n, d, dpad, k, lay, metric, perm, norms, *L, st, sh->sparse, &sh->leaf_tile);
     if (rc) return rc;
     C->tuned[key].first = sh->leaf_tile;
   }
@@ -953,7 +970,7 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
                        log, kev, sh.tc_group);
   } else {
     rc = run_leaf(C, P.X, n, d, P.dpad, k, trees, lay, metric, T.perm, norms, &L, stats ? counters : nullptr, st,
-                  log, sh.leaf_tile, kev);
+                  log, sh.leaf_tile, kev, sh.sparse);
   }
   if (rc) return rc;
   if (tune_prop) {
@@ -1032,6 +1049,7 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
     stats->leaf_path = tensor_leaf ? o.precision : 0;
     stats->tc_group = tensor_leaf ? std::min(std::max(sh.tc_group, 1), lay.tc_group_max) : 0;
     stats->leaf_fallback = (o.precision != KNN_PREC_FP32 && !tensor_leaf) ? 1 : 0;
+    stats->sparse_dims = (!tensor_leaf && sh.sparse) ? 1 : 0;
     stats->prop_warps = sh.prop_warps;
     unsigned long long host[2 + KNN_MAX_PROPS];
     KNN_CK(cudaMemcpy(host, counters, sizeof(host), cudaMemcpyDeviceToHost));
@@ -1147,7 +1165,7 @@ int group_compute(knn_context* C, const BatchGroup& g, int k, int trees, int pro
                        st, log, nullptr, sh.tc_group);
   else
     rc = run_leaf(C, X, g.ntot, g.d, g.dpad, k, trees, lay, metric, T.perm, norms, &L, nullptr, st, log,
-                  sh.leaf_tile);
+                  sh.leaf_tile, nullptr, sh.sparse);
   if (rc) return rc;
   if (tune_prop) {
     rc = finish_prop_tuning(C, o, X, g.ntot, g.d, g.dpad, k, metric, norms, T.perm, &L, lay.maxleaf, st, &sh);

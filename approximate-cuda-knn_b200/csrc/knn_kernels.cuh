@@ -97,6 +97,7 @@ struct LeafArgs {
   SegView segs;
   int64_t leaves;
   int64_t maxleaf;       // points in the largest leaf (query tiles per leaf)
+  int64_t maxblock;      // points in the largest leaf block (0: maxleaf)
   const int32_t* perm;   // [trees][n]
   const float* norms;    // [n] (COSINE) or null
   float* rkey;           // [n][k] in/out, sorted
@@ -108,6 +109,12 @@ struct LeafArgs {
   const int64_t* ftable;
   const int64_t* foff;
   const int64_t* fcount;
+  // sparse rows (EUCLIDEAN / TAXICAB, median trees): per tree, each leaf block's
+  // non-zero dims; null dlist: every block reads all dims
+  uint32_t* dmask;       // [leaves][dpad / 32 + 1]
+  int32_t* dlist;        // [leaves][lmax]
+  int32_t* dnch;         // [leaves]
+  int lmax;              // 256 * ceil(dpad / 256)
   cudaStream_t stream;
 };
 int leaf_stage(const LeafArgs& a, LaunchLog& log);

@@ -35,6 +35,82 @@ __device__ __forceinline__ void load_r(const float* p, float (&v)[R]) {
   }
 }
 
+// ------------------------------------------------------------ sparse rows --
+// A dim where every row of a leaf block is zero adds an exact +0 to each of the
+// block's EUCLIDEAN and TAXICAB sums ((0-0)^2 and |0-0|, added to a partial sum
+// that is never negative), so leaving it out keeps every key's bits.  Per leaf
+// block: a bit mask of the dims that are non-zero in some row, then the list of
+// those dims with the 256-dim groups kept apart (each group's dims padded with
+// -1 to whole 32-dim chunks), so that the per-group partial sums are formed over
+// the same terms in the same order as over all dims.
+constexpr int kDimRows = 1024;  // rows of a leaf block per mask block
+
+// grid (leaf, row part); mask [leaves][W] zeroed beforehand, W = dpad / 32 + 1.
+// Thread t of the block tests dims t, t + 256, ...: warp w's 32 lanes cover one
+// mask word, so each warp ORs whole words.
+__global__ void __launch_bounds__(256) k_leaf_dim_mask(const float* __restrict__ X, int dpad, SegView segs,
+                                                       int k, const int32_t* __restrict__ perm,
+                                                       uint32_t* __restrict__ mask, int W) {
+  const int64_t leaf = blockIdx.x;
+  int64_t j, lo, hi, blo, bhi;
+  const SegEntry seg = segs.leaf(leaf, &j);
+  leaf_block(seg, j, k, &lo, &hi, &blo, &bhi);
+  for (int64_t r0 = blo + (int64_t)blockIdx.y * kDimRows; r0 < bhi; r0 += (int64_t)gridDim.y * kDimRows) {
+    const int64_t r1 = min(bhi, r0 + kDimRows);
+    for (int dim0 = 0; dim0 < dpad; dim0 += 256) {
+      const int dim = dim0 + (int)threadIdx.x;
+      bool nz = false;
+      if (dim < dpad) {
+        int64_t r = r0;
+        for (; r + 4 <= r1 && !nz; r += 4) {  // four rows in flight
+          const int32_t p0 = __ldg(perm + r), p1 = __ldg(perm + r + 1);
+          const int32_t p2 = __ldg(perm + r + 2), p3 = __ldg(perm + r + 3);
+          const float v0 = __ldg(X + (size_t)p0 * dpad + dim), v1 = __ldg(X + (size_t)p1 * dpad + dim);
+          const float v2 = __ldg(X + (size_t)p2 * dpad + dim), v3 = __ldg(X + (size_t)p3 * dpad + dim);
+          nz = (v0 != 0.f) | (v1 != 0.f) | (v2 != 0.f) | (v3 != 0.f);
+        }
+        for (; r < r1 && !nz; ++r) nz = __ldg(X + (size_t)__ldg(perm + r) * dpad + dim) != 0.f;
+      }
+      const uint32_t bits = __ballot_sync(0xFFFFFFFFu, nz);
+      if ((threadIdx.x & 31) == 0 && bits) atomicOr(mask + leaf * W + (dim >> 5), bits);
+    }
+  }
+}
+
+// One warp per leaf: the listed dims of every 256-dim group in increasing order,
+// each group padded with -1 to a multiple of 32 entries; dnch[leaf] = chunks of
+// 32, or -1 when the list saves no chunk over the ceil(d / 32) chunks of all dims
+// (the block then reads rows whole).
+__global__ void __launch_bounds__(256) k_leaf_dim_list(const uint32_t* __restrict__ mask, int W, int d, int dpad,
+                                                       int64_t leaves, int32_t* __restrict__ dlist,
+                                                       int32_t* __restrict__ dnch, int lmax) {
+  const int64_t leaf = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (leaf >= leaves) return;
+  const uint32_t* m = mask + leaf * W;
+  int32_t* out = dlist + leaf * lmax;
+  int pos = 0;
+  for (int g = 0; g * 256 < dpad; ++g) {
+    // lane l holds dims 256 g + 8 l .. + 7
+    const int w = 8 * g + (lane >> 2);
+    const uint32_t bits = w < W ? (m[w] >> (8 * (lane & 3))) & 0xFFu : 0u;
+    const int c = __popc(bits);
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    int at = pos + incl - c;
+    for (uint32_t b = bits; b; b &= b - 1) out[at++] = 256 * g + 8 * lane + (__ffs(b) - 1);
+    const int padded = (total + 31) & ~31;
+    for (int e = total + lane; e < padded; e += 32) out[pos + e] = -1;
+    pos += padded;
+  }
+  if (lane == 0) dnch[leaf] = pos / 32 < (d + 31) / 32 ? pos / 32 : -1;
+}
+
 // TILE x TILE (query x candidate) tiles, 16 x 16 threads each holding an
 // R x R register tile, R = TILE / 16.  Every key is summed over dims in the
 // same order whatever the tile, and each row's list is the k best of the
@@ -45,7 +121,9 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* _
                                               const int32_t* __restrict__ perm,
                                               const float* __restrict__ norms,
                                               float* __restrict__ rkey, uint32_t* __restrict__ rid,
-                                              unsigned long long* __restrict__ pair_counter) {
+                                              unsigned long long* __restrict__ pair_counter,
+                                              const int32_t* __restrict__ dlist,
+                                              const int32_t* __restrict__ dnch, int lmax) {
   constexpr int kTile = TILE;
   constexpr int kSP = TILE + 4;
   constexpr int R = TILE / 16;
@@ -78,7 +156,13 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* _
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   const int warp = tid >> 5, lane = tid & 31;
   const float kInf = __int_as_float(0x7F800000);
-  const int nchunks = (d + kDC - 1) / kDC;
+  // sparse rows: this block's non-zero dims, 32 per chunk (null: all dims)
+  const int32_t* dl = nullptr;
+  int nchunks = (d + kDC - 1) / kDC;
+  if (METRIC != KNN_METRIC_COSINE && dlist && dnch[leaf] >= 0) {
+    dl = dlist + leaf * lmax;
+    nchunks = dnch[leaf];
+  }
 
   for (int q0 = (int)blockIdx.y * kTile; q0 < nq; q0 += (int)gridDim.y * kTile) {
     if (pair_counter && tid == 0)
@@ -112,10 +196,28 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* _
         for (int h = 0; h < kTile / 32; ++h) {
           const int f = tid + h * 256;
           const int r = f >> 3, c4 = f & 7;
-          const int dim = cd + 4 * c4;
           float4 qv = make_float4(0.f, 0.f, 0.f, 0.f), cv = qv;
-          if (r < mq && dim < dpad) qv = __ldg(reinterpret_cast<const float4*>(X + (size_t)qid[r] * dpad + dim));
-          if (r < mc && dim < dpad) cv = __ldg(reinterpret_cast<const float4*>(X + (size_t)cid[r] * dpad + dim));
+          if (dl) {  // four listed dims (-1: padding, read as zero)
+            const int4 dm = __ldg(reinterpret_cast<const int4*>(dl + cd + 4 * c4));
+            if (r < mq) {
+              const float* row = X + (size_t)qid[r] * dpad;
+              if (dm.x >= 0) qv.x = __ldg(row + dm.x);
+              if (dm.y >= 0) qv.y = __ldg(row + dm.y);
+              if (dm.z >= 0) qv.z = __ldg(row + dm.z);
+              if (dm.w >= 0) qv.w = __ldg(row + dm.w);
+            }
+            if (r < mc) {
+              const float* row = X + (size_t)cid[r] * dpad;
+              if (dm.x >= 0) cv.x = __ldg(row + dm.x);
+              if (dm.y >= 0) cv.y = __ldg(row + dm.y);
+              if (dm.z >= 0) cv.z = __ldg(row + dm.z);
+              if (dm.w >= 0) cv.w = __ldg(row + dm.w);
+            }
+          } else {
+            const int dim = cd + 4 * c4;
+            if (r < mq && dim < dpad) qv = __ldg(reinterpret_cast<const float4*>(X + (size_t)qid[r] * dpad + dim));
+            if (r < mc && dim < dpad) cv = __ldg(reinterpret_cast<const float4*>(X + (size_t)cid[r] * dpad + dim));
+          }
           Qs[4 * c4 + 0][r] = qv.x;
           Qs[4 * c4 + 1][r] = qv.y;
           Qs[4 * c4 + 2][r] = qv.z;
@@ -136,7 +238,10 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* _
 #pragma unroll
             for (int b = 0; b < R; ++b) part[a][b] = acc_step<METRIC>(qa[a], cb[b], part[a][b]);
         }
-        if (((cd + kDC) & 255) == 0 || ch == nchunks - 1) {
+        // end of a 256-dim group: its partial sum joins the total
+        const bool gend = ch == nchunks - 1 ||
+                          (dl ? (__ldg(dl + cd + kDC) >> 8) != (__ldg(dl + cd) >> 8) : ((cd + kDC) & 255) == 0);
+        if (gend) {
 #pragma unroll
           for (int a = 0; a < R; ++a)
 #pragma unroll
@@ -203,25 +308,38 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* _
 }
 
 template <int METRIC, int TILE>
-static void launch_leaf_tile(const LeafArgs& a, const int32_t* perm, const int64_t* ftab, int64_t leaves, int kpl) {
+static void launch_leaf_tile(const LeafArgs& a, const int32_t* perm, const int64_t* ftab, int64_t leaves, int kpl,
+                             const int32_t* dlist) {
   if (leaves <= 0) return;
   const int64_t qtiles = (a.maxleaf + TILE - 1) / TILE;
   dim3 grid((unsigned)leaves, (unsigned)std::min<int64_t>(qtiles, 65535));
   if (kpl == 1)
-    k_leaf<METRIC, 1, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 1, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter, dlist, a.dnch, a.lmax);
   else if (kpl == 2)
-    k_leaf<METRIC, 2, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 2, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter, dlist, a.dnch, a.lmax);
   else
-    k_leaf<METRIC, 4, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter);
+    k_leaf<METRIC, 4, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter, dlist, a.dnch, a.lmax);
 }
 
 template <int METRIC>
-static void launch_leaf_metric(const LeafArgs& a, int t, int kpl) {
+static void launch_leaf_metric(const LeafArgs& a, int t, int kpl, LaunchLog& log) {
   const int32_t* perm = a.perm + (size_t)t * a.n;
   const int64_t* ftab = a.ftable ? a.ftable + 4 * a.foff[t] : nullptr;
   const int64_t leaves = a.ftable ? a.fcount[t] : a.leaves;
-  if (a.tile == 32) launch_leaf_tile<METRIC, 32>(a, perm, ftab, leaves, kpl);
-  else launch_leaf_tile<METRIC, 64>(a, perm, ftab, leaves, kpl);
+  const int32_t* dlist = nullptr;
+  if (a.dlist && !ftab && METRIC != KNN_METRIC_COSINE && leaves > 0) {
+    const int W = a.dpad / 32 + 1;
+    cudaMemsetAsync(a.dmask, 0, sizeof(uint32_t) * (size_t)leaves * W, a.stream);
+    const int64_t splits = (std::max(a.maxblock, a.maxleaf) + kDimRows - 1) / kDimRows;
+    k_leaf_dim_mask<<<dim3((unsigned)leaves, (unsigned)std::min<int64_t>(splits, 65535)), 256, 0, a.stream>>>(
+        a.X, a.dpad, a.segs, a.k, perm, a.dmask, W);
+    k_leaf_dim_list<<<(unsigned)((leaves + 7) / 8), 256, 0, a.stream>>>(a.dmask, W, a.d, a.dpad, leaves,
+                                                                        a.dlist, a.dnch, a.lmax);
+    log.add(3);
+    dlist = a.dlist;
+  }
+  if (a.tile == 32) launch_leaf_tile<METRIC, 32>(a, perm, ftab, leaves, kpl, dlist);
+  else launch_leaf_tile<METRIC, 64>(a, perm, ftab, leaves, kpl, dlist);
 }
 
 // One launch per tree: a point sits in one leaf per tree, so the leaves of a
@@ -230,9 +348,9 @@ int leaf_stage(const LeafArgs& a, LaunchLog& log) {
   const int kpl = kpl_for(a.k);
   for (int t = a.first_tree; t < a.first_tree + a.trees; ++t) {
     if (a.kev) cudaEventRecord(a.kev[2 * (t - a.first_tree)], a.stream);
-    if (a.metric == KNN_METRIC_EUCLIDEAN) launch_leaf_metric<KNN_METRIC_EUCLIDEAN>(a, t, kpl);
-    else if (a.metric == KNN_METRIC_TAXICAB) launch_leaf_metric<KNN_METRIC_TAXICAB>(a, t, kpl);
-    else launch_leaf_metric<KNN_METRIC_COSINE>(a, t, kpl);
+    if (a.metric == KNN_METRIC_EUCLIDEAN) launch_leaf_metric<KNN_METRIC_EUCLIDEAN>(a, t, kpl, log);
+    else if (a.metric == KNN_METRIC_TAXICAB) launch_leaf_metric<KNN_METRIC_TAXICAB>(a, t, kpl, log);
+    else launch_leaf_metric<KNN_METRIC_COSINE>(a, t, kpl, log);
     if (a.kev) cudaEventRecord(a.kev[2 * (t - a.first_tree) + 1], a.stream);
     log.add();
   }

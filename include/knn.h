@@ -106,7 +106,12 @@ typedef struct knn_options {
                                 1, 2 or 4 (0: tuned with autotune, else the most that
                                 fit); a row keeps its own leaf's columns, so results do
                                 not depend on it; capped at what the leaves allow      */
-  int32_t reserved[2];
+  int32_t sparse_dims;       /* FP32 leaf tiles, EUCLIDEAN and TAXICAB: 1 each leaf block
+                                reads only the dims that are non-zero in some of its
+                                rows (the left-out terms are exact zeros, so the keys
+                                keep their bits); -1 never; 0 when leaves hold at
+                                least 1024 points                                     */
+  int32_t reserved[1];
 } knn_options;
 
 typedef struct knn_stats {
@@ -131,7 +136,8 @@ typedef struct knn_stats {
                                 tiles, 2 FP16 tensor-core tiles                        */
   int32_t leaf_fallback;     /* 1: tensor-core precision was asked for, FP32 ran        */
   int32_t tc_group;          /* sibling leaves per tensor-core tile used (0: FP32 path) */
-  int32_t reserved32;
+  int32_t sparse_dims;       /* 1: the FP32 leaf tiles read each block's non-zero dims
+                                (knn_build_ex; 0 from knn_build_batch)               */
   int64_t reserved[4];
 } knn_stats;
 
