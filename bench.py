@@ -725,6 +725,7 @@ CONFIG_TARGETS = {
 }
 PATH_OPTIONS = {
     "plain_fp32": dict(precision=0),
+    "plain_fp32_all_dims": dict(precision=0, sparse_dims=-1),
     "mixed": dict(precision=1),
     "mixed_f16": dict(precision=2),
     "mixed_learned": dict(precision=1, learned_splits=1),
@@ -778,6 +779,9 @@ def run_config(args):
     peak, peak_kind = measured_peaks()
     runs = {f"{p}@target": (p, tuple(v)) for p, v in CONFIG_TARGETS[args.workload].items() if v}
     runs["plain_fp32@literal"] = ("plain_fp32", (cfg["trees"], cfg["leaf"], cfg["props"]))
+    if args.ab_sparse and CONFIG_TARGETS[args.workload].get("plain_fp32"):
+        # the same graph with every leaf block reading all dims
+        runs["plain_fp32_all_dims@target"] = ("plain_fp32_all_dims", tuple(CONFIG_TARGETS[args.workload]["plain_fp32"]))
     res = {}
     for name, (path, (T, L, P)) in runs.items():
         kw = dict(PATH_OPTIONS[path])
@@ -809,6 +813,7 @@ def run_config(args):
         sd = st.as_dict()
         res[name] = {"params": {"trees": T, "leaf": L, "props": P}, "ms_per_build": ms,
                      "points_per_s": n / (ms / 1e3), "accuracy": acc, "leaf_path": sd["leaf_path"],
+                     "sparse_dims": sd["sparse_dims"],
                      "stages_ms": {kk: sd[kk] for kk in ("ms_learn", "ms_trees", "ms_leaf", "ms_propagate")},
                      "propagate_roofline": prop_roofline(n, d, k, s_bytes, sd["prop_candidates"],
                                                          sd["ms_propagate"], peak)}
@@ -816,8 +821,12 @@ def run_config(args):
     ratios = {}
     if plain:
         for name, r in res.items():
-            if name.endswith("@target") and name != "plain_fp32@target":
+            if name.endswith("@target") and not name.startswith("plain_fp32"):
                 ratios[name.split("@")[0] + "_vs_plain_at_equal_recall"] = plain["ms_per_build"] / r["ms_per_build"]
+        dense = res.get("plain_fp32_all_dims@target")
+        if dense:
+            ratios["sparse_rows_speedup"] = dense["ms_per_build"] / plain["ms_per_build"]
+            ratios["sparse_rows_identical_recall"] = dense["accuracy"] == plain["accuracy"]
     print(json.dumps({"workload": args.workload, "n": n, "d": d, "k": k, "metric": METRIC_NAMES[metric],
                       "dtype": str(x.dtype), "queries": int(len(q)), "steps": args.steps, "warmup": args.warmup,
                       "peak_source": peak_kind, "paths": res, **ratios}), flush=True)
@@ -1377,6 +1386,8 @@ def main():
     ap.add_argument("--grid-leaf", default=None, help="comma-separated leaf sizes to sweep")
     ap.add_argument("--max-props", type=int, default=None)
     ap.add_argument("--paths", default=None, help="comma-separated paths to sweep")
+    ap.add_argument("--ab-sparse", action="store_true",
+                    help="configurations: also time the plain target with sparse-row leaf tiles off")
     ap.add_argument("--reference-gpu", action="store_true",
                     help="time the reference's own sm_100a build (oracle/_ref/hello) on the workload")
     ap.add_argument("--ref-limit", type=float, default=300.0, help="seconds per reference run")
