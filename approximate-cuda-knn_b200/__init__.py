@@ -76,7 +76,7 @@ class KnnOptions(ctypes.Structure):
         ("split_rule", ctypes.c_int32),
         ("tc_group", ctypes.c_int32),
         ("sparse_dims", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 1),
+        ("tile_pairs", ctypes.c_int32),
     ]
 
 
@@ -103,7 +103,9 @@ class KnnStats(ctypes.Structure):
         ("leaf_fallback", ctypes.c_int32),
         ("tc_group", ctypes.c_int32),
         ("sparse_dims", ctypes.c_int32),
-        ("reserved", ctypes.c_int64 * 4),
+        ("tile_pairs", ctypes.c_int32),
+        ("reserved32", ctypes.c_int32),
+        ("reserved", ctypes.c_int64 * 3),
     ]
 
     def as_dict(self) -> dict:
@@ -116,7 +118,7 @@ class KnnStats(ctypes.Structure):
             "launches": self.launches, "leaf_pairs": self.leaf_pairs,
             "leaf_tile": self.leaf_tile, "prop_warps": self.prop_warps,
             "leaf_path": self.leaf_path, "leaf_fallback": self.leaf_fallback, "tc_group": self.tc_group,
-            "sparse_dims": self.sparse_dims,
+            "sparse_dims": self.sparse_dims, "tile_pairs": self.tile_pairs,
             "prop_candidates": [self.prop_candidates[i] for i in range(n)],
         }
 
@@ -220,12 +222,14 @@ def knn_build(points, k: int, trees: int, leaf: int, props: int, metric: int = 0
               seed: int = 0, precision: int = PREC_FP32, learned: bool = False,
               stats: bool = False, context=None, mlp_sample: int = 0, mlp_steps: int = 0,
               autotune: bool = False, leaf_tile: int = 0, prop_warps: int = 0,
-              split_rule: int = 0, tc_group: int = 0, sparse_dims: int = 0):
+              split_rule: int = 0, tc_group: int = 0, sparse_dims: int = 0, tile_pairs: int = 0):
     """k-NN graph of ``points`` ([n, d] float32/float16, host memory).
 
     ``sparse_dims`` (FP32 leaf tiles, EUCLIDEAN/TAXICAB): 1 each leaf block
     reads only its rows' non-zero dims, -1 never, 0 when leaves hold >= 1024
-    points; the graph is the same either way.  ``learned`` builds the trees on the learned split network's embedding
+    points; the graph is the same either way.  ``tile_pairs`` -1 computes
+    every FP32 leaf key from both of its points instead of once (same graph).
+    ``learned`` builds the trees on the learned split network's embedding
     (trained on a sample of ``mlp_sample`` points for ``mlp_steps`` steps; 0
     picks the library default).  Returns ``(idx int32 [n, k], dist float32
     [n, k])`` sorted by (distance, index), plus a stats dict when ``stats``."""
@@ -238,7 +242,7 @@ def knn_build(points, k: int, trees: int, leaf: int, props: int, metric: int = 0
                           learned_splits=int(bool(learned)), mlp_sample=mlp_sample,
                           mlp_steps=mlp_steps, autotune=int(bool(autotune)), leaf_tile=leaf_tile,
                           prop_warps=prop_warps, split_rule=split_rule, tc_group=tc_group,
-                          sparse_dims=sparse_dims)
+                          sparse_dims=sparse_dims, tile_pairs=tile_pairs)
     st = KnnStats()
     st.struct_size = ctypes.sizeof(KnnStats)
     rc = lib.knn_build_ex(context, _ptr(x), n, d, k, trees, leaf, props, metric, seed,
@@ -251,7 +255,7 @@ def knn_build(points, k: int, trees: int, leaf: int, props: int, metric: int = 0
 def knn_build_batch(datasets, k: int, trees: int, leaf: int, props: int, metric: int = 0,
                     seeds=None, precision: int = PREC_FP32, stats: bool = False, context=None,
                     autotune: bool = False, leaf_tile: int = 0, prop_warps: int = 0, tc_group: int = 0,
-                    sparse_dims: int = 0):
+                    sparse_dims: int = 0, tile_pairs: int = 0):
     """k-NN graphs of many independent point sets in one call.
 
     ``datasets``: sequence of [n_i, d_i] arrays (all float32 or all float16);
@@ -277,7 +281,7 @@ def knn_build_batch(datasets, k: int, trees: int, leaf: int, props: int, metric:
     f16 = bool(xs) and xs[0].dtype == np.float16
     opt = default_options(dtype=F16 if f16 else F32, precision=precision,
                           autotune=int(bool(autotune)), leaf_tile=leaf_tile, prop_warps=prop_warps,
-                          tc_group=tc_group, sparse_dims=sparse_dims)
+                          tc_group=tc_group, sparse_dims=sparse_dims, tile_pairs=tile_pairs)
     st = KnnStats()
     st.struct_size = ctypes.sizeof(KnnStats)
     _check(load_library().knn_build_batch(context, arr, len(xs), k, trees, leaf, props, metric,

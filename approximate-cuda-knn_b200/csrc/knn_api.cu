@@ -385,6 +385,7 @@ struct Layout {
   int64_t leaves = 1, maxleaf = 1;
   int64_t maxblock = 0;  // bound on the points of a leaf block (0: unknown)
   int tc_group_max = 1;  // sibling leaves a tensor-core tile may hold (1, 2 or 4)
+  bool own_blocks = false;  // every leaf holds k+1 points, so each leaf is its own block
   // reference-rule trees: explicit leaf table (device) and per-tree offsets / counts (host)
   const int64_t* ftable = nullptr;
   const int64_t* foff = nullptr;
@@ -405,6 +406,14 @@ int64_t host_max_block(int64_t n, int depth, int k) {
 // points, the smallest leaf of every segment (floor(n / 2^depth) points)
 // holding k+1, and every segment at least log2 G levels deep so that groups
 // never straddle two sets.
+// Every leaf of every segment holds at least k+1 points (the smallest leaf of a
+// median tree holds floor(n / 2^depth)), so no leaf block climbs above its leaf.
+bool leaves_own_blocks(const knn::SegEntry* hsegs, int nseg, int k) {
+  for (int i = 0; i < nseg; ++i)
+    if ((hsegs[i].n >> hsegs[i].depth) < k + 1) return false;
+  return true;
+}
+
 int tc_group_max(const knn::SegEntry* hsegs, int nseg, int k, int64_t maxleaf) {
   int g = 1;
   for (int cand = 2, lg = 1; cand <= 4; cand *= 2, ++lg) {
@@ -429,7 +438,7 @@ Layout single_layout(int64_t n, int depth) {
 int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, int trees,
              const Layout& lay, int metric, const int32_t* perm, const float* norms, Lists* L,
              unsigned long long* counter, cudaStream_t st, knn::LaunchLog& log, int tile = 0,
-             cudaEvent_t* kev = nullptr, bool sparse = false) {
+             cudaEvent_t* kev = nullptr, bool sparse = false, bool pairs = false) {
   const int kw = (k + 31) / 32;
   knn::launch_init_lists(L->key[L->cur], L->id[L->cur], L->flags[L->cur], n, k, kw, st);
   log.add(2);
@@ -456,6 +465,7 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
   a.foff = lay.foff;
   a.fcount = lay.fcount;
   a.stream = st;
+  a.pairs = pairs && lay.own_blocks && !lay.ftable;
   if (sparse && metric != KNN_METRIC_COSINE && !lay.ftable) {
     a.lmax = 256 * ((dpad + 255) / 256);
     int rc = C->get("dmask", (size_t)lay.leaves * (dpad / 32 + 1), &a.dmask);
@@ -474,6 +484,12 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
 bool use_sparse_dims(const knn_options& o, int metric, const Layout& lay) {
   if (metric == KNN_METRIC_COSINE || lay.ftable || o.sparse_dims < 0) return false;
   return o.sparse_dims > 0 || lay.maxleaf >= 1024;
+}
+
+// Symmetric tile pairs (each key computed once for both of its points): on
+// unless the option turns them off, wherever every leaf is its own block.
+bool use_tile_pairs(const knn_options& o, const Layout& lay) {
+  return o.tile_pairs >= 0 && lay.own_blocks && !lay.ftable;
 }
 
 // Mixed precision: BF16 or FP16 tensor-core tiles select each point's best min(2k, 32)
@@ -578,7 +594,7 @@ int time_since(knn_context* C, cudaStream_t st, float* ms) {
 
 int tune_leaf_tile(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, const Layout& lay,
                    int metric, const int32_t* perm, const float* norms, const Lists& L, cudaStream_t st,
-                   bool sparse, int* best) {
+                   bool sparse, bool pairs, int* best) {
   Lists S = L;
   S.cur = 1 - L.cur;  // scratch lists
   float best_ms = 3.4e38f;
@@ -588,7 +604,8 @@ int tune_leaf_tile(knn_context* C, const float* X, int64_t n, int d, int dpad, i
     for (int rep = 0; rep < 2; ++rep) {
       knn::LaunchLog tl;
       KNN_CK(cudaEventRecord(C->tev[0], st));
-      int rc = run_leaf(C, X, n, d, dpad, k, 1, lay, metric, perm, norms, &S, nullptr, st, tl, tile, nullptr, sparse);
+      int rc = run_leaf(C, X, n, d, dpad, k, 1, lay, metric, perm, norms, &S, nullptr, st, tl, tile, nullptr, sparse,
+                        pairs);
       if (!rc) rc = time_since(C, st, &ms);
       if (rc) return rc;
     }
@@ -628,6 +645,7 @@ int tune_prop_warps(knn_context* C, const float* X, int64_t n, int d, int dpad, 
 struct Shapes {
   int leaf_tile = 0, prop_warps = 0;
   bool sparse = false;  // FP32 leaf tiles read each block's non-zero dims only
+  bool pairs = false;   // FP32 leaf tiles computed once per tile pair
   int tc_group = 0;  // tensor-core tiles: sibling leaves per tile
 };
 
@@ -666,6 +684,7 @@ int pick_shapes(knn_context* C, const knn_options& o, bool may_tune, bool fp32_l
   sh->leaf_tile = o.leaf_tile;
   sh->prop_warps = o.prop_warps;
   sh->sparse = fp32_leaf && use_sparse_dims(o, metric, lay);
+  sh->pairs = fp32_leaf && use_tile_pairs(o, lay);
   *tune_prop_after = false;
   const std::string key = tune_key(metric, d, k, lay.maxleaf);
   if (!fp32_leaf) {
@@ -693,7 +712,8 @@ int pick_shapes(knn_context* C, const knn_options& o, bool may_tune, bool fp32_l
   }
   if (!may_tune) return KNN_OK;
   if (fp32_leaf && !sh->leaf_tile) {
-    int rc = tune_leaf_tile(C, X, n, d, dpad, k, lay, metric, perm, norms, *L, st, sh->sparse, &sh->leaf_tile);
+    int rc = tune_leaf_tile(C, X, n, d, dpad, k, lay, metric, perm, norms, *L, st, sh->sparse, sh->pairs,
+                            &sh->leaf_tile);
     if (rc) return rc;
     C->tuned[key].first = sh->leaf_tile;
   }
@@ -945,6 +965,7 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
     e.n = n;
     e.depth = T.depth;
     lay.tc_group_max = tc_group_max(&e, 1, k, lay.maxleaf);
+    lay.own_blocks = leaves_own_blocks(&e, 1, k);
   }
   if (ftab_d) {
     lay.ftable = ftab_d;
@@ -970,7 +991,7 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
                        log, kev, sh.tc_group);
   } else {
     rc = run_leaf(C, P.X, n, d, P.dpad, k, trees, lay, metric, T.perm, norms, &L, stats ? counters : nullptr, st,
-                  log, sh.leaf_tile, kev, sh.sparse);
+                  log, sh.leaf_tile, kev, sh.sparse, sh.pairs);
   }
   if (rc) return rc;
   if (tune_prop) {
@@ -1050,6 +1071,7 @@ int build_impl(knn_context* C, const void* points, int64_t n, int32_t d, int32_t
     stats->tc_group = tensor_leaf ? std::min(std::max(sh.tc_group, 1), lay.tc_group_max) : 0;
     stats->leaf_fallback = (o.precision != KNN_PREC_FP32 && !tensor_leaf) ? 1 : 0;
     stats->sparse_dims = (!tensor_leaf && sh.sparse) ? 1 : 0;
+    stats->tile_pairs = (!tensor_leaf && sh.pairs) ? 1 : 0;
     stats->prop_warps = sh.prop_warps;
     unsigned long long host[2 + KNN_MAX_PROPS];
     KNN_CK(cudaMemcpy(host, counters, sizeof(host), cudaMemcpyDeviceToHost));
@@ -1153,6 +1175,7 @@ int group_compute(knn_context* C, const BatchGroup& g, int k, int trees, int pro
   lay.maxleaf = g.maxleaf;
   for (const auto& e : g.hsegs) lay.maxblock = std::max(lay.maxblock, host_max_block(e.n, e.depth, k));
   lay.tc_group_max = tc_group_max(g.hsegs.data(), (int)g.hsegs.size(), k, g.maxleaf);
+  lay.own_blocks = leaves_own_blocks(g.hsegs.data(), (int)g.hsegs.size(), k);
   const bool tensor_leaf = precision != KNN_PREC_FP32 && metric != KNN_METRIC_TAXICAB && g.d <= 256 &&
                            k <= 32;
   Shapes sh;
@@ -1165,7 +1188,7 @@ int group_compute(knn_context* C, const BatchGroup& g, int k, int trees, int pro
                        st, log, nullptr, sh.tc_group);
   else
     rc = run_leaf(C, X, g.ntot, g.d, g.dpad, k, trees, lay, metric, T.perm, norms, &L, nullptr, st, log,
-                  sh.leaf_tile, nullptr, sh.sparse);
+                  sh.leaf_tile, nullptr, sh.sparse, sh.pairs);
   if (rc) return rc;
   if (tune_prop) {
     rc = finish_prop_tuning(C, o, X, g.ntot, g.d, g.dpad, k, metric, norms, T.perm, &L, lay.maxleaf, st, &sh);

@@ -115,6 +115,9 @@ struct LeafArgs {
   int32_t* dlist;        // [leaves][lmax]
   int32_t* dnch;         // [leaves]
   int lmax;              // 256 * ceil(dpad / 256)
+  // every leaf is its own block (at least k+1 points, median trees): each tile
+  // pair of a leaf is computed once and merged into both sides (k_leaf_pair)
+  bool pairs;
   cudaStream_t stream;
 };
 int leaf_stage(const LeafArgs& a, LaunchLog& log);

@@ -111,10 +111,154 @@ __global__ void __launch_bounds__(256) k_leaf_dim_list(const uint32_t* __restric
   if (lane == 0) dnch[leaf] = pos / 32 < (d + 31) / 32 ? pos / 32 : -1;
 }
 
-// TILE x TILE (query x candidate) tiles, 16 x 16 threads each holding an
-// R x R register tile, R = TILE / 16.  Every key is summed over dims in the
-// same order whatever the tile, and each row's list is the k best of the
-// union under (key, id), so all TILE variants give identical lists.
+// Keys of one TILE x TILE tile: rows qid[0..mq) against columns cid[0..mc)
+// (ids; -1 past the end), 16 x 16 threads each holding an R x R register
+// tile, R = TILE / 16.  Each key is summed over the block's chunks of 32 dims
+// (all dims, or the listed non-zero dims dl of a sparse block) in the
+// reference's order: a sequential partial per 256-dim group, added to the
+// total at the group's end.  Ks receives the keys, +inf outside mq x mc.
+template <int METRIC, int TILE>
+__device__ __forceinline__ void tile_keys(const float* __restrict__ X, int dpad, const int32_t* __restrict__ dl,
+                                          int nchunks, int mq, int mc, const int32_t* qid, const int32_t* cid,
+                                          const float* qnorm, const float* cnorm, float (*Qs)[TILE + 4],
+                                          float (*Cs)[TILE + 4], float (*Ks)[TILE + 1]) {
+  constexpr int R = TILE / 16;
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  float part[R][R], total[R][R];
+#pragma unroll
+  for (int a = 0; a < R; ++a)
+#pragma unroll
+    for (int b = 0; b < R; ++b) {
+      part[a][b] = 0.f;
+      total[a][b] = 0.f;
+    }
+  for (int ch = 0; ch < nchunks; ++ch) {
+    const int cd = ch * kDC;
+#pragma unroll
+    for (int h = 0; h < TILE / 32; ++h) {
+      const int f = tid + h * 256;
+      const int r = f >> 3, c4 = f & 7;
+      float4 qv = make_float4(0.f, 0.f, 0.f, 0.f), cv = qv;
+      if (dl) {  // four listed dims (-1: padding, read as zero)
+        const int4 dm = __ldg(reinterpret_cast<const int4*>(dl + cd + 4 * c4));
+        if (r < mq) {
+          const float* row = X + (size_t)qid[r] * dpad;
+          if (dm.x >= 0) qv.x = __ldg(row + dm.x);
+          if (dm.y >= 0) qv.y = __ldg(row + dm.y);
+          if (dm.z >= 0) qv.z = __ldg(row + dm.z);
+          if (dm.w >= 0) qv.w = __ldg(row + dm.w);
+        }
+        if (r < mc) {
+          const float* row = X + (size_t)cid[r] * dpad;
+          if (dm.x >= 0) cv.x = __ldg(row + dm.x);
+          if (dm.y >= 0) cv.y = __ldg(row + dm.y);
+          if (dm.z >= 0) cv.z = __ldg(row + dm.z);
+          if (dm.w >= 0) cv.w = __ldg(row + dm.w);
+        }
+      } else {
+        const int dim = cd + 4 * c4;
+        if (r < mq && dim < dpad) qv = __ldg(reinterpret_cast<const float4*>(X + (size_t)qid[r] * dpad + dim));
+        if (r < mc && dim < dpad) cv = __ldg(reinterpret_cast<const float4*>(X + (size_t)cid[r] * dpad + dim));
+      }
+      Qs[4 * c4 + 0][r] = qv.x;
+      Qs[4 * c4 + 1][r] = qv.y;
+      Qs[4 * c4 + 2][r] = qv.z;
+      Qs[4 * c4 + 3][r] = qv.w;
+      Cs[4 * c4 + 0][r] = cv.x;
+      Cs[4 * c4 + 1][r] = cv.y;
+      Cs[4 * c4 + 2][r] = cv.z;
+      Cs[4 * c4 + 3][r] = cv.w;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int dd = 0; dd < kDC; ++dd) {
+      float qa[R], cb[R];
+      load_r<R>(&Qs[dd][ty * R], qa);
+      load_r<R>(&Cs[dd][tx * R], cb);
+#pragma unroll
+      for (int a = 0; a < R; ++a)
+#pragma unroll
+        for (int b = 0; b < R; ++b) part[a][b] = acc_step<METRIC>(qa[a], cb[b], part[a][b]);
+    }
+    // end of a 256-dim group: its partial sum joins the total
+    const bool gend = ch == nchunks - 1 ||
+                      (dl ? (__ldg(dl + cd + kDC) >> 8) != (__ldg(dl + cd) >> 8) : ((cd + kDC) & 255) == 0);
+    if (gend) {
+#pragma unroll
+      for (int a = 0; a < R; ++a)
+#pragma unroll
+        for (int b = 0; b < R; ++b) {
+          total[a][b] = __fadd_rn(total[a][b], part[a][b]);
+          part[a][b] = 0.f;
+        }
+    }
+    __syncthreads();
+  }
+  const float kInf = __int_as_float(0x7F800000);
+#pragma unroll
+  for (int a = 0; a < R; ++a)
+#pragma unroll
+    for (int b = 0; b < R; ++b) {
+      const int qq = ty * R + a, cc = tx * R + b;
+      float key = total[a][b];
+      if (METRIC == KNN_METRIC_COSINE) key = cosine_key(key, qnorm[qq], cnorm[cc]);
+      Ks[qq][cc] = (qq < mq && cc < mc) ? key : kInf;
+    }
+}
+
+// Merge rows rowid[0..mrow) of a tile into their running sorted lists against
+// the tile's columns colid[0..mcol): keys Ks[row][col], or Ks[col][row] when
+// TRANS (the tile read from its other side: every key is symmetric in its two
+// points, bit for bit).  One warp per row: bitonic insertion via shuffles.
+template <int KPL, int TILE, bool TRANS>
+__device__ __forceinline__ void merge_rows(int k, int mrow, int mcol, const int32_t* rowid, const int32_t* colid,
+                                           const float (*Ks)[TILE + 1], float* __restrict__ rkey,
+                                           uint32_t* __restrict__ rid) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const float kInf = __int_as_float(0x7F800000);
+  for (int rr = warp; rr < mrow; rr += 8) {
+    const uint32_t i = (uint32_t)rowid[rr];
+    WarpList<KPL> L;
+#pragma unroll
+    for (int r = 0; r < KPL; ++r) {
+      const int e = r * 32 + lane;
+      if (e < k) {
+        L.key[r] = rkey[(size_t)i * k + e];
+        L.id[r] = rid[(size_t)i * k + e];
+      } else {
+        L.key[r] = kInf;
+        L.id[r] = kNoId;
+      }
+    }
+    for (int cb = 0; cb < mcol; cb += 32) {
+      const int c = cb + lane;
+      const bool inrange = c < mcol;
+      const float ck = inrange ? (TRANS ? Ks[c][rr] : Ks[rr][c]) : kInf;
+      const uint32_t ci = inrange ? (uint32_t)colid[c] : kNoId;
+      float tk;
+      uint32_t ti;
+      warp_list_get(L, k - 1, tk, ti);
+      bool pass = inrange && ci != i && cand_less(ck, ci, tk, ti);
+      if (!__any_sync(0xFFFFFFFFu, pass)) continue;
+      const bool dup = warp_list_contains(L, ci, k);
+      pass = pass && !dup;
+      if (!__any_sync(0xFFFFFFFFu, pass)) continue;
+      warp_list_insert(L, pass ? ck : kInf, pass ? ci : kNoId);
+    }
+#pragma unroll
+    for (int r = 0; r < KPL; ++r) {
+      const int e = r * 32 + lane;
+      if (e < k) {
+        rkey[(size_t)i * k + e] = L.key[r];
+        rid[(size_t)i * k + e] = L.id[r];
+      }
+    }
+  }
+}
+
+// Every key is summed over dims in the same order whatever the tile, and each
+// row's list is the k best of the union under (key, id), so all TILE variants
+// (and the pair schedule below) give identical lists.
 template <int METRIC, int KPL, int TILE>
 __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* __restrict__ X, int d, int dpad,
                                               SegView segs, const int64_t* __restrict__ ftab, int k,
@@ -125,11 +269,9 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* _
                                               const int32_t* __restrict__ dlist,
                                               const int32_t* __restrict__ dnch, int lmax) {
   constexpr int kTile = TILE;
-  constexpr int kSP = TILE + 4;
-  constexpr int R = TILE / 16;
-  static_assert(R == 2 || R == 4, "tile of 32 or 64");
-  __shared__ __align__(16) float Qs[kDC][kSP];
-  __shared__ __align__(16) float Cs[kDC][kSP];
+  static_assert(TILE == 32 || TILE == 64, "tile of 32 or 64");
+  __shared__ __align__(16) float Qs[kDC][TILE + 4];
+  __shared__ __align__(16) float Cs[kDC][TILE + 4];
   __shared__ float Ks[kTile][kTile + 1];
   __shared__ int32_t qid[kTile], cid[kTile];
   __shared__ float qnorm[kTile], cnorm[kTile];
@@ -152,10 +294,7 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* _
   }
   const int nq = (int)(hi - lo);
   const int nb = (int)(bhi - blo);
-
-  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
-  const int warp = tid >> 5, lane = tid & 31;
-  const float kInf = __int_as_float(0x7F800000);
+  const int tid = threadIdx.x;
   // sparse rows: this block's non-zero dims, 32 per chunk (null: all dims)
   const int32_t* dl = nullptr;
   int nchunks = (d + kDC - 1) / kDC;
@@ -181,136 +320,110 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* _
         if (METRIC == KNN_METRIC_COSINE) cnorm[tid] = id >= 0 ? norms[id] : 0.f;
       }
       __syncthreads();
-
-      float part[R][R], total[R][R];
-#pragma unroll
-      for (int a = 0; a < R; ++a)
-#pragma unroll
-        for (int b = 0; b < R; ++b) {
-          part[a][b] = 0.f;
-          total[a][b] = 0.f;
-        }
-      for (int ch = 0; ch < nchunks; ++ch) {
-        const int cd = ch * kDC;
-#pragma unroll
-        for (int h = 0; h < kTile / 32; ++h) {
-          const int f = tid + h * 256;
-          const int r = f >> 3, c4 = f & 7;
-          float4 qv = make_float4(0.f, 0.f, 0.f, 0.f), cv = qv;
-          if (dl) {  // four listed dims (-1: padding, read as zero)
-            const int4 dm = __ldg(reinterpret_cast<const int4*>(dl + cd + 4 * c4));
-            if (r < mq) {
-              const float* row = X + (size_t)qid[r] * dpad;
-              if (dm.x >= 0) qv.x = __ldg(row + dm.x);
-              if (dm.y >= 0) qv.y = __ldg(row + dm.y);
-              if (dm.z >= 0) qv.z = __ldg(row + dm.z);
-              if (dm.w >= 0) qv.w = __ldg(row + dm.w);
-            }
-            if (r < mc) {
-              const float* row = X + (size_t)cid[r] * dpad;
-              if (dm.x >= 0) cv.x = __ldg(row + dm.x);
-              if (dm.y >= 0) cv.y = __ldg(row + dm.y);
-              if (dm.z >= 0) cv.z = __ldg(row + dm.z);
-              if (dm.w >= 0) cv.w = __ldg(row + dm.w);
-            }
-          } else {
-            const int dim = cd + 4 * c4;
-            if (r < mq && dim < dpad) qv = __ldg(reinterpret_cast<const float4*>(X + (size_t)qid[r] * dpad + dim));
-            if (r < mc && dim < dpad) cv = __ldg(reinterpret_cast<const float4*>(X + (size_t)cid[r] * dpad + dim));
-          }
-          Qs[4 * c4 + 0][r] = qv.x;
-          Qs[4 * c4 + 1][r] = qv.y;
-          Qs[4 * c4 + 2][r] = qv.z;
-          Qs[4 * c4 + 3][r] = qv.w;
-          Cs[4 * c4 + 0][r] = cv.x;
-          Cs[4 * c4 + 1][r] = cv.y;
-          Cs[4 * c4 + 2][r] = cv.z;
-          Cs[4 * c4 + 3][r] = cv.w;
-        }
-        __syncthreads();
-#pragma unroll 8
-        for (int dd = 0; dd < kDC; ++dd) {
-          float qa[R], cb[R];
-          load_r<R>(&Qs[dd][ty * R], qa);
-          load_r<R>(&Cs[dd][tx * R], cb);
-#pragma unroll
-          for (int a = 0; a < R; ++a)
-#pragma unroll
-            for (int b = 0; b < R; ++b) part[a][b] = acc_step<METRIC>(qa[a], cb[b], part[a][b]);
-        }
-        // end of a 256-dim group: its partial sum joins the total
-        const bool gend = ch == nchunks - 1 ||
-                          (dl ? (__ldg(dl + cd + kDC) >> 8) != (__ldg(dl + cd) >> 8) : ((cd + kDC) & 255) == 0);
-        if (gend) {
-#pragma unroll
-          for (int a = 0; a < R; ++a)
-#pragma unroll
-            for (int b = 0; b < R; ++b) {
-              total[a][b] = __fadd_rn(total[a][b], part[a][b]);
-              part[a][b] = 0.f;
-            }
-        }
-        __syncthreads();
-      }
-#pragma unroll
-      for (int a = 0; a < R; ++a)
-#pragma unroll
-        for (int b = 0; b < R; ++b) {
-          const int qq = ty * R + a, cc = tx * R + b;
-          float key = total[a][b];
-          if (METRIC == KNN_METRIC_COSINE) key = cosine_key(key, qnorm[qq], cnorm[cc]);
-          Ks[qq][cc] = (qq < mq && cc < mc) ? key : kInf;
-        }
+      tile_keys<METRIC, TILE>(X, dpad, dl, nchunks, mq, mc, qid, cid, qnorm, cnorm, Qs, Cs, Ks);
       __syncthreads();
-
-      // Merge every query row of the tile into its running list.
-      for (int qq = warp; qq < mq; qq += 8) {
-        const uint32_t i = (uint32_t)qid[qq];
-        WarpList<KPL> L;
-#pragma unroll
-        for (int r = 0; r < KPL; ++r) {
-          const int e = r * 32 + lane;
-          if (e < k) {
-            L.key[r] = rkey[(size_t)i * k + e];
-            L.id[r] = rid[(size_t)i * k + e];
-          } else {
-            L.key[r] = kInf;
-            L.id[r] = kNoId;
-          }
-        }
-        for (int cb = 0; cb < mc; cb += 32) {
-          const int c = cb + lane;
-          const bool inrange = c < mc;
-          const float ck = inrange ? Ks[qq][c] : kInf;
-          const uint32_t ci = inrange ? (uint32_t)cid[c] : kNoId;
-          float tk;
-          uint32_t ti;
-          warp_list_get(L, k - 1, tk, ti);
-          bool pass = inrange && ci != i && cand_less(ck, ci, tk, ti);
-          if (!__any_sync(0xFFFFFFFFu, pass)) continue;
-          const bool dup = warp_list_contains(L, ci, k);
-          pass = pass && !dup;
-          if (!__any_sync(0xFFFFFFFFu, pass)) continue;
-          warp_list_insert(L, pass ? ck : kInf, pass ? ci : kNoId);
-        }
-#pragma unroll
-        for (int r = 0; r < KPL; ++r) {
-          const int e = r * 32 + lane;
-          if (e < k) {
-            rkey[(size_t)i * k + e] = L.key[r];
-            rid[(size_t)i * k + e] = L.id[r];
-          }
-        }
-      }
+      merge_rows<KPL, TILE, false>(k, mq, mc, qid, cid, Ks, rkey, rid);
       __syncthreads();
     }
   }
 }
 
+// Tile pairs of a leaf that is its own block (queries = candidates): the key of
+// (q, c) equals the key of (c, q) bit for bit (the terms are |q-c|, (q-c)^2 or
+// q*c in the same dim order), so each unordered pair of a leaf's T tiles is
+// computed once and merged into both tiles' rows.  The pairs are scheduled in
+// rounds by the circle method over T' = T rounded up to even: in round r < T'-1
+// pair i is (r, T'-1) for i = 0, else ((r + i) mod (T'-1), (r - i) mod (T'-1));
+// the pairs of one round are disjoint, so each row's list is read and written
+// by one block per round.  Round T'-1 takes the diagonal tiles (t, t).  Pairs
+// with a tile past the leaf's own T are skipped.  One launch per round.
+template <int METRIC, int KPL, int TILE>
+__global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf_pair(
+    const float* __restrict__ X, int d, int dpad, SegView segs, int k, const int32_t* __restrict__ perm,
+    const float* __restrict__ norms, float* __restrict__ rkey, uint32_t* __restrict__ rid,
+    unsigned long long* __restrict__ pair_counter, const int32_t* __restrict__ dlist,
+    const int32_t* __restrict__ dnch, int lmax, int round, int tpr) {
+  static_assert(TILE == 32 || TILE == 64, "tile of 32 or 64");
+  __shared__ __align__(16) float Qs[kDC][TILE + 4];
+  __shared__ __align__(16) float Cs[kDC][TILE + 4];
+  __shared__ float Ks[TILE][TILE + 1];
+  __shared__ int32_t qid[TILE], cid[TILE];
+  __shared__ float qnorm[TILE], cnorm[TILE];
+
+  const int64_t leaf = blockIdx.x;
+  int64_t j, lo, hi, blo, bhi;
+  const SegEntry seg = segs.leaf(leaf, &j);
+  leaf_block(seg, j, k, &lo, &hi, &blo, &bhi);  // the host launches this only when blo = lo, bhi = hi
+  const int n = (int)(hi - lo);
+  const int T = (n + TILE - 1) / TILE;
+  int a, b;
+  if (round == tpr - 1) {
+    a = b = (int)blockIdx.y;
+  } else {
+    const int m = tpr - 1;
+    const int i = (int)blockIdx.y;
+    a = i == 0 ? round : (round + i) % m;
+    b = i == 0 ? m : (round - i + m) % m;
+  }
+  if (a >= T || b >= T) return;
+  const int tid = threadIdx.x;
+  const int32_t* dl = nullptr;
+  int nchunks = (d + kDC - 1) / kDC;
+  if (METRIC != KNN_METRIC_COSINE && dlist && dnch[leaf] >= 0) {
+    dl = dlist + leaf * lmax;
+    nchunks = dnch[leaf];
+  }
+  const int mq = min(TILE, n - a * TILE), mc = min(TILE, n - b * TILE);
+  if (pair_counter && tid == 0)
+    atomicAdd(pair_counter, a == b ? (unsigned long long)mq * (unsigned long long)(mq - 1)
+                                   : 2ull * (unsigned long long)mq * (unsigned long long)mc);
+  if (tid < TILE) {
+    const int32_t qi = tid < mq ? perm[lo + a * TILE + tid] : -1;
+    const int32_t ci = tid < mc ? perm[lo + b * TILE + tid] : -1;
+    qid[tid] = qi;
+    cid[tid] = ci;
+    if (METRIC == KNN_METRIC_COSINE) {
+      qnorm[tid] = qi >= 0 ? norms[qi] : 0.f;
+      cnorm[tid] = ci >= 0 ? norms[ci] : 0.f;
+    }
+  }
+  __syncthreads();
+  tile_keys<METRIC, TILE>(X, dpad, dl, nchunks, mq, mc, qid, cid, qnorm, cnorm, Qs, Cs, Ks);
+  __syncthreads();
+  merge_rows<KPL, TILE, false>(k, mq, mc, qid, cid, Ks, rkey, rid);
+  if (a != b) merge_rows<KPL, TILE, true>(k, mc, mq, cid, qid, Ks, rkey, rid);
+}
+
+// Rounds of the pair schedule for leaves of at most maxleaf points: T' = the
+// tiles of the largest leaf rounded up to even; 0 when the schedule does not
+// apply (a leaf of one tile, or more tiles than a grid dimension holds).
+template <int TILE>
+static int pair_tiles(int64_t maxleaf) {
+  const int64_t t = (maxleaf + TILE - 1) / TILE;
+  const int64_t tp = (t + 1) / 2 * 2;
+  return (t >= 2 && tp <= 65535) ? (int)tp : 0;
+}
+
 template <int METRIC, int TILE>
-static void launch_leaf_tile(const LeafArgs& a, const int32_t* perm, const int64_t* ftab, int64_t leaves, int kpl,
-                             const int32_t* dlist) {
-  if (leaves <= 0) return;
+static int launch_leaf_tile(const LeafArgs& a, const int32_t* perm, const int64_t* ftab, int64_t leaves, int kpl,
+                            const int32_t* dlist) {
+  if (leaves <= 0) return 0;
+  const int tpr = (a.pairs && !ftab) ? pair_tiles<TILE>(a.maxleaf) : 0;
+  if (tpr) {
+    for (int r = 0; r < tpr; ++r) {
+      const dim3 grid((unsigned)leaves, (unsigned)(r == tpr - 1 ? tpr : tpr / 2));
+      if (kpl == 1)
+        k_leaf_pair<METRIC, 1, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey,
+                                                                  a.rid, a.pair_counter, dlist, a.dnch, a.lmax, r, tpr);
+      else if (kpl == 2)
+        k_leaf_pair<METRIC, 2, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey,
+                                                                  a.rid, a.pair_counter, dlist, a.dnch, a.lmax, r, tpr);
+      else
+        k_leaf_pair<METRIC, 4, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey,
+                                                                  a.rid, a.pair_counter, dlist, a.dnch, a.lmax, r, tpr);
+    }
+    return tpr;
+  }
   const int64_t qtiles = (a.maxleaf + TILE - 1) / TILE;
   dim3 grid((unsigned)leaves, (unsigned)std::min<int64_t>(qtiles, 65535));
   if (kpl == 1)
@@ -319,6 +432,7 @@ static void launch_leaf_tile(const LeafArgs& a, const int32_t* perm, const int64
     k_leaf<METRIC, 2, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter, dlist, a.dnch, a.lmax);
   else
     k_leaf<METRIC, 4, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, ftab, a.k, perm, a.norms, a.rkey, a.rid, a.pair_counter, dlist, a.dnch, a.lmax);
+  return 1;
 }
 
 template <int METRIC>
@@ -338,8 +452,9 @@ static void launch_leaf_metric(const LeafArgs& a, int t, int kpl, LaunchLog& log
     log.add(3);
     dlist = a.dlist;
   }
-  if (a.tile == 32) launch_leaf_tile<METRIC, 32>(a, perm, ftab, leaves, kpl, dlist);
-  else launch_leaf_tile<METRIC, 64>(a, perm, ftab, leaves, kpl, dlist);
+  const int launches = a.tile == 32 ? launch_leaf_tile<METRIC, 32>(a, perm, ftab, leaves, kpl, dlist)
+                                    : launch_leaf_tile<METRIC, 64>(a, perm, ftab, leaves, kpl, dlist);
+  log.add(launches);
 }
 
 // One launch per tree: a point sits in one leaf per tree, so the leaves of a
@@ -352,7 +467,6 @@ int leaf_stage(const LeafArgs& a, LaunchLog& log) {
     else if (a.metric == KNN_METRIC_TAXICAB) launch_leaf_metric<KNN_METRIC_TAXICAB>(a, t, kpl, log);
     else launch_leaf_metric<KNN_METRIC_COSINE>(a, t, kpl, log);
     if (a.kev) cudaEventRecord(a.kev[2 * (t - a.first_tree) + 1], a.stream);
-    log.add();
   }
   return cudaPeekAtLastError() == cudaSuccess ? KNN_OK : KNN_ERR_CUDA;
 }

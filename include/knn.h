@@ -111,7 +111,10 @@ typedef struct knn_options {
                                 rows (the left-out terms are exact zeros, so the keys
                                 keep their bits); -1 never; 0 when leaves hold at
                                 least 1024 points                                     */
-  int32_t reserved[1];
+  int32_t tile_pairs;        /* FP32 leaf tiles where every leaf is its own block: each
+                                key is computed once for both of its points (keys are
+                                symmetric bit for bit, so the graph is the same); -1 off,
+                                else on                                               */
 } knn_options;
 
 typedef struct knn_stats {
@@ -138,7 +141,9 @@ typedef struct knn_stats {
   int32_t tc_group;          /* sibling leaves per tensor-core tile used (0: FP32 path) */
   int32_t sparse_dims;       /* 1: the FP32 leaf tiles read each block's non-zero dims
                                 (knn_build_ex; 0 from knn_build_batch)               */
-  int64_t reserved[4];
+  int32_t tile_pairs;        /* 1: the FP32 leaf tiles ran as tile pairs (knn_build_ex) */
+  int32_t reserved32;
+  int64_t reserved[3];
 } knn_stats;
 
 typedef struct knn_context knn_context;
