@@ -721,7 +721,7 @@ def run_batch(args):
 CONFIG_TARGETS = {
     "sparse_prototypes": {"plain_fp32": (4, 131072, 1)},
     "normalized_mixture": {"plain_fp32": (24, 2048, 0), "mixed_f16": (16, 4096, 0),
-                           "mixed_f16_learned": (16, 4096, 0)},
+                           "mixed_f16_learned": (16, 4096, 1)},
 }
 PATH_OPTIONS = {
     "plain_fp32": dict(precision=0),
