@@ -471,6 +471,15 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
     int rc = C->get("dmask", (size_t)lay.leaves * (dpad / 32 + 1), &a.dmask);
     if (!rc) rc = C->get("dlist", (size_t)lay.leaves * a.lmax, &a.dlist);
     if (!rc) rc = C->get("dnch", (size_t)lay.leaves, &a.dnch);
+    if (!rc && a.pairs && dpad <= 4096) {
+      // tile pairs read the union of their two tiles' dims: the leaf stage
+      // reorders positions within each leaf of the trees' order (context
+      // scratch) by row bucket, which leaves every leaf's point set as it is
+      a.perm_w = const_cast<int32_t*>(perm);
+      rc = C->get("rbucket", (size_t)n, &a.bucket);
+      if (!rc) rc = C->get("sort_tmp", (size_t)n, &a.sort_tmp);
+      if (!rc) rc = C->get("tmask", (size_t)lay.leaves * ((lay.maxleaf + 31) / 32) * ((dpad + 31) / 32), &a.tmask);
+    }
     if (rc) return rc;
   }
   int rc = knn::leaf_stage(a, log);

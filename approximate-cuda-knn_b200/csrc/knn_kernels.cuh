@@ -118,6 +118,12 @@ struct LeafArgs {
   // every leaf is its own block (at least k+1 points, median trees): each tile
   // pair of a leaf is computed once and merged into both sides (k_leaf_pair)
   bool pairs;
+  // sparse rows with tile pairs: positions within each leaf reordered by row
+  // bucket (perm_w: writable alias of perm), per-tile dim masks
+  int32_t* perm_w;       // [trees][n] or null
+  uint8_t* bucket;       // [n]
+  int32_t* sort_tmp;     // [n]
+  uint32_t* tmask;       // [leaves][ceil(maxleaf / tile)][ceil(dpad / 32)]
   cudaStream_t stream;
 };
 int leaf_stage(const LeafArgs& a, LaunchLog& log);

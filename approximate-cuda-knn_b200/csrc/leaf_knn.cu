@@ -77,6 +77,42 @@ __global__ void __launch_bounds__(256) k_leaf_dim_mask(const float* __restrict__
   }
 }
 
+// The dims set in mask words word(0..W) into out, one warp: every 256-dim group's
+// dims in increasing order (lane l holds dims 256 g + 8 l .. + 7 of group g),
+// padded with -1 to a multiple of 32 entries.  Returns the chunks of 32, or -1
+// when the list saves no chunk over the ceil(d / 32) chunks of all dims.
+template <typename LT, typename MaskFn>
+__device__ __forceinline__ int warp_dim_list(MaskFn word, int W, int d, int dpad, LT* out) {
+  const int lane = threadIdx.x & 31;
+  int pos = 0;
+  for (int g = 0; g * 256 < dpad; ++g) {
+    const int w = 8 * g + (lane >> 2);
+    const uint32_t bits = w < W ? (word(w) >> (8 * (lane & 3))) & 0xFFu : 0u;
+    const int c = __popc(bits);
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    int at = pos + incl - c;
+    for (uint32_t b = bits; b; b &= b - 1) out[at++] = (LT)(256 * g + 8 * lane + (__ffs(b) - 1));
+    const int padded = (total + 31) & ~31;
+    for (int e = total + lane; e < padded; e += 32) out[pos + e] = (LT)-1;
+    pos += padded;
+  }
+  return pos / 32 < (d + 31) / 32 ? pos / 32 : -1;
+}
+
+__device__ __forceinline__ int4 load_dims4(const int32_t* p) { return __ldg(reinterpret_cast<const int4*>(p)); }
+__device__ __forceinline__ int4 load_dims4(const int16_t* p) {
+  const short4 v = *reinterpret_cast<const short4*>(p);
+  return make_int4(v.x, v.y, v.z, v.w);
+}
+__device__ __forceinline__ int load_dim(const int32_t* p) { return __ldg(p); }
+__device__ __forceinline__ int load_dim(const int16_t* p) { return *p; }
+
 // One warp per leaf: the listed dims of every 256-dim group in increasing order,
 // each group padded with -1 to a multiple of 32 entries; dnch[leaf] = chunks of
 // 32, or -1 when the list saves no chunk over the ceil(d / 32) chunks of all dims
@@ -88,28 +124,120 @@ __global__ void __launch_bounds__(256) k_leaf_dim_list(const uint32_t* __restric
   const int lane = threadIdx.x & 31;
   if (leaf >= leaves) return;
   const uint32_t* m = mask + leaf * W;
-  int32_t* out = dlist + leaf * lmax;
-  int pos = 0;
-  for (int g = 0; g * 256 < dpad; ++g) {
-    // lane l holds dims 256 g + 8 l .. + 7
-    const int w = 8 * g + (lane >> 2);
-    const uint32_t bits = w < W ? (m[w] >> (8 * (lane & 3))) & 0xFFu : 0u;
-    const int c = __popc(bits);
-    int incl = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if (lane >= o) incl += v;
-    }
-    const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-    int at = pos + incl - c;
-    for (uint32_t b = bits; b; b &= b - 1) out[at++] = 256 * g + 8 * lane + (__ffs(b) - 1);
-    const int padded = (total + 31) & ~31;
-    for (int e = total + lane; e < padded; e += 32) out[pos + e] = -1;
-    pos += padded;
-  }
-  if (lane == 0) dnch[leaf] = pos / 32 < (d + 31) / 32 ? pos / 32 : -1;
+  const int nch = warp_dim_list<int32_t>([&](int w) { return m[w]; }, W, d, dpad, dlist + leaf * lmax);
+  if (lane == 0) dnch[leaf] = nch;
 }
+
+// Tiles of rows with one zero pattern read fewer dims than tiles that mix
+// patterns, and a leaf's graph does not depend on the order of its positions.
+// So, with tile pairs, each tree's leaves are ordered by a bucket of the rows'
+// non-zero patterns and each tile pair reads the union of its two tiles' dims.
+constexpr int kBucketBits = 6;
+constexpr int kMaxListDims = 4096;  // padded dims of a tile pair's list in shared memory
+
+// bucket[row]: the top 6 bits of a hash of the row's non-zero pattern (one
+// ballot word per 32 dims).  One warp per row.
+__global__ void __launch_bounds__(256) k_row_bucket(const float* __restrict__ X, int64_t n, int dpad,
+                                                    uint8_t* __restrict__ bucket) {
+  const int64_t row = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const float* x = X + (size_t)row * dpad;
+  uint64_t h = 0x9E3779B97F4A7C15ull;
+  for (int d0 = 0; d0 < dpad; d0 += 32) {
+    const bool nz = d0 + lane < dpad && x[d0 + lane] != 0.f;
+    const uint32_t w = __ballot_sync(0xFFFFFFFFu, nz);
+    h = (h ^ w) * 0x100000001B3ull;
+    h ^= h >> 29;
+  }
+  if (lane == 0) bucket[row] = (uint8_t)(h >> (64 - kBucketBits));
+}
+
+// Each leaf's positions stably ordered by bucket.  One block of 1024 threads
+// per leaf; warp w takes the w-th of 32 equal ranges of the leaf's positions,
+// counts them per bucket, and scatters them in order after the prefix over
+// (bucket, warp); tmp holds the new order until it is copied back.
+__global__ void __launch_bounds__(1024) k_leaf_bucket_sort(int32_t* __restrict__ perm, SegView segs, int k,
+                                                           const uint8_t* __restrict__ bucket,
+                                                           int32_t* __restrict__ tmp) {
+  constexpr int NB = 1 << kBucketBits;
+  __shared__ int cnt[32][NB];
+  __shared__ int tot[NB];
+  const int64_t leaf = blockIdx.x;
+  int64_t j, lo, hi, blo, bhi;
+  const SegEntry seg = segs.leaf(leaf, &j);
+  leaf_block(seg, j, k, &lo, &hi, &blo, &bhi);
+  const int n = (int)(hi - lo);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int per = (n + 31) / 32;
+  const int r0 = min(n, warp * per), r1 = min(n, r0 + per);
+  for (int e = threadIdx.x; e < 32 * NB; e += 1024) (&cnt[0][0])[e] = 0;
+  __syncthreads();
+  for (int r = r0 + lane; r < r1; r += 32) atomicAdd(&cnt[warp][bucket[perm[lo + r]]], 1);
+  __syncthreads();
+  if (threadIdx.x < NB) {
+    int t = 0;
+    for (int w = 0; w < 32; ++w) t += cnt[w][threadIdx.x];
+    tot[threadIdx.x] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int b = 0; b < NB; ++b) {
+      const int t = tot[b];
+      tot[b] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < NB) {
+    int run = tot[threadIdx.x];
+    for (int w = 0; w < 32; ++w) {
+      const int c = cnt[w][threadIdx.x];
+      cnt[w][threadIdx.x] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+  for (int c0 = r0; c0 < r1; c0 += 32) {
+    const int r = c0 + lane;
+    const bool valid = r < r1;
+    const int32_t id = valid ? perm[lo + r] : -1;
+    const int b = valid ? (int)bucket[id] : NB;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    if (valid) tmp[lo + cnt[warp][b] + rank] = id;
+    __syncwarp();
+    if (valid && rank == 0) cnt[warp][b] += __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < n; r += 1024) perm[lo + r] = tmp[lo + r];
+}
+
+// tmask[leaf][t][w]: the dims non-zero in some row of the leaf's tile t (TILE
+// positions), W = ceil(dpad / 32) words, every word written.  grid (leaf, tile).
+__global__ void __launch_bounds__(256) k_tile_dim_mask(const float* __restrict__ X, int dpad, SegView segs, int k,
+                                                       const int32_t* __restrict__ perm, int tile, int tpl,
+                                                       uint32_t* __restrict__ tmask, int W) {
+  const int64_t leaf = blockIdx.x;
+  int64_t j, lo, hi, blo, bhi;
+  const SegEntry seg = segs.leaf(leaf, &j);
+  leaf_block(seg, j, k, &lo, &hi, &blo, &bhi);
+  const int64_t r0 = lo + (int64_t)blockIdx.y * tile;
+  if (r0 >= hi) return;
+  const int64_t r1 = min(hi, r0 + tile);
+  uint32_t* out = tmask + ((size_t)leaf * tpl + blockIdx.y) * W;
+  for (int dim0 = 0; dim0 < dpad; dim0 += 256) {
+    const int dim = dim0 + (int)threadIdx.x;
+    bool nz = false;
+    if (dim < dpad)
+      for (int64_t r = r0; r < r1 && !nz; ++r) nz = __ldg(X + (size_t)__ldg(perm + r) * dpad + dim) != 0.f;
+    const uint32_t bits = __ballot_sync(0xFFFFFFFFu, nz);
+    if ((threadIdx.x & 31) == 0 && dim < dpad) out[dim >> 5] = bits;
+  }
+}
+
 
 // Keys of one TILE x TILE tile: rows qid[0..mq) against columns cid[0..mc)
 // (ids; -1 past the end), 16 x 16 threads each holding an R x R register
@@ -117,8 +245,8 @@ __global__ void __launch_bounds__(256) k_leaf_dim_list(const uint32_t* __restric
 // (all dims, or the listed non-zero dims dl of a sparse block) in the
 // reference's order: a sequential partial per 256-dim group, added to the
 // total at the group's end.  Ks receives the keys, +inf outside mq x mc.
-template <int METRIC, int TILE>
-__device__ __forceinline__ void tile_keys(const float* __restrict__ X, int dpad, const int32_t* __restrict__ dl,
+template <int METRIC, int TILE, typename LT>
+__device__ __forceinline__ void tile_keys(const float* __restrict__ X, int dpad, const LT* __restrict__ dl,
                                           int nchunks, int mq, int mc, const int32_t* qid, const int32_t* cid,
                                           const float* qnorm, const float* cnorm, float (*Qs)[TILE + 4],
                                           float (*Cs)[TILE + 4], float (*Ks)[TILE + 1]) {
@@ -140,7 +268,7 @@ __device__ __forceinline__ void tile_keys(const float* __restrict__ X, int dpad,
       const int r = f >> 3, c4 = f & 7;
       float4 qv = make_float4(0.f, 0.f, 0.f, 0.f), cv = qv;
       if (dl) {  // four listed dims (-1: padding, read as zero)
-        const int4 dm = __ldg(reinterpret_cast<const int4*>(dl + cd + 4 * c4));
+        const int4 dm = load_dims4(dl + cd + 4 * c4);
         if (r < mq) {
           const float* row = X + (size_t)qid[r] * dpad;
           if (dm.x >= 0) qv.x = __ldg(row + dm.x);
@@ -182,7 +310,7 @@ __device__ __forceinline__ void tile_keys(const float* __restrict__ X, int dpad,
     }
     // end of a 256-dim group: its partial sum joins the total
     const bool gend = ch == nchunks - 1 ||
-                      (dl ? (__ldg(dl + cd + kDC) >> 8) != (__ldg(dl + cd) >> 8) : ((cd + kDC) & 255) == 0);
+                      (dl ? (load_dim(dl + cd + kDC) >> 8) != (load_dim(dl + cd) >> 8) : ((cd + kDC) & 255) == 0);
     if (gend) {
 #pragma unroll
       for (int a = 0; a < R; ++a)
@@ -320,7 +448,7 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* _
         if (METRIC == KNN_METRIC_COSINE) cnorm[tid] = id >= 0 ? norms[id] : 0.f;
       }
       __syncthreads();
-      tile_keys<METRIC, TILE>(X, dpad, dl, nchunks, mq, mc, qid, cid, qnorm, cnorm, Qs, Cs, Ks);
+      tile_keys<METRIC, TILE, int32_t>(X, dpad, dl, nchunks, mq, mc, qid, cid, qnorm, cnorm, Qs, Cs, Ks);
       __syncthreads();
       merge_rows<KPL, TILE, false>(k, mq, mc, qid, cid, Ks, rkey, rid);
       __syncthreads();
@@ -337,18 +465,24 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* _
 // the pairs of one round are disjoint, so each row's list is read and written
 // by one block per round.  Round T'-1 takes the diagonal tiles (t, t).  Pairs
 // with a tile past the leaf's own T are skipped.  One launch per round.
+// Sparse rows: with tmask (per-tile dim masks, W words each, tpl tiles per
+// leaf) a block reads the union of its two tiles' non-zero dims, listed in
+// shared memory; else with dlist the leaf block's list.
 template <int METRIC, int KPL, int TILE>
 __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf_pair(
     const float* __restrict__ X, int d, int dpad, SegView segs, int k, const int32_t* __restrict__ perm,
     const float* __restrict__ norms, float* __restrict__ rkey, uint32_t* __restrict__ rid,
     unsigned long long* __restrict__ pair_counter, const int32_t* __restrict__ dlist,
-    const int32_t* __restrict__ dnch, int lmax, int round, int tpr) {
+    const int32_t* __restrict__ dnch, int lmax, const uint32_t* __restrict__ tmask, int tpl, int W, int round,
+    int tpr) {
   static_assert(TILE == 32 || TILE == 64, "tile of 32 or 64");
   __shared__ __align__(16) float Qs[kDC][TILE + 4];
   __shared__ __align__(16) float Cs[kDC][TILE + 4];
   __shared__ float Ks[TILE][TILE + 1];
   __shared__ int32_t qid[TILE], cid[TILE];
   __shared__ float qnorm[TILE], cnorm[TILE];
+  __shared__ __align__(16) int16_t sl[METRIC == KNN_METRIC_COSINE ? 4 : kMaxListDims];
+  __shared__ int snch;
 
   const int64_t leaf = blockIdx.x;
   int64_t j, lo, hi, blo, bhi;
@@ -369,10 +503,21 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf_pair(
   const int tid = threadIdx.x;
   const int32_t* dl = nullptr;
   int nchunks = (d + kDC - 1) / kDC;
-  if (METRIC != KNN_METRIC_COSINE && dlist && dnch[leaf] >= 0) {
+  if (METRIC != KNN_METRIC_COSINE && dlist && !tmask && dnch[leaf] >= 0) {
     dl = dlist + leaf * lmax;
     nchunks = dnch[leaf];
   }
+  if (METRIC != KNN_METRIC_COSINE && tmask) {  // block-uniform
+    if (tid < 32) {
+      const uint32_t* ma = tmask + ((size_t)leaf * tpl + a) * W;
+      const uint32_t* mb = tmask + ((size_t)leaf * tpl + b) * W;
+      const int nch = warp_dim_list<int16_t>([&](int w) { return __ldg(ma + w) | __ldg(mb + w); }, W, d, dpad, sl);
+      if (tid == 0) snch = nch;
+    }
+    __syncthreads();
+    if (snch >= 0) nchunks = snch;
+  }
+  const int16_t* sdl = (METRIC != KNN_METRIC_COSINE && tmask && snch >= 0) ? sl : nullptr;
   const int mq = min(TILE, n - a * TILE), mc = min(TILE, n - b * TILE);
   if (pair_counter && tid == 0)
     atomicAdd(pair_counter, a == b ? (unsigned long long)mq * (unsigned long long)(mq - 1)
@@ -388,7 +533,8 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf_pair(
     }
   }
   __syncthreads();
-  tile_keys<METRIC, TILE>(X, dpad, dl, nchunks, mq, mc, qid, cid, qnorm, cnorm, Qs, Cs, Ks);
+  if (sdl) tile_keys<METRIC, TILE, int16_t>(X, dpad, sdl, nchunks, mq, mc, qid, cid, qnorm, cnorm, Qs, Cs, Ks);
+  else tile_keys<METRIC, TILE, int32_t>(X, dpad, dl, nchunks, mq, mc, qid, cid, qnorm, cnorm, Qs, Cs, Ks);
   __syncthreads();
   merge_rows<KPL, TILE, false>(k, mq, mc, qid, cid, Ks, rkey, rid);
   if (a != b) merge_rows<KPL, TILE, true>(k, mc, mq, cid, qid, Ks, rkey, rid);
@@ -404,25 +550,47 @@ static int pair_tiles(int64_t maxleaf) {
   return (t >= 2 && tp <= 65535) ? (int)tp : 0;
 }
 
+// Sparse tile pairs: each leaf's positions ordered by row bucket, then the
+// dim masks of its tiles (two launches before the rounds).
+template <int TILE>
+static int sparse_tile_masks(const LeafArgs& a, int32_t* perm, int64_t leaves, int tpl, int W) {
+  k_leaf_bucket_sort<<<(unsigned)leaves, 1024, 0, a.stream>>>(perm, a.segs, a.k, a.bucket, a.sort_tmp);
+  k_tile_dim_mask<<<dim3((unsigned)leaves, (unsigned)tpl), 256, 0, a.stream>>>(a.X, a.dpad, a.segs, a.k, perm, TILE,
+                                                                               tpl, a.tmask, W);
+  return 2;
+}
+
 template <int METRIC, int TILE>
 static int launch_leaf_tile(const LeafArgs& a, const int32_t* perm, const int64_t* ftab, int64_t leaves, int kpl,
-                            const int32_t* dlist) {
+                            const int32_t* dlist, int32_t* perm_w) {
   if (leaves <= 0) return 0;
   const int tpr = (a.pairs && !ftab) ? pair_tiles<TILE>(a.maxleaf) : 0;
   if (tpr) {
+    const int tpl = (int)((a.maxleaf + TILE - 1) / TILE);
+    const int W = (a.dpad + 31) / 32;
+    int extra = 0;
+    const uint32_t* tmask = nullptr;
+    if (METRIC != KNN_METRIC_COSINE && a.tmask && perm_w && a.dpad <= kMaxListDims) {
+      extra = sparse_tile_masks<TILE>(a, perm_w, leaves, tpl, W);
+      tmask = a.tmask;
+      dlist = nullptr;
+    }
     for (int r = 0; r < tpr; ++r) {
       const dim3 grid((unsigned)leaves, (unsigned)(r == tpr - 1 ? tpr : tpr / 2));
       if (kpl == 1)
         k_leaf_pair<METRIC, 1, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey,
-                                                                  a.rid, a.pair_counter, dlist, a.dnch, a.lmax, r, tpr);
+                                                                  a.rid, a.pair_counter, dlist, a.dnch, a.lmax, tmask,
+                                                                  tpl, W, r, tpr);
       else if (kpl == 2)
         k_leaf_pair<METRIC, 2, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey,
-                                                                  a.rid, a.pair_counter, dlist, a.dnch, a.lmax, r, tpr);
+                                                                  a.rid, a.pair_counter, dlist, a.dnch, a.lmax, tmask,
+                                                                  tpl, W, r, tpr);
       else
         k_leaf_pair<METRIC, 4, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey,
-                                                                  a.rid, a.pair_counter, dlist, a.dnch, a.lmax, r, tpr);
+                                                                  a.rid, a.pair_counter, dlist, a.dnch, a.lmax, tmask,
+                                                                  tpl, W, r, tpr);
     }
-    return tpr;
+    return tpr + extra;
   }
   const int64_t qtiles = (a.maxleaf + TILE - 1) / TILE;
   dim3 grid((unsigned)leaves, (unsigned)std::min<int64_t>(qtiles, 65535));
@@ -441,7 +609,8 @@ static void launch_leaf_metric(const LeafArgs& a, int t, int kpl, LaunchLog& log
   const int64_t* ftab = a.ftable ? a.ftable + 4 * a.foff[t] : nullptr;
   const int64_t leaves = a.ftable ? a.fcount[t] : a.leaves;
   const int32_t* dlist = nullptr;
-  if (a.dlist && !ftab && METRIC != KNN_METRIC_COSINE && leaves > 0) {
+  int32_t* perm_w = a.perm_w ? a.perm_w + (size_t)t * a.n : nullptr;
+  if (a.dlist && !a.tmask && !ftab && METRIC != KNN_METRIC_COSINE && leaves > 0) {
     const int W = a.dpad / 32 + 1;
     cudaMemsetAsync(a.dmask, 0, sizeof(uint32_t) * (size_t)leaves * W, a.stream);
     const int64_t splits = (std::max(a.maxblock, a.maxleaf) + kDimRows - 1) / kDimRows;
@@ -452,8 +621,8 @@ static void launch_leaf_metric(const LeafArgs& a, int t, int kpl, LaunchLog& log
     log.add(3);
     dlist = a.dlist;
   }
-  const int launches = a.tile == 32 ? launch_leaf_tile<METRIC, 32>(a, perm, ftab, leaves, kpl, dlist)
-                                    : launch_leaf_tile<METRIC, 64>(a, perm, ftab, leaves, kpl, dlist);
+  const int launches = a.tile == 32 ? launch_leaf_tile<METRIC, 32>(a, perm, ftab, leaves, kpl, dlist, perm_w)
+                                    : launch_leaf_tile<METRIC, 64>(a, perm, ftab, leaves, kpl, dlist, perm_w);
   log.add(launches);
 }
 
@@ -461,6 +630,10 @@ static void launch_leaf_metric(const LeafArgs& a, int t, int kpl, LaunchLog& log
 // tree update disjoint lists, and stream order serialises the trees.
 int leaf_stage(const LeafArgs& a, LaunchLog& log) {
   const int kpl = kpl_for(a.k);
+  if (a.tmask && a.bucket && a.n > 0) {
+    k_row_bucket<<<(unsigned)((a.n + 7) / 8), 256, 0, a.stream>>>(a.X, a.n, a.dpad, a.bucket);
+    log.add();
+  }
   for (int t = a.first_tree; t < a.first_tree + a.trees; ++t) {
     if (a.kev) cudaEventRecord(a.kev[2 * (t - a.first_tree)], a.stream);
     if (a.metric == KNN_METRIC_EUCLIDEAN) launch_leaf_metric<KNN_METRIC_EUCLIDEAN>(a, t, kpl, log);

@@ -52,13 +52,19 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("pairs", [0, -1], ids=["tile_pairs", "one_sided"])
 @pytest.mark.parametrize("metric", [0, 1])
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
-def test_sparse_tiles_bit_identical(lib, oracle, case, metric):
+def test_sparse_tiles_bit_identical(lib, oracle, case, metric, pairs):
+    """With tile pairs each pair reads the union of its two tiles' dims (each
+    leaf's positions ordered by row pattern first); one-sided tiles read the
+    leaf block's dims."""
     name, n, d, k, trees, leaf, props, kw = case
     x = _prototypes(n, d, seed=len(name) * 31 + d, **kw)
-    *on, st_on = lib.knn_build(x, k, trees, leaf, props, metric, seed=3, sparse_dims=1, stats=True)
-    *off, st_off = lib.knn_build(x, k, trees, leaf, props, metric, seed=3, sparse_dims=-1, stats=True)
+    *on, st_on = lib.knn_build(x, k, trees, leaf, props, metric, seed=3, sparse_dims=1, tile_pairs=pairs,
+                               stats=True)
+    *off, st_off = lib.knn_build(x, k, trees, leaf, props, metric, seed=3, sparse_dims=-1, tile_pairs=pairs,
+                                 stats=True)
     assert st_on["sparse_dims"] == 1 and st_off["sparse_dims"] == 0
     _same(on, off, f"{name}/metric{metric}: sparse vs all dims")
     _same(on, oracle.knn_build(x, k, trees, leaf, props, metric, seed=3), f"{name}/metric{metric}: vs oracle")
