@@ -132,10 +132,10 @@ __global__ void __launch_bounds__(256) k_leaf_dim_list(const uint32_t* __restric
 // patterns, and a leaf's graph does not depend on the order of its positions.
 // So, with tile pairs, each tree's leaves are ordered by a bucket of the rows'
 // non-zero patterns and each tile pair reads the union of its two tiles' dims.
-constexpr int kBucketBits = 6;
+constexpr int kBucketBits = 8;
 constexpr int kMaxListDims = 4096;  // padded dims of a tile pair's list in shared memory
 
-// bucket[row]: the top 6 bits of a hash of the row's non-zero pattern (one
+// bucket[row]: the top 8 bits of a hash of the row's non-zero pattern (one
 // ballot word per 32 dims).  One warp per row.
 __global__ void __launch_bounds__(256) k_row_bucket(const float* __restrict__ X, int64_t n, int dpad,
                                                     uint8_t* __restrict__ bucket) {
