@@ -12,6 +12,11 @@
 // shuffles).  Taking the k best of every tree in turn and dropping ids already
 // listed gives the k best of the union, so no bitmap is needed.
 //
+// Two result-neutral shortcuts: where every leaf is its own block, each tile
+// pair of a leaf is computed once and merged into both sides (k_leaf_pair; the
+// keys are symmetric bit for bit), and on sparse rows a tile reads only the dims
+// that are non-zero in some of its rows (the left-out terms are exact zeros).
+//
 // The block of a leaf is its smallest ancestor holding at least k+1 points
 // (the climb of .cu:87-105); all points of a leaf share it.
 #include "knn_internal.cuh"
