@@ -68,20 +68,27 @@ int prop_hash_bits(int k) {
   return b;
 }
 
-// hash set | candidates [k*k] | N(i) ids and flags | query row (float, d
-// rounded to 8) | the row-slice buffer (32 rows, padded pitch)
-size_t prop_warp_bytes(int k, int d) {
-  size_t b = ((size_t)4 << prop_hash_bits(k)) + (size_t)4 * round_up(k * k, 32) + (size_t)8 * round_up(k, 32) +
+// hash set (with two buffers: also the second row-slice buffer, since the
+// hash is done with before the first row is staged) | candidates [k*k] | N(i)
+// ids and flags | query row (float, d rounded to 8) | the row-slice buffer
+// (32 rows, padded pitch)
+size_t prop_region0_bytes(int k, int nbuf) {
+  const size_t h = (size_t)4 << prop_hash_bits(k);
+  return nbuf == 2 ? std::max(h, (size_t)32 * kRowStride) : h;
+}
+size_t prop_warp_bytes(int k, int d, int nbuf) {
+  size_t b = prop_region0_bytes(k, nbuf) + (size_t)4 * round_up(k * k, 32) + (size_t)8 * round_up(k, 32) +
              (size_t)4 * round_up(d, 8) + (size_t)32 * kRowStride;
   return (b + 15) & ~(size_t)15;
 }
 
 // HALF: rows are FP16 [n][ldr] (ldr % 8 == 0), else float32 [n][ldr] (ldr % 4 == 0);
-// zero padded beyond d.
-template <int METRIC, int KPL, bool HALF>
+// zero padded beyond d.  NBUF 2: the next stage's row slices load while the
+// current stage is summed (used where the second buffer costs no warps per SM).
+template <int METRIC, int KPL, bool HALF, int NBUF>
 __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
     const void* __restrict__ Xrows, int ldr, int64_t n, int64_t r0, int64_t cnt, int d, int k, int kw, int hbits,
-    size_t warp_bytes, const float* __restrict__ norms, const int32_t* __restrict__ order,
+    size_t warp_bytes, size_t region0, const float* __restrict__ norms, const int32_t* __restrict__ order,
     const float* __restrict__ key_in, const uint32_t* __restrict__ id_in,
     const uint32_t* __restrict__ flags_in, float* __restrict__ key_out,
     uint32_t* __restrict__ id_out, uint32_t* __restrict__ flags_out,
@@ -98,11 +105,12 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
   const int kr = (k + 31) & ~31;
   const int dq = (d + 7) & ~7;
   int32_t* H = reinterpret_cast<int32_t*>(base);
-  uint32_t* Q = reinterpret_cast<uint32_t*>(base + (size_t)4 * hsize);
+  uint32_t* Q = reinterpret_cast<uint32_t*>(base + region0);
   uint32_t* nbid = Q + ((kk + 31) & ~31);
   uint32_t* nbfl = nbid + kr;
   float* xq = reinterpret_cast<float*>(nbfl + kr);
-  unsigned char* rows = reinterpret_cast<unsigned char*>(xq + dq);  // [32][kRowStride]
+  unsigned char* rows1 = reinterpret_cast<unsigned char*>(xq + dq);  // [32][kRowStride]
+  unsigned char* rows0 = NBUF == 2 ? base : rows1;                    // over the hash set
   const float kInf = __int_as_float(0x7F800000);
   const uint32_t lt_mask = (1u << lane) - 1u;
   const int nch = (d + kCH - 1) / kCH;
@@ -186,22 +194,38 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
     // 8-lane phase and the unit offsets are compile-time constants
     const int stages = ((qn + 31) >> 5) * nch;
     const int half = lane >> 4, c16 = lane & 15;
+    // stage t: rows 32 b .. of the candidates, dims c * kCH .. of each, into buffer t mod NBUF
+    auto stage_rows = [&](int t) {
+      const int b = t / nch, c = t - b * nch;
+      const int m = min(32, qn - 32 * b);
+      const int dim = c * kCH + kEPU * c16;
+      const bool ok = dim < ldr;
+      unsigned char* buf = (NBUF == 2 && (t & 1)) ? rows1 : rows0;
+      for (int r = half; r < m; r += 2) {
+        const uint32_t jid = Q[32 * b + r];
+        cp_async16(buf + r * kRowStride + c16 * 16, X + (size_t)jid * ldr + (ok ? dim : 0), ok ? 16 : 0);
+      }
+      cp_async_commit();
+    };
     float total = 0.f, part = 0.f;
+    if (NBUF == 2 && stages > 0) stage_rows(0);
     for (int t = 0; t < stages; ++t) {
       const int b = t / nch, c = t - b * nch;
       const int m = min(32, qn - 32 * b);
       const int cd = c * kCH;
-      {
-        const int dim = cd + kEPU * c16;
-        const bool ok = dim < ldr;
-        for (int r = half; r < m; r += 2) {
-          const uint32_t jid = Q[32 * b + r];
-          cp_async16(rows + r * kRowStride + c16 * 16, X + (size_t)jid * ldr + (ok ? dim : 0), ok ? 16 : 0);
+      if (NBUF == 2) {
+        if (t + 1 < stages) {
+          stage_rows(t + 1);  // its buffer was last read in stage t - 1, before that stage's closing syncwarp
+          cp_async_wait<1>();
+        } else {
+          cp_async_wait<0>();
         }
-        cp_async_commit();
+      } else {
+        stage_rows(t);
         cp_async_wait<0>();
       }
       __syncwarp();
+      const unsigned char* rows = (NBUF == 2 && (t & 1)) ? rows1 : rows0;
       if (lane < m) {
         const unsigned char* myrow = rows + lane * kRowStride;
         const int nu = (min(kCH, d - cd) + kEPU - 1) / kEPU;  // 16-byte units holding dims
@@ -265,20 +289,21 @@ __global__ void __launch_bounds__(kPropMaxWarps * 32) k_propagate(
   if (cand_counter && lane == 0 && evaluated) atomicAdd(cand_counter, evaluated);
 }
 
-template <int METRIC, bool HALF>
+template <int METRIC, bool HALF, int NBUF>
 static void launch_prop_metric(const PropArgs& a, int kpl, int hbits, size_t wb, int wpb, unsigned grid) {
   const int kw = (a.k + 31) / 32;
   const int64_t r0 = a.r0, cnt = (a.r1 > 0 ? a.r1 : a.n) - a.r0;
   const size_t smem = wb * wpb;
   const void* rows = HALF ? static_cast<const void*>(a.Xh) : static_cast<const void*>(a.X);
   const int ldr = HALF ? a.ldh : a.dpad;
-#define KNN_PROP_LAUNCH(KP)                                                                         \
-  do {                                                                                              \
-    cudaFuncSetAttribute(k_propagate<METRIC, KP, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                         (int)kPropSmemBudget);                                                     \
-    k_propagate<METRIC, KP, HALF><<<grid, wpb * 32, smem, a.stream>>>(                              \
-        rows, ldr, a.n, r0, cnt, a.d, a.k, kw, hbits, wb, a.norms, a.order, a.key_in, a.id_in,      \
-        a.flags_in, a.key_out, a.id_out, a.flags_out, a.cand_counter);                              \
+  const size_t region0 = prop_region0_bytes(a.k, NBUF);
+#define KNN_PROP_LAUNCH(KP)                                                                                \
+  do {                                                                                                     \
+    cudaFuncSetAttribute(k_propagate<METRIC, KP, HALF, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                         (int)kPropSmemBudget);                                                            \
+    k_propagate<METRIC, KP, HALF, NBUF><<<grid, wpb * 32, smem, a.stream>>>(                               \
+        rows, ldr, a.n, r0, cnt, a.d, a.k, kw, hbits, wb, region0, a.norms, a.order, a.key_in, a.id_in,    \
+        a.flags_in, a.key_out, a.id_out, a.flags_out, a.cand_counter);                                     \
   } while (0)
   if (kpl == 1) KNN_PROP_LAUNCH(1);
   else if (kpl == 2) KNN_PROP_LAUNCH(2);
@@ -287,15 +312,20 @@ static void launch_prop_metric(const PropArgs& a, int kpl, int hbits, size_t wb,
 }
 
 template <int METRIC>
-static void launch_prop_rows(const PropArgs& a, int kpl, int hbits, size_t wb, int wpb, unsigned grid) {
-  if (a.Xh) launch_prop_metric<METRIC, true>(a, kpl, hbits, wb, wpb, grid);
-  else launch_prop_metric<METRIC, false>(a, kpl, hbits, wb, wpb, grid);
+static void launch_prop_rows(const PropArgs& a, int kpl, int hbits, size_t wb, int wpb, unsigned grid, int nbuf) {
+  if (nbuf == 2) {
+    if (a.Xh) launch_prop_metric<METRIC, true, 2>(a, kpl, hbits, wb, wpb, grid);
+    else launch_prop_metric<METRIC, false, 2>(a, kpl, hbits, wb, wpb, grid);
+  } else {
+    if (a.Xh) launch_prop_metric<METRIC, true, 1>(a, kpl, hbits, wb, wpb, grid);
+    else launch_prop_metric<METRIC, false, 1>(a, kpl, hbits, wb, wpb, grid);
+  }
 }
 
 int propagate_step(const PropArgs& a, LaunchLog& log) {
   const int kpl = kpl_for(a.k);
   const int hbits = prop_hash_bits(a.k);
-  const size_t wb = prop_warp_bytes(a.k, a.d);
+  size_t wb = prop_warp_bytes(a.k, a.d, 1);
   int wpb = (int)(kPropSmemBudget / wb);
   if (wpb > kPropMaxWarps) wpb = kPropMaxWarps;
   if (wpb < 1) return KNN_ERR_UNSUPPORTED;
@@ -305,14 +335,22 @@ int propagate_step(const PropArgs& a, LaunchLog& log) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int per_sm = (int)((220 * 1024) / (wb * wpb));
   if (per_sm < 1) per_sm = 1;
+  // a second row-slice buffer where it leaves the warps per SM as they are
+  // (the results do not depend on it)
+  int nbuf = 1;
+  const size_t wb2 = prop_warp_bytes(a.k, a.d, 2);
+  if (wb2 * wpb <= kPropSmemBudget && (int)((220 * 1024) / (wb2 * wpb)) >= per_sm) {
+    nbuf = 2;
+    wb = wb2;
+  }
   const int64_t cnt = (a.r1 > 0 ? a.r1 : a.n) - a.r0;
   if (cnt <= 0) return KNN_OK;
   const int64_t want = (cnt + wpb - 1) / wpb;
   const int64_t cap = (int64_t)sms * per_sm;
   const unsigned grid = (unsigned)(want < cap ? want : cap);
-  if (a.metric == KNN_METRIC_EUCLIDEAN) launch_prop_rows<KNN_METRIC_EUCLIDEAN>(a, kpl, hbits, wb, wpb, grid);
-  else if (a.metric == KNN_METRIC_TAXICAB) launch_prop_rows<KNN_METRIC_TAXICAB>(a, kpl, hbits, wb, wpb, grid);
-  else launch_prop_rows<KNN_METRIC_COSINE>(a, kpl, hbits, wb, wpb, grid);
+  if (a.metric == KNN_METRIC_EUCLIDEAN) launch_prop_rows<KNN_METRIC_EUCLIDEAN>(a, kpl, hbits, wb, wpb, grid, nbuf);
+  else if (a.metric == KNN_METRIC_TAXICAB) launch_prop_rows<KNN_METRIC_TAXICAB>(a, kpl, hbits, wb, wpb, grid, nbuf);
+  else launch_prop_rows<KNN_METRIC_COSINE>(a, kpl, hbits, wb, wpb, grid, nbuf);
   log.add();
   return cudaPeekAtLastError() == cudaSuccess ? KNN_OK : KNN_ERR_CUDA;
 }
