@@ -576,7 +576,7 @@ def run_single(args, w):
 # ---------------------------------------------------------- dataset batch --
 # Cheapest settings reaching aggregate recall@15 >= 0.95 over the batch, per
 # path, from `--workload dataset_batch --sweep`.
-BATCH_TARGETS = {"plain_fp32": (8, 512, 3), "mixed": (8, 2048, 0)}
+BATCH_TARGETS = {"plain_fp32": (8, 512, 3), "mixed": (3, 4096, 0)}
 
 
 def run_batch(args):
