@@ -720,7 +720,7 @@ def run_batch(args):
 # reach the target within the swept grid (its best setting is given instead).
 CONFIG_TARGETS = {
     "sparse_prototypes": {"plain_fp32": (4, 131072, 1)},
-    "normalized_mixture": {"plain_fp32": (24, 2048, 0), "mixed_f16": (16, 4096, 0),
+    "normalized_mixture": {"plain_fp32": (24, 2048, 0), "mixed_f16": (15, 4096, 0),
                            "mixed_f16_learned": (16, 4096, 1)},
 }
 PATH_OPTIONS = {
