@@ -25,11 +25,10 @@
 //     w reads lane quarter w%4, two 32-column slices); three instructions per
 //     key filter it against a slightly widened bound of the row's last entry
 //     into a survivor bit mask, then (while the next tile's MMA runs) the warps
-//     of each lane quarter read each 32-column slice holding survivors of
-//     their rows back from tensor memory once, move a row's products across
-//     the lanes by shuffles, compute the survivors' exact keys and insert them
-//     into the query's sorted list (held in shared memory for the whole block)
-//     with one ballot and one lane shift each.  Two block barriers per tile.
+//     of each lane quarter read their rows' few survivors back from tensor
+//     memory, compute their exact keys and insert them into the query's sorted
+//     list (held in shared memory for the whole block) with one ballot and one
+//     lane shift each.  Two block barriers per tile.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -571,68 +570,60 @@ __global__ void __launch_bounds__(kUThreads, 2)
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (has_next && tid == 0) issue_mma(s + 1);
     if (pass == 1) {
-      // The quarter's rows with survivors (one ballot) alternate between its
-      // two warps.  Per 32-column slice the warp reads its lane quarter of
-      // tensor memory once (lane r: row r's 32 products); each of its rows
-      // with survivors there takes its products across the lanes by 32
-      // shuffles (lane j: column j), and the survivors' exact keys are
-      // inserted from registers.  One tensor-memory load per slice instead of
-      // one per survivor: a load waits behind the next tile's MMA.
+      // The quarter's rows with survivors (one ballot) alternate between
+      // its two warps; survivors' products come from the warp's lane
+      // quarter of tensor memory.
       const int rowq = quarter * 32 + lane;
-      uint32_t mrow[4];
-#pragma unroll
-      for (int h = 0; h < 4; ++h) mrow[h] = rowq < mq ? msk[rowq * 4 + h] : 0u;
-      const bool has = (mrow[0] | mrow[1] | mrow[2] | mrow[3]) != 0;
+      const bool has = rowq < mq && (msk[rowq * 4] | msk[rowq * 4 + 1] | msk[rowq * 4 + 2] | msk[rowq * 4 + 3]) != 0;
       const uint32_t all = __ballot_sync(0xFFFFFFFFu, has);
       const bool mine = has && (__popc(all & ((1u << lane) - 1u)) & 1) == half;
-#pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        uint32_t rws = __ballot_sync(0xFFFFFFFFu, mine && mrow[h] != 0u);
-        if (rws == 0) continue;
-        const int cb = h * 32;  // the slice's first column in the tile
-        uint32_t v[32];
-        tmem_ld32(tq + (uint32_t)cb, v);
-        const float cnl = cn[cb + lane];
-        const uint32_t cil = (uint32_t)cid[cb + lane];
+      uint32_t rows = __ballot_sync(0xFFFFFFFFu, mine);
+      while (rows) {
+        const int ql = __ffs(rows) - 1;  // row within the quarter
+        const int qq = quarter * 32 + ql;
+        rows &= rows - 1;
+        float lk = Lk[qq * kLS + lane];
+        uint32_t li = Li[qq * kLS + lane];
+        const float myn = qn[qq];
 #pragma unroll 1
-        while (rws) {
-          const int ql = __ffs(rws) - 1;  // row within the quarter
-          const int qq = quarter * 32 + ql;
-          rws &= rws - 1;
-          uint32_t bal = __shfl_sync(0xFFFFFFFFu, mrow[h], ql);
-          // lane j <- product of column cb + j of row qq
-          float dot = 0.f;
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const float t = __shfl_sync(0xFFFFFFFFu, __uint_as_float(v[j]), ql);
-            if (lane == j) dot = t;
-          }
-          const float myn = qn[qq];
-          const bool sv = (bal >> lane) & 1u;
-          const float ck = !sv ? kInf
-                               : (METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cnl))
-                                                                 : __fsub_rn(1.f, dot));
-          const uint32_t ci = sv ? cil : kNoId;
-          float lk = Lk[qq * kLS + lane];
-          uint32_t li = Li[qq * kLS + lane];
+        for (int h = 0; h < 4; ++h) {
+          uint32_t bal = msk[qq * 4 + h];
+          if (bal == 0) continue;
+          const int cb = h * 32;  // the slice's first column in the tile
           if (FIRST && __popc(bal) >= kBulkMerge) {
-            float sk = ck;
-            uint32_t si = ci;
-            warp_bitonic_sort32(sk, si);
-            warp_merge_lower(lk, li, sk, si);
-          } else {
-            while (bal) {
-              const int j = __ffs(bal) - 1;
-              bal &= bal - 1;
-              const float k1 = __shfl_sync(0xFFFFFFFFu, ck, j);
-              const uint32_t i1 = __shfl_sync(0xFFFFFFFFu, ci, j);
-              const bool dup = !FIRST && !xcl && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
-              if (!dup) warp_insert1(lk, li, k1, i1);
+            // lane j <- product of column cb + j of row qq
+            uint32_t v[32];
+            tmem_ld32(tq + (uint32_t)cb, v);
+            float dot = 0.f;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const float t = __shfl_sync(0xFFFFFFFFu, __uint_as_float(v[j]), ql);
+              if (lane == j) dot = t;
             }
+            float ck = kInf;
+            uint32_t ci = kNoId;
+            if ((bal >> lane) & 1u) {
+              ck = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[cb + lane]))
+                                                  : __fsub_rn(1.f, dot);
+              ci = (uint32_t)cid[cb + lane];
+            }
+            warp_bitonic_sort32(ck, ci);
+            warp_merge_lower(lk, li, ck, ci);
+            continue;
           }
-          Lk[qq * kLS + lane] = lk;
-          Li[qq * kLS + lane] = li;
+          while (bal) {
+            const int j = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const float dot = __shfl_sync(0xFFFFFFFFu, __uint_as_float(tmem_ld1(tq + (uint32_t)(cb + j))), ql);
+            const float k1 = METRIC == KNN_METRIC_EUCLIDEAN ? __fmaf_rn(-2.f, dot, __fadd_rn(myn, cn[cb + j]))
+                                                            : __fsub_rn(1.f, dot);
+            const uint32_t i1 = (uint32_t)cid[cb + j];
+            const bool dup = !FIRST && !xcl && __ballot_sync(0xFFFFFFFFu, lane < kq && li == i1) != 0;
+            if (!dup) warp_insert1(lk, li, k1, i1);
+          }
         }
+        Lk[qq * kLS + lane] = lk;
+        Li[qq * kLS + lane] = li;
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
