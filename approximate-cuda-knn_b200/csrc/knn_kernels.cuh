@@ -123,7 +123,7 @@ struct LeafArgs {
   int32_t* perm_w;       // [trees][n] or null
   uint8_t* bucket;       // [n]
   int32_t* sort_tmp;     // [n]
-  uint32_t* tmask;       // [leaves][ceil(maxleaf / tile)][ceil(dpad / 32)]
+  uint32_t* tmask;       // [leaves][ceil(maxleaf / tile)][ceil(dpad / 32) + 1]
   cudaStream_t stream;
 };
 int leaf_stage(const LeafArgs& a, LaunchLog& log);

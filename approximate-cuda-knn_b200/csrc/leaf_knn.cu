@@ -220,11 +220,15 @@ __global__ void __launch_bounds__(1024) k_leaf_bucket_sort(int32_t* __restrict__
   for (int r = threadIdx.x; r < n; r += 1024) perm[lo + r] = tmp[lo + r];
 }
 
-// tmask[leaf][t][w]: the dims non-zero in some row of the leaf's tile t (TILE
-// positions), W = ceil(dpad / 32) words, every word written.  grid (leaf, tile).
+// tmask[leaf][t][0..W): the dims non-zero in some row of the leaf's tile t
+// (TILE positions), W = ceil(dpad / 32) words, every word written; word W: the
+// 32-dim chunks of the tile's own list (each 256-dim group padded), so that a
+// pair with a tile whose list saves nothing skips building one.  grid (leaf, tile).
 __global__ void __launch_bounds__(256) k_tile_dim_mask(const float* __restrict__ X, int dpad, SegView segs, int k,
                                                        const int32_t* __restrict__ perm, int tile, int tpl,
                                                        uint32_t* __restrict__ tmask, int W) {
+  __shared__ int gcount;
+  int chunks = 0;  // thread 0
   const int64_t leaf = blockIdx.x;
   int64_t j, lo, hi, blo, bhi;
   const SegEntry seg = segs.leaf(leaf, &j);
@@ -232,15 +236,23 @@ __global__ void __launch_bounds__(256) k_tile_dim_mask(const float* __restrict__
   const int64_t r0 = lo + (int64_t)blockIdx.y * tile;
   if (r0 >= hi) return;
   const int64_t r1 = min(hi, r0 + tile);
-  uint32_t* out = tmask + ((size_t)leaf * tpl + blockIdx.y) * W;
-  for (int dim0 = 0; dim0 < dpad; dim0 += 256) {
+  uint32_t* out = tmask + ((size_t)leaf * tpl + blockIdx.y) * (W + 1);
+  for (int dim0 = 0; dim0 < dpad; dim0 += 256) {  // one 256-dim group per pass
     const int dim = dim0 + (int)threadIdx.x;
+    if (threadIdx.x == 0) gcount = 0;
+    __syncthreads();
     bool nz = false;
     if (dim < dpad)
       for (int64_t r = r0; r < r1 && !nz; ++r) nz = __ldg(X + (size_t)__ldg(perm + r) * dpad + dim) != 0.f;
     const uint32_t bits = __ballot_sync(0xFFFFFFFFu, nz);
-    if ((threadIdx.x & 31) == 0 && dim < dpad) out[dim >> 5] = bits;
+    if ((threadIdx.x & 31) == 0 && dim < dpad) {
+      out[dim >> 5] = bits;
+      if (bits) atomicAdd(&gcount, __popc(bits));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) chunks += (gcount + 31) / 32;
   }
+  if (threadIdx.x == 0) out[W] = (uint32_t)chunks;
 }
 
 
@@ -512,17 +524,21 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf_pair(
     dl = dlist + leaf * lmax;
     nchunks = dnch[leaf];
   }
-  if (METRIC != KNN_METRIC_COSINE && tmask) {  // block-uniform
+  // the union of two tiles' dims lists no fewer chunks than either tile's own
+  // list, so a pair with a tile whose list saves nothing reads rows whole
+  const uint32_t* ma = tmask ? tmask + ((size_t)leaf * tpl + a) * (W + 1) : nullptr;
+  const uint32_t* mb = tmask ? tmask + ((size_t)leaf * tpl + b) * (W + 1) : nullptr;
+  const bool listed = METRIC != KNN_METRIC_COSINE && tmask && (int)__ldg(ma + W) < nchunks &&
+                      (int)__ldg(mb + W) < nchunks;  // block-uniform
+  if (listed) {
     if (tid < 32) {
-      const uint32_t* ma = tmask + ((size_t)leaf * tpl + a) * W;
-      const uint32_t* mb = tmask + ((size_t)leaf * tpl + b) * W;
       const int nch = warp_dim_list<int16_t>([&](int w) { return __ldg(ma + w) | __ldg(mb + w); }, W, d, dpad, sl);
       if (tid == 0) snch = nch;
     }
     __syncthreads();
     if (snch >= 0) nchunks = snch;
   }
-  const int16_t* sdl = (METRIC != KNN_METRIC_COSINE && tmask && snch >= 0) ? sl : nullptr;
+  const int16_t* sdl = (listed && snch >= 0) ? sl : nullptr;
   const int mq = min(TILE, n - a * TILE), mc = min(TILE, n - b * TILE);
   if (pair_counter && tid == 0)
     atomicAdd(pair_counter, a == b ? (unsigned long long)mq * (unsigned long long)(mq - 1)
