@@ -477,6 +477,7 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
       // scratch) by row bucket, which leaves every leaf's point set as it is
       a.perm_w = const_cast<int32_t*>(perm);
       rc = C->get("rbucket", (size_t)n, &a.bucket);
+      if (!rc) rc = C->get("rzeros", 1, &a.zeros);
       if (!rc) rc = C->get("sort_tmp", (size_t)n, &a.sort_tmp);
       if (!rc)
         rc = C->get("tmask", (size_t)lay.leaves * ((lay.maxleaf + 31) / 32) * ((dpad + 31) / 32 + 1), &a.tmask);

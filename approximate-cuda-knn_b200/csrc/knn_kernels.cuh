@@ -122,6 +122,7 @@ struct LeafArgs {
   // bucket (perm_w: writable alias of perm), per-tile dim masks
   int32_t* perm_w;       // [trees][n] or null
   uint8_t* bucket;       // [n]
+  uint32_t* zeros;       // [1]: some row has a zero among its d dims
   int32_t* sort_tmp;     // [n]
   uint32_t* tmask;       // [leaves][ceil(maxleaf / tile)][ceil(dpad / 32) + 1]
   cudaStream_t stream;

@@ -141,21 +141,28 @@ constexpr int kBucketBits = 8;
 constexpr int kMaxListDims = 4096;  // padded dims of a tile pair's list in shared memory
 
 // bucket[row]: the top 8 bits of a hash of the row's non-zero pattern (one
-// ballot word per 32 dims).  One warp per row.
-__global__ void __launch_bounds__(256) k_row_bucket(const float* __restrict__ X, int64_t n, int dpad,
-                                                    uint8_t* __restrict__ bucket) {
+// ballot word per 32 dims).  One warp per row.  *zeros (cleared beforehand)
+// becomes 1 when some row has a zero among its d dims: without one, every tile
+// reads rows whole, and the order and masks below are skipped.
+__global__ void __launch_bounds__(256) k_row_bucket(const float* __restrict__ X, int64_t n, int d, int dpad,
+                                                    uint8_t* __restrict__ bucket, uint32_t* __restrict__ zeros) {
   const int64_t row = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= n) return;
   const float* x = X + (size_t)row * dpad;
   uint64_t h = 0x9E3779B97F4A7C15ull;
+  int nnz = 0;
   for (int d0 = 0; d0 < dpad; d0 += 32) {
-    const bool nz = d0 + lane < dpad && x[d0 + lane] != 0.f;
+    const bool nz = d0 + lane < d && x[d0 + lane] != 0.f;
     const uint32_t w = __ballot_sync(0xFFFFFFFFu, nz);
     h = (h ^ w) * 0x100000001B3ull;
     h ^= h >> 29;
+    nnz += __popc(w);
   }
-  if (lane == 0) bucket[row] = (uint8_t)(h >> (64 - kBucketBits));
+  if (lane == 0) {
+    bucket[row] = (uint8_t)(h >> (64 - kBucketBits));
+    if (nnz < d && *reinterpret_cast<volatile uint32_t*>(zeros) == 0u) atomicOr(zeros, 1u);
+  }
 }
 
 // Each leaf's positions stably ordered by bucket.  One block of 1024 threads
@@ -164,10 +171,12 @@ __global__ void __launch_bounds__(256) k_row_bucket(const float* __restrict__ X,
 // (bucket, warp); tmp holds the new order until it is copied back.
 __global__ void __launch_bounds__(1024) k_leaf_bucket_sort(int32_t* __restrict__ perm, SegView segs, int k,
                                                            const uint8_t* __restrict__ bucket,
-                                                           int32_t* __restrict__ tmp) {
+                                                           int32_t* __restrict__ tmp,
+                                                           const uint32_t* __restrict__ zeros) {
   constexpr int NB = 1 << kBucketBits;
   __shared__ int cnt[32][NB];
   __shared__ int tot[NB];
+  if (*zeros == 0u) return;  // no zero anywhere: nothing to order
   const int64_t leaf = blockIdx.x;
   int64_t j, lo, hi, blo, bhi;
   const SegEntry seg = segs.leaf(leaf, &j);
@@ -226,9 +235,11 @@ __global__ void __launch_bounds__(1024) k_leaf_bucket_sort(int32_t* __restrict__
 // pair with a tile whose list saves nothing skips building one.  grid (leaf, tile).
 __global__ void __launch_bounds__(256) k_tile_dim_mask(const float* __restrict__ X, int dpad, SegView segs, int k,
                                                        const int32_t* __restrict__ perm, int tile, int tpl,
-                                                       uint32_t* __restrict__ tmask, int W) {
+                                                       uint32_t* __restrict__ tmask, int W,
+                                                       const uint32_t* __restrict__ zeros) {
   __shared__ int gcount;
   int chunks = 0;  // thread 0
+  if (*zeros == 0u) return;  // no zero anywhere: the pairs read rows whole
   const int64_t leaf = blockIdx.x;
   int64_t j, lo, hi, blo, bhi;
   const SegEntry seg = segs.leaf(leaf, &j);
@@ -490,8 +501,8 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf_pair(
     const float* __restrict__ X, int d, int dpad, SegView segs, int k, const int32_t* __restrict__ perm,
     const float* __restrict__ norms, float* __restrict__ rkey, uint32_t* __restrict__ rid,
     unsigned long long* __restrict__ pair_counter, const int32_t* __restrict__ dlist,
-    const int32_t* __restrict__ dnch, int lmax, const uint32_t* __restrict__ tmask, int tpl, int W, int round,
-    int tpr) {
+    const int32_t* __restrict__ dnch, int lmax, const uint32_t* __restrict__ tmask, int tpl, int W,
+    const uint32_t* __restrict__ zeros, int round, int tpr) {
   static_assert(TILE == 32 || TILE == 64, "tile of 32 or 64");
   __shared__ __align__(16) float Qs[kDC][TILE + 4];
   __shared__ __align__(16) float Cs[kDC][TILE + 4];
@@ -528,7 +539,7 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf_pair(
   // list, so a pair with a tile whose list saves nothing reads rows whole
   const uint32_t* ma = tmask ? tmask + ((size_t)leaf * tpl + a) * (W + 1) : nullptr;
   const uint32_t* mb = tmask ? tmask + ((size_t)leaf * tpl + b) * (W + 1) : nullptr;
-  const bool listed = METRIC != KNN_METRIC_COSINE && tmask && (int)__ldg(ma + W) < nchunks &&
+  const bool listed = METRIC != KNN_METRIC_COSINE && tmask && *zeros != 0u && (int)__ldg(ma + W) < nchunks &&
                       (int)__ldg(mb + W) < nchunks;  // block-uniform
   if (listed) {
     if (tid < 32) {
@@ -575,9 +586,10 @@ static int pair_tiles(int64_t maxleaf) {
 // dim masks of its tiles (two launches before the rounds).
 template <int TILE>
 static int sparse_tile_masks(const LeafArgs& a, int32_t* perm, int64_t leaves, int tpl, int W) {
-  k_leaf_bucket_sort<<<(unsigned)leaves, 1024, 0, a.stream>>>(perm, a.segs, a.k, a.bucket, a.sort_tmp);
+  k_leaf_bucket_sort<<<(unsigned)leaves, 1024, 0, a.stream>>>(perm, a.segs, a.k, a.bucket, a.sort_tmp,
+                                                               a.zeros);
   k_tile_dim_mask<<<dim3((unsigned)leaves, (unsigned)tpl), 256, 0, a.stream>>>(a.X, a.dpad, a.segs, a.k, perm, TILE,
-                                                                               tpl, a.tmask, W);
+                                                                               tpl, a.tmask, W, a.zeros);
   return 2;
 }
 
@@ -601,15 +613,15 @@ static int launch_leaf_tile(const LeafArgs& a, const int32_t* perm, const int64_
       if (kpl == 1)
         k_leaf_pair<METRIC, 1, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey,
                                                                   a.rid, a.pair_counter, dlist, a.dnch, a.lmax, tmask,
-                                                                  tpl, W, r, tpr);
+                                                                  tpl, W, a.zeros, r, tpr);
       else if (kpl == 2)
         k_leaf_pair<METRIC, 2, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey,
                                                                   a.rid, a.pair_counter, dlist, a.dnch, a.lmax, tmask,
-                                                                  tpl, W, r, tpr);
+                                                                  tpl, W, a.zeros, r, tpr);
       else
         k_leaf_pair<METRIC, 4, TILE><<<grid, 256, 0, a.stream>>>(a.X, a.d, a.dpad, a.segs, a.k, perm, a.norms, a.rkey,
                                                                   a.rid, a.pair_counter, dlist, a.dnch, a.lmax, tmask,
-                                                                  tpl, W, r, tpr);
+                                                                  tpl, W, a.zeros, r, tpr);
     }
     return tpr + extra;
   }
@@ -652,7 +664,8 @@ static void launch_leaf_metric(const LeafArgs& a, int t, int kpl, LaunchLog& log
 int leaf_stage(const LeafArgs& a, LaunchLog& log) {
   const int kpl = kpl_for(a.k);
   if (a.tmask && a.bucket && a.n > 0) {
-    k_row_bucket<<<(unsigned)((a.n + 7) / 8), 256, 0, a.stream>>>(a.X, a.n, a.dpad, a.bucket);
+    cudaMemsetAsync(a.zeros, 0, sizeof(uint32_t), a.stream);
+    k_row_bucket<<<(unsigned)((a.n + 7) / 8), 256, 0, a.stream>>>(a.X, a.n, a.d, a.dpad, a.bucket, a.zeros);
     log.add();
   }
   for (int t = a.first_tree; t < a.first_tree + a.trees; ++t) {
