@@ -492,8 +492,9 @@ int run_leaf(knn_context* C, const float* X, int64_t n, int d, int dpad, int k, 
 // Sparse-row leaf tiles (same keys, fewer dims read): forced on or off by the
 // option, else on when leaves hold at least 1024 points, where the per-tree
 // mask pass (one read of the points) is small beside the tiles.
-bool use_sparse_dims(const knn_options& o, int metric, const Layout& lay) {
-  if (metric == KNN_METRIC_COSINE || lay.ftable || o.sparse_dims < 0) return false;
+bool use_sparse_dims(const knn_options& o, int metric, const Layout& lay, int dpad) {
+  // dim lists are 16-bit
+  if (metric == KNN_METRIC_COSINE || lay.ftable || o.sparse_dims < 0 || dpad > 32767) return false;
   return o.sparse_dims > 0 || lay.maxleaf >= 1024;
 }
 
@@ -694,7 +695,7 @@ int pick_shapes(knn_context* C, const knn_options& o, bool may_tune, bool fp32_l
                 int* err_flag) {
   sh->leaf_tile = o.leaf_tile;
   sh->prop_warps = o.prop_warps;
-  sh->sparse = fp32_leaf && use_sparse_dims(o, metric, lay);
+  sh->sparse = fp32_leaf && use_sparse_dims(o, metric, lay, dpad);
   sh->pairs = fp32_leaf && use_tile_pairs(o, lay);
   *tune_prop_after = false;
   const std::string key = tune_key(metric, d, k, lay.maxleaf);

@@ -112,7 +112,7 @@ struct LeafArgs {
   // sparse rows (EUCLIDEAN / TAXICAB, median trees): per tree, each leaf block's
   // non-zero dims; null dlist: every block reads all dims
   uint32_t* dmask;       // [leaves][dpad / 32 + 1]
-  int32_t* dlist;        // [leaves][lmax]
+  int16_t* dlist;        // [leaves][lmax], dims below 32768
   int32_t* dnch;         // [leaves]
   int lmax;              // 256 * ceil(dpad / 256)
   // every leaf is its own block (at least k+1 points, median trees): each tile

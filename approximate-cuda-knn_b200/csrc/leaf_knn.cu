@@ -110,12 +110,12 @@ __device__ __forceinline__ int warp_dim_list(MaskFn word, int W, int d, int dpad
   return pos / 32 < (d + 31) / 32 ? pos / 32 : -1;
 }
 
-__device__ __forceinline__ int4 load_dims4(const int32_t* p) { return __ldg(reinterpret_cast<const int4*>(p)); }
+// Dim lists are 16-bit (dims below 32768), in global memory (a leaf block's
+// list) or shared memory (a tile pair's): generic loads serve both.
 __device__ __forceinline__ int4 load_dims4(const int16_t* p) {
   const short4 v = *reinterpret_cast<const short4*>(p);
   return make_int4(v.x, v.y, v.z, v.w);
 }
-__device__ __forceinline__ int load_dim(const int32_t* p) { return __ldg(p); }
 __device__ __forceinline__ int load_dim(const int16_t* p) { return *p; }
 
 // One warp per leaf: the listed dims of every 256-dim group in increasing order,
@@ -123,13 +123,13 @@ __device__ __forceinline__ int load_dim(const int16_t* p) { return *p; }
 // 32, or -1 when the list saves no chunk over the ceil(d / 32) chunks of all dims
 // (the block then reads rows whole).
 __global__ void __launch_bounds__(256) k_leaf_dim_list(const uint32_t* __restrict__ mask, int W, int d, int dpad,
-                                                       int64_t leaves, int32_t* __restrict__ dlist,
+                                                       int64_t leaves, int16_t* __restrict__ dlist,
                                                        int32_t* __restrict__ dnch, int lmax) {
   const int64_t leaf = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (leaf >= leaves) return;
   const uint32_t* m = mask + leaf * W;
-  const int nch = warp_dim_list<int32_t>([&](int w) { return m[w]; }, W, d, dpad, dlist + leaf * lmax);
+  const int nch = warp_dim_list<int16_t>([&](int w) { return m[w]; }, W, d, dpad, dlist + leaf * lmax);
   if (lane == 0) dnch[leaf] = nch;
 }
 
@@ -273,8 +273,8 @@ __global__ void __launch_bounds__(256) k_tile_dim_mask(const float* __restrict__
 // (all dims, or the listed non-zero dims dl of a sparse block) in the
 // reference's order: a sequential partial per 256-dim group, added to the
 // total at the group's end.  Ks receives the keys, +inf outside mq x mc.
-template <int METRIC, int TILE, typename LT>
-__device__ __forceinline__ void tile_keys(const float* __restrict__ X, int dpad, const LT* __restrict__ dl,
+template <int METRIC, int TILE>
+__device__ __forceinline__ void tile_keys(const float* __restrict__ X, int dpad, const int16_t* dl,
                                           int nchunks, int mq, int mc, const int32_t* qid, const int32_t* cid,
                                           const float* qnorm, const float* cnorm, float (*Qs)[TILE + 4],
                                           float (*Cs)[TILE + 4], float (*Ks)[TILE + 1]) {
@@ -422,7 +422,7 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* _
                                               const float* __restrict__ norms,
                                               float* __restrict__ rkey, uint32_t* __restrict__ rid,
                                               unsigned long long* __restrict__ pair_counter,
-                                              const int32_t* __restrict__ dlist,
+                                              const int16_t* __restrict__ dlist,
                                               const int32_t* __restrict__ dnch, int lmax) {
   constexpr int kTile = TILE;
   static_assert(TILE == 32 || TILE == 64, "tile of 32 or 64");
@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* _
   const int nb = (int)(bhi - blo);
   const int tid = threadIdx.x;
   // sparse rows: this block's non-zero dims, 32 per chunk (null: all dims)
-  const int32_t* dl = nullptr;
+  const int16_t* dl = nullptr;
   int nchunks = (d + kDC - 1) / kDC;
   if (METRIC != KNN_METRIC_COSINE && dlist && dnch[leaf] >= 0) {
     dl = dlist + leaf * lmax;
@@ -476,7 +476,7 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf(const float* _
         if (METRIC == KNN_METRIC_COSINE) cnorm[tid] = id >= 0 ? norms[id] : 0.f;
       }
       __syncthreads();
-      tile_keys<METRIC, TILE, int32_t>(X, dpad, dl, nchunks, mq, mc, qid, cid, qnorm, cnorm, Qs, Cs, Ks);
+      tile_keys<METRIC, TILE>(X, dpad, dl, nchunks, mq, mc, qid, cid, qnorm, cnorm, Qs, Cs, Ks);
       __syncthreads();
       merge_rows<KPL, TILE, false>(k, mq, mc, qid, cid, Ks, rkey, rid);
       __syncthreads();
@@ -500,7 +500,7 @@ template <int METRIC, int KPL, int TILE>
 __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf_pair(
     const float* __restrict__ X, int d, int dpad, SegView segs, int k, const int32_t* __restrict__ perm,
     const float* __restrict__ norms, float* __restrict__ rkey, uint32_t* __restrict__ rid,
-    unsigned long long* __restrict__ pair_counter, const int32_t* __restrict__ dlist,
+    unsigned long long* __restrict__ pair_counter, const int16_t* __restrict__ dlist,
     const int32_t* __restrict__ dnch, int lmax, const uint32_t* __restrict__ tmask, int tpl, int W,
     const uint32_t* __restrict__ zeros, int round, int tpr) {
   static_assert(TILE == 32 || TILE == 64, "tile of 32 or 64");
@@ -529,7 +529,7 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf_pair(
   }
   if (a >= T || b >= T) return;
   const int tid = threadIdx.x;
-  const int32_t* dl = nullptr;
+  const int16_t* dl = nullptr;
   int nchunks = (d + kDC - 1) / kDC;
   if (METRIC != KNN_METRIC_COSINE && dlist && !tmask && dnch[leaf] >= 0) {
     dl = dlist + leaf * lmax;
@@ -547,9 +547,11 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf_pair(
       if (tid == 0) snch = nch;
     }
     __syncthreads();
-    if (snch >= 0) nchunks = snch;
+    if (snch >= 0) {
+      nchunks = snch;
+      dl = sl;
+    }
   }
-  const int16_t* sdl = (listed && snch >= 0) ? sl : nullptr;
   const int mq = min(TILE, n - a * TILE), mc = min(TILE, n - b * TILE);
   if (pair_counter && tid == 0)
     atomicAdd(pair_counter, a == b ? (unsigned long long)mq * (unsigned long long)(mq - 1)
@@ -565,8 +567,7 @@ __global__ void __launch_bounds__(256, TILE == 64 ? 4 : 5) k_leaf_pair(
     }
   }
   __syncthreads();
-  if (sdl) tile_keys<METRIC, TILE, int16_t>(X, dpad, sdl, nchunks, mq, mc, qid, cid, qnorm, cnorm, Qs, Cs, Ks);
-  else tile_keys<METRIC, TILE, int32_t>(X, dpad, dl, nchunks, mq, mc, qid, cid, qnorm, cnorm, Qs, Cs, Ks);
+  tile_keys<METRIC, TILE>(X, dpad, dl, nchunks, mq, mc, qid, cid, qnorm, cnorm, Qs, Cs, Ks);
   __syncthreads();
   merge_rows<KPL, TILE, false>(k, mq, mc, qid, cid, Ks, rkey, rid);
   if (a != b) merge_rows<KPL, TILE, true>(k, mc, mq, cid, qid, Ks, rkey, rid);
@@ -595,7 +596,7 @@ static int sparse_tile_masks(const LeafArgs& a, int32_t* perm, int64_t leaves, i
 
 template <int METRIC, int TILE>
 static int launch_leaf_tile(const LeafArgs& a, const int32_t* perm, const int64_t* ftab, int64_t leaves, int kpl,
-                            const int32_t* dlist, int32_t* perm_w) {
+                            const int16_t* dlist, int32_t* perm_w) {
   if (leaves <= 0) return 0;
   const int tpr = (a.pairs && !ftab) ? pair_tiles<TILE>(a.maxleaf) : 0;
   if (tpr) {
@@ -641,7 +642,7 @@ static void launch_leaf_metric(const LeafArgs& a, int t, int kpl, LaunchLog& log
   const int32_t* perm = a.perm + (size_t)t * a.n;
   const int64_t* ftab = a.ftable ? a.ftable + 4 * a.foff[t] : nullptr;
   const int64_t leaves = a.ftable ? a.fcount[t] : a.leaves;
-  const int32_t* dlist = nullptr;
+  const int16_t* dlist = nullptr;
   int32_t* perm_w = a.perm_w ? a.perm_w + (size_t)t * a.n : nullptr;
   if (a.dlist && !a.tmask && !ftab && METRIC != KNN_METRIC_COSINE && leaves > 0) {
     const int W = a.dpad / 32 + 1;
