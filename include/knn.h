@@ -106,11 +106,13 @@ typedef struct knn_options {
                                 1, 2 or 4 (0: tuned with autotune, else the most that
                                 fit); a row keeps its own leaf's columns, so results do
                                 not depend on it; capped at what the leaves allow      */
-  int32_t sparse_dims;       /* FP32 leaf tiles, EUCLIDEAN and TAXICAB: 1 each leaf block
-                                reads only the dims that are non-zero in some of its
-                                rows (the left-out terms are exact zeros, so the keys
-                                keep their bits); -1 never; 0 when leaves hold at
-                                least 1024 points                                     */
+  int32_t sparse_dims;       /* FP32 leaf tiles, EUCLIDEAN and TAXICAB, d < 32768: 1 each
+                                tile reads only the dims that are non-zero in some of
+                                its rows (with tile pairs: the union of the pair's two
+                                tiles, each leaf's points ordered by zero pattern;
+                                the left-out terms are exact zeros, so the keys keep
+                                their bits); -1 never; 0 when leaves hold at least
+                                1024 points                                           */
   int32_t tile_pairs;        /* FP32 leaf tiles where every leaf is its own block: each
                                 key is computed once for both of its points (keys are
                                 symmetric bit for bit, so the graph is the same); -1 off,
