@@ -378,9 +378,10 @@ __global__ void __launch_bounds__(kUThreads, 2)
       Li[(warp + 8 * i) * kLS + lane] = lir[i];
     }
     if (xcl) {
-      // the listed ids' columns in this block, sorted per row (the 16
-      // rows' bitonic networks interleaved stage by stage)
-      uint32_t pos[kBM / 8];
+      // the listed ids' columns in this block, sorted per row: the 16 rows'
+      // bitonic networks interleaved stage by stage, two rows' 16-bit
+      // positions packed per register (halfword min / max)
+      uint32_t pk[kBM / 16];
 #pragma unroll
       for (int i = 0; i < kBM / 8; ++i) {
         uint32_t p = kXEnd;
@@ -388,7 +389,8 @@ __global__ void __launch_bounds__(kUThreads, 2)
           const int64_t q = (int64_t)inv[lir[i]] - blo;
           if (q >= 0 && q < nb) p = (uint32_t)q;
         }
-        pos[i] = p;
+        if (i & 1) pk[i >> 1] |= p << 16;
+        else pk[i >> 1] = p;
       }
 #pragma unroll
       for (int size = 2; size <= 32; size <<= 1) {
@@ -396,15 +398,15 @@ __global__ void __launch_bounds__(kUThreads, 2)
         for (int m = size >> 1; m >= 1; m >>= 1) {
           const bool keep_min = ((lane & size) == 0) == ((lane & m) == 0);
 #pragma unroll
-          for (int i = 0; i < kBM / 8; ++i) {
-            const uint32_t o = __shfl_xor_sync(0xFFFFFFFFu, pos[i], m);
-            pos[i] = keep_min ? min(pos[i], o) : max(pos[i], o);
+          for (int j = 0; j < kBM / 16; ++j) {
+            const uint32_t o = __shfl_xor_sync(0xFFFFFFFFu, pk[j], m);
+            pk[j] = keep_min ? __vminu2(pk[j], o) : __vmaxu2(pk[j], o);
           }
         }
       }
 #pragma unroll
       for (int i = 0; i < kBM / 8; ++i) {
-        xp[(warp + 8 * i) * kXS + lane] = (uint16_t)pos[i];
+        xp[(warp + 8 * i) * kXS + lane] = (uint16_t)((i & 1) ? (pk[i >> 1] >> 16) : (pk[i >> 1] & 0xFFFFu));
         if (lane == 0) xp[(warp + 8 * i) * kXS + 32] = (uint16_t)kXEnd;
       }
     }
