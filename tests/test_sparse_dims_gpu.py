@@ -76,3 +76,23 @@ def test_automatic_switch(lib):
     small = lib.knn_build(x, 8, 2, 512, 0, 1, seed=1, stats=True)[2]  # leaves of 512 points
     cos = lib.knn_build(x, 8, 2, 2048, 0, 2, seed=1, stats=True)[2]   # COSINE reads all dims
     assert (big["sparse_dims"], small["sparse_dims"], cos["sparse_dims"]) == (1, 0, 0)
+
+
+def test_batch_sparse_tile_pairs(lib, oracle):
+    """Batched sets of sparse rows (segments of different sizes and depths):
+    the per-leaf ordering, the tile masks and the pair lists work across
+    segments, and every set gets the oracle's graph."""
+    sets = [_prototypes(n, 200, protos=3, density=0.2, seed=40 + i) for i, n in enumerate((2600, 1500, 3900))]
+    got = lib.knn_build_batch(sets, 9, 2, 700, 1, 1, seeds=[5, 6, 7], sparse_dims=1)
+    off = lib.knn_build_batch(sets, 9, 2, 700, 1, 1, seeds=[5, 6, 7], sparse_dims=-1, tile_pairs=-1)
+    for i, x in enumerate(sets):
+        _same(got[i], off[i], f"set {i}: sparse tile pairs vs all dims one-sided")
+        _same(got[i], oracle.knn_build(x, 9, 2, 700, 1, 1, seed=5 + i), f"set {i}: vs oracle")
+
+
+def test_autotuned_sparse_tile_pairs(lib, oracle):
+    """The leaf-tile tuner times both tiles on tree 0 with the same shortcuts;
+    the graph does not depend on its choice."""
+    x = _prototypes(3000, 300, protos=4, density=0.2, seed=77)
+    tuned = lib.knn_build(x, 10, 3, 1500, 1, 0, seed=2, sparse_dims=1, autotune=True)
+    _same(tuned, oracle.knn_build(x, 10, 3, 1500, 1, 0, seed=2), "autotuned sparse tile pairs vs oracle")
