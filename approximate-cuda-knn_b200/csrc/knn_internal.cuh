@@ -222,6 +222,36 @@ __device__ __forceinline__ float group_project(const float* __restrict__ x,
   return acc;
 }
 
+// Four projections of one row at once (directions v[0..3]), each summed in
+// group_project's order, so each equals group_project's result bit for bit;
+// the four chains and their loads overlap.
+template <int G>
+__device__ __forceinline__ void group_project4(const float* __restrict__ x, const float* const (&v)[4], int dpad,
+                                               int gl, float (&out)[4]) {
+  const float4* x4 = reinterpret_cast<const float4*>(x);
+  const int nc = dpad >> 2;
+  float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  for (int c = gl; c < nc; c += G) {
+    const float4 a = __ldg(x4 + c);
+    float4 b[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) b[u] = __ldg(reinterpret_cast<const float4*>(v[u]) + c);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      acc[u] = __fmaf_rn(a.x, b[u].x, acc[u]);
+      acc[u] = __fmaf_rn(a.y, b[u].y, acc[u]);
+      acc[u] = __fmaf_rn(a.z, b[u].z, acc[u]);
+      acc[u] = __fmaf_rn(a.w, b[u].w, acc[u]);
+    }
+  }
+#pragma unroll
+  for (int off = G / 2; off >= 1; off >>= 1)
+#pragma unroll
+    for (int u = 0; u < 4; ++u) acc[u] = __fadd_rn(acc[u], __shfl_xor_sync(0xFFFFFFFFu, acc[u], off, G));
+#pragma unroll
+  for (int u = 0; u < 4; ++u) out[u] = acc[u];
+}
+
 // ------------------------------------------------------------- pair keys --
 __device__ __forceinline__ float cosine_key(float dot, float na, float nb) {
   if (na == 0.0f || nb == 0.0f) return 1.0f;

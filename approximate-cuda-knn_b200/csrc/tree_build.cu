@@ -81,12 +81,23 @@ __global__ void __launch_bounds__(256) k_project(const float* __restrict__ X, in
     const bool valid = i0 < ntot && a < active;
     if (a >= active) a = 0;
     const float* row = X + (size_t)i * dpad;
-    for (int t = 0; t < trees; ++t) {
-      const int64_t p = inv[(size_t)t * ntot + i];
-      const int64_t j = valid ? node[(size_t)t * ntot + i] : 0;
-      const float proj =
-          group_project<G>(row, dirs + (((size_t)a * trees + t) * nodes + j) * dpad, dpad, gl);
-      if (valid && gl == 0) keys[(size_t)t * ntot + p] = proj_key(proj, (uint32_t)i);
+    // four trees at a time: their index loads, direction loads and sums overlap
+    for (int t0 = 0; t0 < trees; t0 += 4) {
+      const int nt = min(4, trees - t0);  // warp-uniform
+      int64_t p[4];
+      const float* v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int t = t0 + (u < nt ? u : 0);  // past the last tree: a valid direction, result unused
+        p[u] = inv[(size_t)t * ntot + i];
+        const int64_t j = valid ? node[(size_t)t * ntot + i] : 0;
+        v[u] = dirs + (((size_t)a * trees + t) * nodes + j) * dpad;
+      }
+      float proj[4];
+      group_project4<G>(row, v, dpad, gl, proj);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (u < nt && valid && gl == 0) keys[(size_t)(t0 + u) * ntot + p[u]] = proj_key(proj[u], (uint32_t)i);
     }
   }
 }
